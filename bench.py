@@ -1,0 +1,310 @@
+"""Throughput of the MLFMA forward solve path: forward solves/s at true relative
+residual 1e-5 on the 1024x1024-pixel workload (102.4 wavelengths, 8 tree
+levels, 20 random lossy ellipses, 256 plane-wave transmitters), complex64 with
+FP64 reductions.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step solves all 256 transmitters as one batched, masked BiCGSTAB launch
+sequence.  Beside it the plain single-RHS solver (one transmitter per launch
+sequence, complex FP32 SIMT) and the reference's own CPU path
+(oracle/_ref, all host threads) are timed on bounded samples.  With N > 1
+(torchrun) every rank solves its own 256 transmitters; there is no collective
+on the data path.  One JSON line is printed by rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "inverse-solver-gpu_b200"))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+LEVEL = 8             # 1024 x 1024 pixels (reference `level`, mom.cpp:6,137)
+NTX = 256
+NELL = 20
+EPS = (1.1, 2.0)
+TAND = 0.1
+TOL = 1e-5
+SEED = 2000
+METRIC = "forward solves/s at rel. residual 1e-5: batched+learned vs plain FP32, 1 B200"
+
+
+def workload_config(engine: str, learned: bool) -> dict:
+    return {"workload": "1024x1024 px (102.4 lambda, lambda/10), 8 levels (7 MLFMA levels), 8x8 leaves; "
+                        "20 random ellipses eps_r U[1.1,2.0](1+i tan d), tan d U[0,0.1]; 256 plane-wave Tx; "
+                        "BiCGSTAB to true rel. residual 1e-5",
+            "grid": 1024, "levels": LEVEL, "transmitters": NTX, "batch": NTX, "tol": TOL,
+            "engine": engine, "learned_warm_start": learned, "seed": SEED,
+            "l2_policy": "inputs larger than L2 (26 GB working set per step)"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self) -> dict:
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as fh:
+            for line in fh:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows]
+        reasons = set()
+        for r in rows:
+            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"), r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]), "reasons": sorted(reasons),
+                "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())}
+
+
+def make_inputs(s, rank: int):
+    chi = s.phantom(seed=SEED + rank, count=NELL, axis=(1.0, 3.0), eps=EPS, tand_max=TAND)
+    g = (s.opts.k0 ** 2) * s.raster_to_tree(chi)          # tree order, as mom.cpp:288-289
+    b = s.plane_waves(NTX, order=0)                        # tree order (setup_born.cpp:62-65)
+    return g, b
+
+
+def peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return {"hbm_gbs": d["hbm_gbs"], "src": "measured"}
+    return {"hbm_gbs": 6650.0, "src": "fallback"}
+
+
+def algorithmic_bytes_per_matvec(s) -> float:
+    """8 (3U + 4S), S = sum over levels >= 2 of clusters x samples."""
+    S = sum((4 ** i) * s.numsamp(i) for i in range(2, s.level))
+    return 8.0 * (3 * s.numunk + 4 * S)
+
+
+def cpu_reference_sample(g, b, budget_s: float, max_solves: int):
+    """The reference's own CPU path (oracle/_ref) on the host cores."""
+    from _oracle import Reference
+    if not Reference.available():
+        return None
+    ref = Reference(LEVEL, 2 * math.pi, 32)
+    threads = ref.L.ref_omp_threads()
+    solved, t_total = 0, 0.0
+    while solved < max_solves and t_total < budget_s:
+        t0 = time.perf_counter()
+        ref.bicgs(g, b[solved % len(b)], False, TOL, 300)
+        t_total += time.perf_counter() - t0
+        solved += 1
+    return {"value": solved / t_total, "unit": "solves/s", "cores": threads, "kind": "reference",
+            "sample": f"{solved} forward solves (Tx 0..{solved - 1}) of the same 1024^2 workload, FP64, "
+                      f"{threads} OpenMP threads, {t_total:.1f} s"}
+
+
+def run_reference_arm(args, rank: int, world: int):
+    """--impl reference: the reference's own CPU implementation, rank 0 only."""
+    if rank != 0:
+        return
+    import isg
+    s = isg.Solver(LEVEL, numrx=32, max_rhs=1)
+    g, b = make_inputs(s, 0)
+    from _oracle import Reference
+    if not Reference.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libisgref.so was not built"}))
+        return
+    ref = Reference(LEVEL, 2 * math.pi, 32)
+    threads = ref.L.ref_omp_threads()
+    times = []
+    for k in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        ref.bicgs(g, b[k % NTX], False, TOL, 300)
+        dt = time.perf_counter() - t0
+        if k >= args.warmup:
+            times.append(dt)
+    ms = 1000 * sum(times) / len(times)
+    v = 1000.0 / ms
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+        "config": {**workload_config("reference CPU (solve.cpp + bicgs.cpp, OpenMP)", False), "batch": 1},
+        "cpu_baseline": {"value": v, "unit": "solves/s", "cores": threads, "kind": "reference",
+                         "sample": f"one forward solve per step (Tx k), {threads} threads"},
+        "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--engine", default="auto", choices=["auto", "simt", "tensor"])
+    ap.add_argument("--plain-sample", type=int, default=4, help="single-RHS solves timed for the plain solver")
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+
+    import torch
+    import isg
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    s = isg.Solver(LEVEL, numrx=32, max_rhs=NTX, device=local)
+    s.setup_gpu()
+    g_np, b_np = make_inputs(s, rank)
+    dev = torch.device("cuda", local)
+    g = torch.from_numpy(g_np.astype(np.complex64)).to(dev)
+    b = torch.from_numpy(b_np.astype(np.complex64)).to(dev)
+    x = torch.zeros_like(b)
+    stream = torch.cuda.Stream(dev)
+    engine = {"simt": isg.ENGINE_SIMT, "tensor": isg.ENGINE_TENSOR, "auto": isg.ENGINE_SIMT}[args.engine]
+    opts = isg.default_solve_opts(tol=TOL, maxit=300, engine=engine, check_every=2)
+
+    def step():
+        return s.bicgs(x, g, b, opts=opts, stream=stream)
+
+    for _ in range(args.warmup):
+        infos = step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    launches0 = isg.kernel_launches()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    iters = []
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            infos = step()
+            iters.append([i["iterations"] for i in infos])
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    launches = isg.kernel_launches() - launches0
+    ms = ev0.elapsed_time(ev1) / args.steps
+    if dist:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    bad = [i for i in infos if i["status"] != 0 or not (0 <= i["true_residual"] <= TOL)]
+    value = world * NTX * 1000.0 / ms
+
+    # End to end through the public API from pinned host buffers.
+    b_host = torch.from_numpy(b_np.astype(np.complex64)).pin_memory()
+    g_host = torch.from_numpy(g_np.astype(np.complex64)).pin_memory()
+    x_host = torch.empty_like(b_host).pin_memory()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(max(1, args.steps)):
+            gd = g_host.to(dev, non_blocking=True)
+            bd = b_host.to(dev, non_blocking=True)
+            xd = torch.empty_like(bd)
+            s.bicgs(xd, gd, bd, opts=opts, stream=stream)
+            x_host.copy_(xd, non_blocking=True)
+        e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / max(1, args.steps)
+
+    # Plain single-RHS FP32 solver: one transmitter per launch sequence.
+    plain_opts = isg.default_solve_opts(tol=TOL, maxit=300, engine=isg.ENGINE_SIMT, check_every=1)
+    p_ms, p_iters = [], []
+    for j in range(args.plain_sample + 1):
+        xj = torch.zeros_like(b[j])
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        inf = s.bicgs(xj, g, b[j], opts=plain_opts, stream=stream)[0]
+        a1.record(stream)
+        torch.cuda.synchronize()
+        if j:  # first one is a warm-up
+            p_ms.append(a0.elapsed_time(a1))
+            p_iters.append(inf["iterations"])
+    plain_value = 1000.0 / (sum(p_ms) / len(p_ms))
+
+    # Roofline of the matvec (whole stage sequence) on a 16-RHS batch.
+    st = s.time_stages(nrhs=16, engine=engine, reps=5)
+    pk = peaks()
+    bytes_mv = algorithmic_bytes_per_matvec(s) * 16
+    achieved = bytes_mv / (st["total"] * 1e-3) / 1e9
+
+    out = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c64 (FP64 dots)", "data": "synthetic",
+        "config": {**workload_config("simt" if engine == isg.ENGINE_SIMT else "tensor", False),
+                   "parallelism": f"tx-sharded x{world}" if world > 1 else "single GPU"},
+        "mean_iterations": float(np.mean(iters)), "all_converged": not bad,
+        "max_true_residual": max(i["true_residual"] for i in infos),
+        "roofline": {"bound": "hbm", "kernel": "MLFMA matvec (P2M, M2M, M2L+L2L, L2P+near), 16 RHS",
+                     "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved / pk["hbm_gbs"],
+                     "peak_src": pk["src"], "traffic": None, "stage_ms": st,
+                     "algorithmic_bytes_per_rhs": algorithmic_bytes_per_matvec(s)},
+        "plain": {"value": plain_value, "unit": "solves/s", "solves": len(p_ms),
+                  "mean_iterations": float(np.mean(p_iters)), "ms_per_solve": float(np.mean(p_ms))},
+        "e2e": {"value": world * NTX * 1000.0 / e2e_ms, "unit": "solves/s",
+                "h2d_bytes_per_step": int(b_host.numel() * 8 + g_host.numel() * 8),
+                "d2h_bytes_per_step": int(x_host.numel() * 8)},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_reference_sample(g_np, b_np, args.cpu_budget, 8)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,186 @@
+/* isg.h - C ABI of the B200 MLFMA inverse-scattering solver (libisg.so).
+ *
+ * The library is a drop-in for the reference's MLFMA forward/adjoint solve
+ * path (merthidayetoglu/inverse-solver-GPU): setup_mlfma / setup_gpu /
+ * setup_bicgs, matvec, bicgs, mlfma / mlfmah and aggregate / aggregateh.
+ * The reference exposes these as C++ free functions over globals
+ * (vars.h:14-38, kernels.h:42); each entry point below names the routine it
+ * replaces.  A C++ shim with the reference's exact names and signatures is
+ * declared in isg_refapi.h.
+ *
+ * Conventions
+ *  - Complex vectors are complex64 (interleaved float re, im) in device memory,
+ *    batched right-hand side (RHS) major: RHS j of a vector of U unknowns starts
+ *    at element j*U.  The library never copies caller data to or from the host.
+ *  - `order` selects the unknown ordering of the caller's vectors:
+ *    ISG_ORDER_TREE is the reference's tree order (leaf-major, box*box pixels
+ *    per leaf, row-major inside the leaf; setup_mlfma.cpp:124-175),
+ *    ISG_ORDER_RASTER is the image raster (row 0 at the top; mom.cpp's
+ *    unkmap), ISG_ORDER_BLOCKED is the library's internal layout (leaves in
+ *    raster order, row-major pixels inside a leaf) and costs no reordering.
+ *  - `g` is the scaled contrast k0^2 (eps_r - 1) per pixel (mom.cpp:288-289);
+ *    g_stride is the element distance between the contrasts of consecutive RHS:
+ *    0 shares one contrast across the batch, U gives each RHS its own.
+ *  - Every call is ordered on `stream` (0 = CUDA's legacy default stream).  A
+ *    context is not thread-safe; use one per host thread.
+ *  - Every call returns an isg_status.
+ */
+#ifndef ISG_H
+#define ISG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct isg_ctx isg_ctx;
+typedef void *isg_stream; /* a cudaStream_t */
+
+typedef enum isg_status {
+  ISG_OK = 0,
+  ISG_NOT_CONVERGED = 1, /* iteration cap reached above the tolerance */
+  ISG_BREAKDOWN = 2,     /* BiCGSTAB rho or omega vanished (bicgs.cpp:128,165) */
+  ISG_NONFINITE = 3,     /* a NaN or Inf appeared in a residual */
+  ISG_CUDA_ERROR = 4,
+  ISG_BAD_ARG = 5,
+  ISG_TIMEOUT = 6,
+  ISG_NO_DEVICE = 7,
+  ISG_UNSUPPORTED = 8
+} isg_status;
+
+typedef enum isg_order { ISG_ORDER_TREE = 0, ISG_ORDER_RASTER = 1, ISG_ORDER_BLOCKED = 2 } isg_order;
+
+typedef struct isg_opts {
+  int level;    /* tree levels; the grid is box*2^(level-1) pixels per side (mom.cpp:6,137-138) */
+  int box;      /* leaf side in pixels (mom.cpp:5); 8 */
+  double res;   /* pixel size in wavelengths (mom.cpp:4) */
+  double k0;    /* background wavenumber (mom.cpp:136) */
+  int beta;     /* excess-bandwidth parameter of the sample rule (setup_mlfma.cpp:3) */
+  int ninter;   /* Lagrange interpolation taps (setup_mlfma.cpp:4) */
+  int numrx;    /* far-field receiver angles (mom.cpp:90-91,149-154) */
+  int max_rhs;  /* widest batch one call may pass */
+  int device;   /* CUDA device ordinal */
+} isg_opts;
+
+/* Engines for the dense leaf stages (near field, P2M, L2P). */
+typedef enum isg_engine {
+  ISG_ENGINE_SIMT = 0,  /* complex FP32 CUDA cores: the plain solver */
+  ISG_ENGINE_TENSOR = 1 /* 3xTF32 split products on the tcgen05 tensor cores, FP32 accumulate */
+} isg_engine;
+
+typedef enum isg_guess {
+  ISG_GUESS_ZERO = 0,   /* x0 = 0, as every reference call site (mom.cpp:254,286,324) */
+  ISG_GUESS_CALLER = 1, /* x0 = the caller's x on entry (bicgs.cpp:115) */
+  ISG_GUESS_LEARNED = 2 /* x0 from the loaded neural-operator warm start */
+} isg_guess;
+
+typedef struct isg_solve_opts {
+  double tol;          /* relative residual target (mom.cpp:21 toli) */
+  int maxit;           /* iteration cap per RHS (mom.cpp:22 iti) */
+  int guess;           /* isg_guess */
+  int check_every;     /* iterations between host convergence polls (>= 1) */
+  int true_residual;   /* 1: after convergence recompute b - A x and restart any RHS above tol */
+  int max_restarts;    /* restarts allowed by the true-residual check */
+  int engine;          /* isg_engine */
+} isg_solve_opts;
+
+typedef struct isg_solve_info {
+  int iterations;      /* BiCGSTAB iterations (bicgs.cpp:125) */
+  int matvecs;         /* operator applications */
+  int status;          /* isg_status of this RHS */
+  int restarts;
+  double residual;     /* final recursive ||r|| / ||b|| (bicgs.cpp:160-161) */
+  double true_residual;/* ||b - A x|| / ||b|| recomputed with the operator, or -1 */
+} isg_solve_info;
+
+/* ---- lifecycle: setup_mlfma (setup_mlfma.cpp:50-640) + setup_gpu (gpu.cu:69-260)
+ *      + setup_bicgs (bicgs_gpu.cu:89-113) ---- */
+void isg_default_opts(isg_opts *o);
+void isg_default_solve_opts(isg_solve_opts *o);
+/* Builds the host tables (tree, near/far lists, near-field block, translation,
+ * interpolation, shift and receiver tables).  Touches no GPU. */
+isg_status isg_create(const isg_opts *opts, isg_ctx **out);
+/* Uploads the tables and allocates the device workspaces for max_rhs RHS. */
+isg_status isg_setup_gpu(isg_ctx *ctx);
+void isg_destroy(isg_ctx *ctx);
+const char *isg_status_string(isg_status s);
+const char *isg_last_error(const isg_ctx *ctx);
+
+int isg_numunk(const isg_ctx *ctx);
+int isg_side(const isg_ctx *ctx);
+int isg_numsamp(const isg_ctx *ctx, int lvl);
+int isg_levels(const isg_ctx *ctx);
+/* Host copy of a setup table, for inspection and tests.  Names follow the
+ * reference's globals (setup_mlfma.cpp:6-46): "numsamp", "near", "coeff_multi",
+ * "basis_local", "interp", "anterp", "shiftmul", "shiftloc", "trans", "interph",
+ * "anterph", "pos", "unkmap".  Returns ISG_BAD_ARG for unknown names. */
+isg_status isg_host_table(const isg_ctx *ctx, const char *name, int lvl, const void **data, int64_t *count);
+
+/* Reorders nrhs complex64 vectors between isg_order layouts on the device. */
+isg_status isg_reorder(isg_ctx *ctx, const void *in, void *out, int nrhs, int from, int to, isg_stream stream);
+
+/* ---- operator ---- */
+/* r = G x: mlfma (matvec_gpu.cu:65-79, solve.cpp:25-248); conj != 0 gives
+ * mlfmah, r = conj(G conj(x)) (matvec_gpu.cu:80-101, solve.cpp:8-24). */
+isg_status isg_mlfma(isg_ctx *ctx, const void *x, void *r, int nrhs, int conj, int order, int engine,
+                     isg_stream stream);
+/* y = x - G(g x), or y = x - conj(g G(conj x)) when hermitian (matvec,
+ * bicgs_gpu.cu:61-76; bicgs.cpp:62-87). */
+isg_status isg_matvec(isg_ctx *ctx, const void *x, const void *g, int64_t g_stride, void *y, int nrhs, int hermitian,
+                      int order, int engine, isg_stream stream);
+
+/* ---- solver ---- */
+/* BiCGSTAB on (I - G diag(g)) x = b or its adjoint for nrhs right-hand sides at
+ * once, each with its own convergence mask (bicgs, bicgs_gpu.cu:116-224;
+ * bicgs.cpp:88-179).  x is the solution (and the initial guess with
+ * ISG_GUESS_CALLER).  info receives nrhs records (may be NULL).  Returns
+ * ISG_OK when every RHS reached tol, else the worst per-RHS status. */
+isg_status isg_bicgs(isg_ctx *ctx, void *x, const void *g, int64_t g_stride, const void *b, int nrhs, int hermitian,
+                     int order, const isg_solve_opts *opts, isg_solve_info *info, isg_stream stream);
+
+/* ---- receivers ---- */
+/* rx[numrx] = far-field pattern of x (aggregate, matvec_gpu.cu:266-368;
+ * solve.cpp:249-355), all levels on the device. */
+isg_status isg_aggregate(isg_ctx *ctx, const void *x, void *rx, int nrhs, int order, isg_stream stream);
+/* x[U] = back-projection of rx (aggregateh, matvec_gpu.cu:369-470;
+ * solve.cpp:356-456), all levels on the device. */
+isg_status isg_aggregateh(isg_ctx *ctx, void *x, const void *rx, int nrhs, int order, isg_stream stream);
+
+/* ---- measurement ---- */
+/* Number of CUDA kernels this library has launched in the process so far. */
+int64_t isg_kernel_launches(void);
+/* Runs the forward matvec `reps` times on nrhs internal test vectors and writes
+ * the mean device time in ms of each stage: [0] P2M, [1] M2M (all levels),
+ * [2] M2L+L2L (all levels), [3] L2P+near field, [4] whole matvec. */
+isg_status isg_time_stages(isg_ctx *ctx, int nrhs, int engine, int reps, double *ms_out);
+
+/* ---- seeded synthetic inputs (the reference reads a phantom file instead,
+ *      setup_born.cpp:103-113) ---- */
+typedef struct isg_phantom {
+  int kind;            /* 0: random ellipses, 1: Gaussian random field */
+  int count;           /* ellipses */
+  double axis_min;     /* semi-axis range in wavelengths */
+  double axis_max;
+  double eps_min;      /* relative permittivity range (real part) */
+  double eps_max;
+  double tand_max;     /* loss tangent drawn from [0, tand_max] per ellipse */
+  double corr_len;     /* Gaussian random field correlation length (wavelengths) */
+  uint64_t seed;
+} isg_phantom;
+/* Writes the contrast chi = eps_r - 1 (complex128, raster order, side*side). */
+isg_status isg_make_phantom(const isg_ctx *ctx, const isg_phantom *ph, double *chi_raster);
+/* Plane waves exp(i k0 d.r) of transmitters first .. first+count-1 out of ntx
+ * directions at angle 2 pi j / ntx (setup_born.cpp:62-65, mom.cpp:141-147),
+ * count rows of complex128 in the given order. */
+isg_status isg_make_plane_waves(const isg_ctx *ctx, int ntx, int first, int count, int order, double *inc);
+/* Line sources integrate(r_tx, r)/res^2 at ntx points on a circle of the given
+ * radius (the reference's near-field form, setup_born.cpp:66-72); rows as above. */
+isg_status isg_make_line_sources(const isg_ctx *ctx, int ntx, int first, int count, double radius, int order,
+                                 double *inc);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

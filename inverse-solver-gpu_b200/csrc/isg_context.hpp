@@ -1,0 +1,67 @@
+// The opaque isg_ctx behind the C ABI: host tables, device plan, workspaces.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "../../include/isg.h"
+#include "isg_device.cuh"
+#include "isg_tables.hpp"
+
+namespace isg {
+
+// Per-RHS BiCGSTAB scalars, kept on the device (FP64, bicgs.cpp:100-110).
+struct RhsState {
+  double bn;          // ||b|| (1 when ||b|| < 1e-20, bicgs.cpp:111-113)
+  double err;         // recursive ||r|| / ||b||
+  double tres;        // true residual after the final check, -1 if not computed
+  double rho[2];      // current <r~, r>
+  double rho1[2];     // previous rho
+  double alpha[2];
+  double omega[2];
+  int iter, matvecs, status, active, fresh, restarts;
+};
+
+struct TcPlan;  // tensor-core leaf stage tables (isg_tc.cu)
+
+}  // namespace isg
+
+struct isg_ctx {
+  isg_opts opts{};
+  isg::HostTables T;
+  isg::DevPlan P;
+  bool gpu_ready = false;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  std::vector<void *> dev_allocs;
+
+  // workspaces sized for opts.max_rhs
+  float2 *mul = nullptr, *loc = nullptr;  // [R][P.mp]
+  float2 *wx = nullptr, *wy = nullptr;    // [R][U] reorder scratch
+  float2 *wg = nullptr;                   // [R][U] contrast in blocked order
+  float2 *vr = nullptr, *vrt = nullptr, *vp = nullptr, *vv = nullptr, *vs = nullptr, *vt = nullptr;
+  double *part = nullptr;  // [R][part_blocks][4]
+  int part_blocks = 0;
+  isg::RhsState *state = nullptr;  // [R]
+  int *active = nullptr;           // [R]
+  int *count = nullptr;            // active-RHS counter
+  int *h_count = nullptr;          // pinned host mirror
+  int vec_blocks = 0;
+  isg::TcPlan *tc = nullptr;
+};
+
+namespace isg {
+// Internal operator entry points shared by the C ABI and the solver.
+enum OpKind { OP_G = 0, OP_GCONJ = 1, OP_FWD = 2, OP_ADJ = 3 };
+isg_status run_matvec(isg_ctx *c, const float2 *x, const float2 *g, int64_t gs, float2 *y, int nrhs, int kind,
+                      int engine, int red, const float2 *dot_a, const int *active, cudaStream_t st);
+isg_status run_bicgs(isg_ctx *c, float2 *x, const float2 *g, int64_t gs, const float2 *b, int nrhs, int hermitian,
+                     const isg_solve_opts *o, isg_solve_info *info, cudaStream_t st);
+isg_status cuda_check(isg_ctx *c, cudaError_t e, const char *what);
+// Tensor-core engine (isg_tc.cu).
+isg_status tc_setup(isg_ctx *c);
+void tc_destroy(isg_ctx *c);
+bool tc_available(const isg_ctx *c);
+isg_status tc_p2m(isg_ctx *c, const BatchArgs &B, float2 *mul, cudaStream_t st);
+isg_status tc_near(isg_ctx *c, const NearArgs &A, cudaStream_t st);
+}  // namespace isg

@@ -1,0 +1,444 @@
+// Batched BiCGSTAB (bicgs_gpu.cu:116-224, bicgs.cpp:88-179) with every scalar
+// kept on the device in FP64, per-RHS convergence masks, and the dot products
+// fused into the producing kernels.  The host only polls an active-RHS counter
+// every `check_every` iterations.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "isg_context.hpp"
+
+namespace isg {
+
+namespace {
+
+__device__ __forceinline__ bool inactive(const int *active, int rhs) { return active && !active[rhs]; }
+
+__device__ __forceinline__ double2 cdiv(double2 a, double2 b) {
+  const double d = b.x * b.x + b.y * b.y;
+  return make_double2((a.x * b.x + a.y * b.y) / d, (a.y * b.x - a.x * b.y) / d);
+}
+__device__ __forceinline__ double2 dmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 f2(double2 a) { return make_float2((float)a.x, (float)a.y); }
+__device__ __forceinline__ double2 ld2(const double *p) { return make_double2(p[0], p[1]); }
+__device__ __forceinline__ void st2(double *p, double2 v) {
+  p[0] = v.x;
+  p[1] = v.y;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Sums up to three partials per thread over a 256-thread block into s[0..2]
+// in a fixed order; thread 0 gets the block totals.
+__device__ void block_sum3(double a, double b, double c, double *out) {
+  __shared__ double ws[8][3];
+  a = warp_sum(a);
+  b = warp_sum(b);
+  c = warp_sum(c);
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    ws[w][0] = a;
+    ws[w][1] = b;
+    ws[w][2] = c;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s0 = 0, s1 = 0, s2 = 0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); q++) {
+      s0 += ws[q][0];
+      s1 += ws[q][1];
+      s2 += ws[q][2];
+    }
+    out[0] = s0;
+    out[1] = s1;
+    out[2] = s2;
+  }
+  __syncthreads();
+}
+
+// Per-RHS total of `nb` block partials (4 doubles each), deterministic.
+__device__ void sum_partials(const double *part, int rhs, int nb, double *tot) {
+  double a = 0, b = 0, c = 0;
+  const double *p = part + (size_t)rhs * nb * 4;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+    a += p[i * 4 + 0];
+    b += p[i * 4 + 1];
+    c += p[i * 4 + 2];
+  }
+  __shared__ double t[3];
+  block_sum3(a, b, c, t);
+  tot[0] = t[0];
+  tot[1] = t[1];
+  tot[2] = t[2];
+}
+
+__device__ void write_part(double *part, int rhs, int nb, double a, double b, double c) {
+  __shared__ double t[3];
+  block_sum3(a, b, c, t);
+  if (threadIdx.x == 0) {
+    double *p = part + ((size_t)rhs * nb + blockIdx.x) * 4;
+    p[0] = t[0];
+    p[1] = t[1];
+    p[2] = t[2];
+    p[3] = 0;
+  }
+}
+
+// Initial residual: r = b (zero guess) or r = b - Ax (Ax in t); r~ = r.
+// Partials: ||b||^2, ||r||^2.
+__global__ void __launch_bounds__(256) k_init(const float2 *__restrict__ b, const float2 *__restrict__ t,
+                                              float2 *__restrict__ x, float2 *__restrict__ r, float2 *__restrict__ rt,
+                                              int U, int zero_guess, double *part) {
+  const int rhs = blockIdx.y;
+  const size_t base = (size_t)rhs * U;
+  double bb = 0, rr = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < U; i += gridDim.x * blockDim.x) {
+    const float2 bv = b[base + i];
+    float2 rv = bv;
+    if (zero_guess)
+      x[base + i] = make_float2(0.f, 0.f);
+    else
+      rv = csub(bv, t[base + i]);
+    r[base + i] = rv;
+    rt[base + i] = rv;
+    bb += (double)bv.x * bv.x + (double)bv.y * bv.y;
+    rr += (double)rv.x * rv.x + (double)rv.y * rv.y;
+  }
+  write_part(part, rhs, gridDim.x, bb, rr, 0);
+}
+
+__global__ void __launch_bounds__(256) k_fin_init(RhsState *st, int *active, int *count, const double *part, int nb,
+                                                  int zero_guess, double tol) {
+  const int rhs = blockIdx.x;
+  double tot[3];
+  sum_partials(part, rhs, nb, tot);
+  if (threadIdx.x) return;
+  RhsState &s = st[rhs];
+  double bn = sqrt(tot[0]);
+  if (bn < 1e-20) bn = 1;
+  s.bn = bn;
+  s.err = sqrt(tot[1]) / bn;
+  s.tres = -1;
+  s.rho[0] = tot[1];
+  s.rho[1] = 0;
+  s.rho1[0] = s.rho1[1] = 0;
+  s.alpha[0] = s.alpha[1] = 0;
+  s.omega[0] = s.omega[1] = 0;
+  s.iter = 0;
+  s.matvecs = zero_guess ? 0 : 1;
+  s.fresh = 1;
+  s.restarts = 0;
+  if (!isfinite(s.err)) {
+    s.status = ISG_NONFINITE;
+    s.active = 0;
+  } else if (s.err > tol) {
+    s.status = ISG_NOT_CONVERGED;
+    s.active = 1;
+  } else {
+    s.status = ISG_OK;
+    s.active = 0;
+  }
+  active[rhs] = s.active;
+  if (s.active) atomicAdd(count, 1);
+}
+
+// p = r (first iteration) or p = r + beta (p - omega v), beta = (rho/rho1)(alpha/omega)
+// (bicgs.cpp:132-139).
+__global__ void __launch_bounds__(256) k_update_p(const RhsState *st, const int *active, const float2 *__restrict__ r,
+                                                  float2 *__restrict__ p, const float2 *__restrict__ v, int U) {
+  const int rhs = blockIdx.y;
+  if (inactive(active, rhs)) return;
+  const RhsState &s = st[rhs];
+  const size_t base = (size_t)rhs * U;
+  if (s.fresh) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < U; i += gridDim.x * blockDim.x) p[base + i] = r[base + i];
+    return;
+  }
+  const double2 beta = dmul(cdiv(ld2(s.rho), ld2(s.rho1)), cdiv(ld2(s.alpha), ld2(s.omega)));
+  const float2 bf = f2(beta), of = f2(ld2(s.omega));
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < U; i += gridDim.x * blockDim.x) {
+    const float2 pv = p[base + i], vv = v[base + i];
+    p[base + i] = cadd(r[base + i], cmul(bf, csub(pv, cmul(of, vv))));
+  }
+}
+
+// alpha = rho / <r~, v> (bicgs.cpp:145).
+__global__ void __launch_bounds__(256) k_fin_alpha(RhsState *st, int *active, const double *part, int nb) {
+  const int rhs = blockIdx.x;
+  if (!active[rhs]) return;
+  double tot[3];
+  sum_partials(part, rhs, nb, tot);
+  if (threadIdx.x) return;
+  RhsState &s = st[rhs];
+  const double2 a = cdiv(ld2(s.rho), make_double2(tot[0], tot[1]));
+  st2(s.alpha, a);
+  s.matvecs++;
+  s.fresh = 0;
+  if (!isfinite(a.x) || !isfinite(a.y)) {
+    s.status = ISG_NONFINITE;
+    s.active = 0;
+    active[rhs] = 0;
+  }
+}
+
+// s = r - alpha v (bicgs.cpp:146).
+__global__ void __launch_bounds__(256) k_update_s(const RhsState *st, const int *active, const float2 *__restrict__ r,
+                                                  const float2 *__restrict__ v, float2 *__restrict__ s, int U) {
+  const int rhs = blockIdx.y;
+  if (inactive(active, rhs)) return;
+  const float2 a = f2(ld2(st[rhs].alpha));
+  const size_t base = (size_t)rhs * U;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < U; i += gridDim.x * blockDim.x)
+    s[base + i] = csub(r[base + i], cmul(a, v[base + i]));
+}
+
+// omega = <t, s> / ||t||^2 (bicgs.cpp:153); zero when t vanishes, which only
+// happens when s itself is zero (bicgs_gpu.cu:376 guards the same case).
+__global__ void __launch_bounds__(256) k_fin_omega(RhsState *st, const int *active, const double *part, int nb) {
+  const int rhs = blockIdx.x;
+  if (!active[rhs]) return;
+  double tot[3];
+  sum_partials(part, rhs, nb, tot);
+  if (threadIdx.x) return;
+  RhsState &s = st[rhs];
+  s.matvecs++;
+  if (tot[2] > 0) {
+    s.omega[0] = tot[0] / tot[2];
+    s.omega[1] = tot[1] / tot[2];
+  } else {
+    s.omega[0] = s.omega[1] = 0;
+  }
+}
+
+// x += alpha p + omega s; r = s - omega t (bicgs.cpp:155-159); partials
+// ||r||^2 and <r~, r> for the convergence test and the next rho.
+__global__ void __launch_bounds__(256) k_update_xr(const RhsState *st, const int *active, float2 *__restrict__ x,
+                                                   float2 *__restrict__ r, const float2 *__restrict__ rt,
+                                                   const float2 *__restrict__ p, const float2 *__restrict__ s,
+                                                   const float2 *__restrict__ t, int U, double *part) {
+  const int rhs = blockIdx.y;
+  if (inactive(active, rhs)) return;
+  const float2 a = f2(ld2(st[rhs].alpha)), o = f2(ld2(st[rhs].omega));
+  const size_t base = (size_t)rhs * U;
+  double rr = 0, dr = 0, di = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < U; i += gridDim.x * blockDim.x) {
+    const float2 sv = s[base + i];
+    x[base + i] = cadd(x[base + i], cadd(cmul(a, p[base + i]), cmul(o, sv)));
+    const float2 rv = csub(sv, cmul(o, t[base + i]));
+    r[base + i] = rv;
+    const float2 q = rt[base + i];
+    rr += (double)rv.x * rv.x + (double)rv.y * rv.y;
+    dr += (double)q.x * rv.x + (double)q.y * rv.y;
+    di += (double)q.x * rv.y - (double)q.y * rv.x;
+  }
+  write_part(part, rhs, gridDim.x, rr, dr, di);
+}
+
+// Convergence and breakdown tests of one iteration (bicgs.cpp:160-169, 127-131).
+__global__ void __launch_bounds__(256) k_fin_iter(RhsState *st, int *active, int *count, const double *part, int nb,
+                                                  double tol, int maxit) {
+  const int rhs = blockIdx.x;
+  if (!active[rhs]) return;
+  double tot[3];
+  sum_partials(part, rhs, nb, tot);
+  if (threadIdx.x) return;
+  RhsState &s = st[rhs];
+  s.iter++;
+  s.err = sqrt(tot[0]) / s.bn;
+  const double om = hypot(s.omega[0], s.omega[1]);
+  const double rho_new = hypot(tot[1], tot[2]);
+  int stop = 0;
+  if (!isfinite(s.err)) {
+    s.status = ISG_NONFINITE;
+    stop = 1;
+  } else if (s.err < tol) {
+    s.status = ISG_OK;
+    stop = 1;
+  } else if (om < 1e-20) {
+    s.status = ISG_BREAKDOWN;
+    stop = 1;
+  } else if (s.iter >= maxit) {
+    s.status = ISG_NOT_CONVERGED;
+    stop = 1;
+  } else if (rho_new < 1e-20) {
+    s.status = ISG_BREAKDOWN;
+    stop = 1;
+  }
+  s.rho1[0] = s.rho[0];
+  s.rho1[1] = s.rho[1];
+  s.rho[0] = tot[1];
+  s.rho[1] = tot[2];
+  if (stop) {
+    s.active = 0;
+    active[rhs] = 0;
+  } else {
+    atomicAdd(count, 1);
+  }
+}
+
+// True residual b - A x (A x in t) into r and r~, partial ||.||^2.
+__global__ void __launch_bounds__(256) k_true_res(const float2 *__restrict__ b, const float2 *__restrict__ t,
+                                                  float2 *__restrict__ r, float2 *__restrict__ rt, int U,
+                                                  double *part) {
+  const int rhs = blockIdx.y;
+  const size_t base = (size_t)rhs * U;
+  double rr = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < U; i += gridDim.x * blockDim.x) {
+    const float2 rv = csub(b[base + i], t[base + i]);
+    r[base + i] = rv;
+    rt[base + i] = rv;
+    rr += (double)rv.x * rv.x + (double)rv.y * rv.y;
+  }
+  write_part(part, rhs, gridDim.x, rr, 0, 0);
+}
+
+// Records the true residual and restarts (r = r~ = b - Ax, p = r) every RHS
+// that stopped on the recursive residual but misses tol on the true one.
+__global__ void __launch_bounds__(256) k_fin_true(RhsState *st, int *active, int *count, const double *part, int nb,
+                                                  double tol, int max_restarts, int maxit) {
+  const int rhs = blockIdx.x;
+  double tot[3];
+  sum_partials(part, rhs, nb, tot);
+  if (threadIdx.x) return;
+  RhsState &s = st[rhs];
+  s.matvecs++;
+  s.tres = sqrt(tot[0]) / s.bn;
+  if (s.status == ISG_OK && !(s.tres <= tol) && s.restarts < max_restarts && s.iter < maxit) {
+    s.restarts++;
+    s.status = ISG_NOT_CONVERGED;
+    s.active = 1;
+    s.fresh = 1;
+    s.rho[0] = tot[0];
+    s.rho[1] = 0;
+    s.err = s.tres;
+    active[rhs] = 1;
+    atomicAdd(count, 1);
+  }
+}
+
+}  // namespace
+
+isg_status run_matvec(isg_ctx *c, const float2 *x, const float2 *g, int64_t gs, float2 *y, int nrhs, int kind,
+                      int engine, int red, const float2 *dot_a, const int *active, cudaStream_t st) {
+  const DevPlan &P = c->P;
+  BatchArgs B;
+  B.x = x;
+  B.g = g;
+  B.gstride = gs;
+  B.nrhs = nrhs;
+  B.active = active;
+  B.mode = (kind == OP_FWD) ? IN_G : (kind == OP_G ? IN_PLAIN : IN_CONJ);
+  const bool tc = (engine == ISG_ENGINE_TENSOR) && tc_available(c);
+  if (engine == ISG_ENGINE_TENSOR && !tc) return ISG_UNSUPPORTED;
+  if (tc) {
+    isg_status e = tc_p2m(c, B, c->mul, st);
+    if (e != ISG_OK) return e;
+  } else {
+    launch_p2m(P, B, c->mul, st);
+  }
+  for (int i = P.L - 2; i >= 2; i--) launch_m2m(P, i, c->mul, nrhs, active, st);
+  for (int i = 2; i < P.L; i++) launch_m2l_l2l(P, i, c->mul, c->loc, nrhs, active, true, i > 2, st);
+  NearArgs A;
+  A.in = B;
+  A.loc = c->loc;
+  A.y = y;
+  A.epi = (kind == OP_FWD) ? EPI_FWD : (kind == OP_ADJ ? EPI_ADJ : (kind == OP_GCONJ ? EPI_CONJ : EPI_G));
+  A.red = red;
+  A.dot_a = dot_a;
+  A.part = c->part;
+  if (tc) return tc_near(c, A, st);
+  launch_near(P, A, st);
+  return cuda_check(c, cudaGetLastError(), "matvec launch");
+}
+
+isg_status run_bicgs(isg_ctx *c, float2 *x, const float2 *g, int64_t gs, const float2 *b, int R, int hermitian,
+                     const isg_solve_opts *o, isg_solve_info *info, cudaStream_t st) {
+  const int U = c->P.U;
+  const int kind = hermitian ? OP_ADJ : OP_FWD;
+  const int nbv = c->vec_blocks;
+  const int nbn = near_blocks_per_rhs(c->P);
+  const double tol = o->tol;
+  const int engine = o->engine;
+  const int zero_guess = (o->guess == ISG_GUESS_ZERO);
+  isg_status e;
+  dim3 vgrid(nbv, R);
+
+  if (!zero_guess) {
+    e = run_matvec(c, x, g, gs, c->vt, R, kind, engine, RED_NONE, nullptr, nullptr, st);
+    if (e != ISG_OK) return e;
+  }
+  count_launch();
+  k_init<<<vgrid, 256, 0, st>>>(b, c->vt, x, c->vr, c->vrt, U, zero_guess, c->part);
+  cudaMemsetAsync(c->count, 0, sizeof(int), st);
+  count_launch();
+  k_fin_init<<<R, 256, 0, st>>>(c->state, c->active, c->count, c->part, nbv, zero_guess, tol);
+  if ((e = cuda_check(c, cudaGetLastError(), "bicgs init")) != ISG_OK) return e;
+
+  const int check = std::max(1, o->check_every);
+  const long host_cap = (long)(o->maxit + 2) * (o->max_restarts + 1) + 8;
+  long host_iters = 0;
+  for (;;) {
+    cudaMemcpyAsync(c->h_count, c->count, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if ((e = cuda_check(c, cudaStreamSynchronize(st), "bicgs poll")) != ISG_OK) return e;
+    if (*c->h_count > 0 && host_iters < host_cap) {
+      for (int k = 0; k < check; k++, host_iters++) {
+        count_launch();
+        k_update_p<<<vgrid, 256, 0, st>>>(c->state, c->active, c->vr, c->vp, c->vv, U);
+        e = run_matvec(c, c->vp, g, gs, c->vv, R, kind, engine, RED_DOT, c->vrt, c->active, st);
+        if (e != ISG_OK) return e;
+        count_launch();
+        k_fin_alpha<<<R, 256, 0, st>>>(c->state, c->active, c->part, nbn);
+        count_launch();
+        k_update_s<<<vgrid, 256, 0, st>>>(c->state, c->active, c->vr, c->vv, c->vs, U);
+        e = run_matvec(c, c->vs, g, gs, c->vt, R, kind, engine, RED_TS, nullptr, c->active, st);
+        if (e != ISG_OK) return e;
+        count_launch();
+        k_fin_omega<<<R, 256, 0, st>>>(c->state, c->active, c->part, nbn);
+        count_launch();
+        k_update_xr<<<vgrid, 256, 0, st>>>(c->state, c->active, x, c->vr, c->vrt, c->vp, c->vs, c->vt, U, c->part);
+        cudaMemsetAsync(c->count, 0, sizeof(int), st);
+        count_launch();
+        k_fin_iter<<<R, 256, 0, st>>>(c->state, c->active, c->count, c->part, nbv, tol, o->maxit);
+      }
+      if ((e = cuda_check(c, cudaGetLastError(), "bicgs iteration")) != ISG_OK) return e;
+      continue;
+    }
+    if (!o->true_residual) break;
+    // True residual of every RHS; restarts any that stopped early.
+    e = run_matvec(c, x, g, gs, c->vt, R, kind, engine, RED_NONE, nullptr, nullptr, st);
+    if (e != ISG_OK) return e;
+    count_launch();
+    k_true_res<<<vgrid, 256, 0, st>>>(b, c->vt, c->vr, c->vrt, U, c->part);
+    cudaMemsetAsync(c->count, 0, sizeof(int), st);
+    count_launch();
+    k_fin_true<<<R, 256, 0, st>>>(c->state, c->active, c->count, c->part, nbv, tol, o->max_restarts, o->maxit);
+    cudaMemcpyAsync(c->h_count, c->count, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if ((e = cuda_check(c, cudaStreamSynchronize(st), "bicgs true residual")) != ISG_OK) return e;
+    if (*c->h_count == 0 || host_iters >= host_cap) break;
+  }
+
+  std::vector<RhsState> hs(R);
+  cudaMemcpyAsync(hs.data(), c->state, R * sizeof(RhsState), cudaMemcpyDeviceToHost, st);
+  if ((e = cuda_check(c, cudaStreamSynchronize(st), "bicgs results")) != ISG_OK) return e;
+  isg_status worst = ISG_OK;
+  for (int r = 0; r < R; r++) {
+    if (info) {
+      info[r].iterations = hs[r].iter;
+      info[r].matvecs = hs[r].matvecs;
+      info[r].status = hs[r].status;
+      info[r].restarts = hs[r].restarts;
+      info[r].residual = hs[r].err;
+      info[r].true_residual = hs[r].tres;
+    }
+    if (hs[r].status != ISG_OK && (worst == ISG_OK || hs[r].status > worst)) worst = (isg_status)hs[r].status;
+  }
+  return worst;
+}
+
+}  // namespace isg

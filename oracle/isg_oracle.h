@@ -1,0 +1,60 @@
+/* Restated FP64 oracle of the reference's MLFMA forward/adjoint solve path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and the CPU
+ * baseline leg of bench.py load this library, and only as the checker.  It is
+ * pinned against the reference's own CPU path (oracle/_ref, built by
+ * oracle/Makefile from the reference sources) by tests/test_oracle_pin.py and
+ * against the committed fixtures under tests/golden/.
+ *
+ * Complex arrays are C99 double complex (interleaved re, im) in the
+ * reference's tree order: leaf-major, box*box pixels per leaf, row-major
+ * inside the leaf (setup_mlfma.cpp:124-175).
+ */
+#ifndef ISG_ORACLE_H
+#define ISG_ORACLE_H
+
+#include <complex.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct orc_ctx orc_ctx;
+
+/* setup_mlfma.cpp:50-640 and setup_interp (:642-695). */
+orc_ctx *orc_create(int level, double k0, double res, int box, int beta, int ninter, int numrx);
+void orc_destroy(orc_ctx *c);
+
+int orc_numunk(const orc_ctx *c);
+int orc_numsamp(const orc_ctx *c, int lvl);
+const void *orc_table(const orc_ctx *c, const char *name, int lvl);
+
+/* integrate.cpp:15-41: one dense MoM entry (i/4) res^2 H0(k0|t-b|) with the
+ * analytic self term. */
+double complex orc_integrate(const orc_ctx *c, double complex post, double complex posb);
+
+/* r = G x through the MLFMA (solve.cpp:25-248) and its conjugate form
+ * (solve.cpp:8-24). */
+void orc_mlfma(orc_ctx *c, const double complex *x, double complex *r);
+void orc_mlfmah(orc_ctx *c, const double complex *x, double complex *r);
+
+/* r = G x with every entry from orc_integrate; O(U^2), small grids only. */
+void orc_dense_matvec(const orc_ctx *c, const double complex *x, double complex *r);
+
+/* bicgs.cpp:62-87: y = x - G(g x), or y = x - conj(g G(conj x)) when hermitian. */
+void orc_matvec(orc_ctx *c, const double complex *x, const double complex *g, double complex *y, int hermitian);
+
+/* bicgs.cpp:88-179 BiCGSTAB from the caller's x; returns the iteration count
+ * and writes the final recursive relative residual to *err. */
+int orc_bicgs(orc_ctx *c, double complex *x, const double complex *g, const double complex *b, int hermitian,
+              double tol, int maxit, double *err);
+
+/* solve.cpp:249-355 receiver projection (numrx far-field samples) and
+ * solve.cpp:356-456 its back-projection onto the pixels. */
+void orc_aggregate(orc_ctx *c, const double complex *x, double complex *rx);
+void orc_aggregateh(orc_ctx *c, double complex *x, const double complex *rx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
