@@ -182,6 +182,8 @@ def main():
     ap.add_argument("--plain-sample", type=int, default=4, help="single-RHS solves timed for the plain solver")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--stages-only", type=int, default=0,
+                    help="only time the matvec stages on this many RHS of the workload (profiling case)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -200,6 +202,16 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
+    if args.stages_only:
+        s = isg.Solver(LEVEL, numrx=32, max_rhs=args.stages_only, device=local)
+        for eng in ([isg.ENGINE_SIMT, isg.ENGINE_TENSOR] if args.engine == "auto" else
+                    [isg.ENGINE_SIMT if args.engine == "simt" else isg.ENGINE_TENSOR]):
+            try:
+                print(json.dumps({"engine": eng, "nrhs": args.stages_only,
+                                  "stage_ms": s.time_stages(args.stages_only, eng, reps=3)}))
+            except isg.IsgError as e:
+                print(json.dumps({"engine": eng, "error": str(e)}))
+        return
     s = isg.Solver(LEVEL, numrx=32, max_rhs=NTX, device=local)
     s.setup_gpu()
     g_np, b_np = make_inputs(s, rank)

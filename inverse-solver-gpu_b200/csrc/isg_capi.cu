@@ -434,7 +434,7 @@ isg_status isg_aggregateh(isg_ctx *c, void *x, const void *rx, int nrhs, int ord
   cudaStream_t st = pick(c, stream);
   const float scale = (float)(-4.0 * c->T.numrx * c->T.res * c->T.res);
   launch_rx_anterp(c->P, (const float2 *)rx, c->loc, nrhs, make_float2(0.f, scale), st);
-  for (int i = 1; i < c->P.L; i++) launch_m2l_l2l(c->P, i, c->mul, c->loc, nrhs, nullptr, false, true, st);
+  for (int i = 1; i < c->P.L; i++) launch_l2l(c->P, i, c->loc, nrhs, nullptr, false, st);
   NearArgs A;
   A.in.nrhs = nrhs;
   A.loc = c->loc;
@@ -480,7 +480,8 @@ isg_status isg_time_stages(isg_ctx *c, int nrhs, int engine, int reps, double *m
     cudaEventRecord(ev[1], st);
     for (int i = P.L - 2; i >= 2; i--) launch_m2m(P, i, c->mul, nrhs, nullptr, st);
     cudaEventRecord(ev[2], st);
-    for (int i = 2; i < P.L; i++) launch_m2l_l2l(P, i, c->mul, c->loc, nrhs, nullptr, true, i > 2, st);
+    for (int i = 2; i < P.L; i++) launch_m2l(P, i, c->mul, c->loc, nrhs, nullptr, st);
+    for (int i = 3; i < P.L; i++) launch_l2l(P, i, c->loc, nrhs, nullptr, true, st);
     cudaEventRecord(ev[3], st);
     if (tc) tc_near(c, A, st); else launch_near(P, A, st);
     cudaEventRecord(ev[4], st);

@@ -98,8 +98,12 @@ int64_t launch_count();
 // ---- launchers (isg_kernels.cu) ----
 void launch_p2m(const DevPlan &P, const BatchArgs &B, float2 *mul, cudaStream_t st);
 void launch_m2m(const DevPlan &P, int lvl, float2 *mul, int nrhs, const int *active, cudaStream_t st);
-void launch_m2l_l2l(const DevPlan &P, int lvl, const float2 *mul, float2 *loc, int nrhs, const int *active,
-                    bool do_m2l, bool do_l2l, cudaStream_t st);
+// M2L into level lvl (overwrites its local expansions).
+void launch_m2l(const DevPlan &P, int lvl, const float2 *mul, float2 *loc, int nrhs, const int *active,
+                cudaStream_t st);
+// L2L from level lvl-1 into level lvl, added to or written over its locals.
+void launch_l2l(const DevPlan &P, int lvl, float2 *loc, int nrhs, const int *active, bool accumulate,
+                cudaStream_t st);
 // y = epilogue(L2P(loc_leaf) + near(x)); optional FP64 partials per block.
 struct NearArgs {
   BatchArgs in;

@@ -60,77 +60,176 @@ __global__ void __launch_bounds__(128) k_p2m(const float2 *__restrict__ x, const
   }
 }
 
+constexpr int kSmemStage = 200 * 1024;  // largest ring staged in shared memory
+
 // M2M (kernels.cu:83-136, solve.cpp:93-112): parent sample km gathers the
-// 30-tap interpolation of each child, shifts it to the parent centre and sums.
+// 30-tap interpolation of each of its four children, shifts it to the parent
+// centre and sums.  The four children's rings are staged in shared memory
+// (STAGE) or read through L1 when they are too large (top levels only).
+template <bool STAGE>
 __global__ void __launch_bounds__(128) k_m2m(float2 *__restrict__ mul, size_t mp, size_t off_p, size_t off_c, int n_p,
-                                             int ns_p, int ns_c, const int *__restrict__ ifirst,
+                                             int ns_p, int ns_c, int nchunk, const int *__restrict__ ifirst,
                                              const float *__restrict__ iw, const float2 *__restrict__ shm,
                                              int ninter, const int *__restrict__ active) {
-  const int rhs = blockIdx.z;
+  extern __shared__ float2 chs[];
+  const int rhs = blockIdx.y;
   if (inactive(active, rhs)) return;
-  const int km = blockIdx.x * blockDim.x + threadIdx.x;
-  if (km >= ns_p) return;
-  const int pc = blockIdx.y, py = pc / n_p, px = pc % n_p, n_c = 2 * n_p;
+  const int pc = blockIdx.x / nchunk, chunk = blockIdx.x % nchunk;
+  const int py = pc / n_p, px = pc % n_p, n_c = 2 * n_p;
   const float2 *base = mul + (size_t)rhs * mp + off_c;
-  const int f = ifirst[km];
+  if (STAGE) {
+    for (int e = threadIdx.x; e < 4 * ns_c; e += blockDim.x) {
+      const int q = e / ns_c;
+      chs[e] = base[(size_t)((2 * py + (q >> 1)) * n_c + 2 * px + (q & 1)) * ns_c + e % ns_c];
+    }
+    __syncthreads();
+  }
+  size_t coff[4];
+#pragma unroll
+  for (int q = 0; q < 4; q++) coff[q] = (size_t)((2 * py + (q >> 1)) * n_c + 2 * px + (q & 1)) * ns_c;
+  const int km = chunk * blockDim.x + threadIdx.x;
+  if (km >= ns_p) return;
+  int idx = ifirst[km];
+  float2 acc[4] = {};
+  for (int t = 0; t < ninter; t++) {
+    const float w = __ldg(&iw[t * ns_p + km]);
+#pragma unroll
+    for (int q = 0; q < 4; q++) rfma(acc[q], w, STAGE ? chs[q * ns_c + idx] : base[coff[q] + idx]);
+    if (++idx == ns_c) idx = 0;
+  }
   float2 res = make_float2(0.f, 0.f);
 #pragma unroll
-  for (int q = 0; q < 4; q++) {
-    const float2 *ch = base + (size_t)((2 * py + (q >> 1)) * n_c + 2 * px + (q & 1)) * ns_c;
-    float2 acc = make_float2(0.f, 0.f);
-    int idx = f;
-    for (int t = 0; t < ninter; t++) {
-      rfma(acc, __ldg(&iw[t * ns_p + km]), ch[idx]);
-      if (++idx == ns_c) idx = 0;
-    }
-    cfma(res, __ldg(&shm[q * ns_p + km]), acc);
-  }
+  for (int q = 0; q < 4; q++) cfma(res, __ldg(&shm[q * ns_p + km]), acc[q]);
   mul[(size_t)rhs * mp + off_p + (size_t)pc * ns_p + km] = res;
 }
 
-// M2L (kernels.cu:239-266, solve.cpp:133-148) fused with L2L from the parent
-// level (kernels.cu:137-238, solve.cpp:149-169).  The far list of a cluster is
-// the 6x6 block of its parent's neighbours' children minus its own 3x3
-// neighbourhood, clipped to the grid; T is indexed by the source offset.
-__global__ void __launch_bounds__(128) k_m2l_l2l(const float2 *__restrict__ mul, float2 *__restrict__ loc, size_t mp,
-                                                 size_t off_c, size_t off_p, int n, int ns, int ns_p,
-                                                 const float2 *__restrict__ T, const int *__restrict__ afirst,
-                                                 const float *__restrict__ aw, int awidth,
-                                                 const float2 *__restrict__ shl_p, int do_m2l, int do_l2l,
-                                                 const int *__restrict__ active) {
-  const int rhs = blockIdx.z;
-  if (inactive(active, rhs)) return;
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= ns) return;
-  const int c = blockIdx.y, cy = c / n, cx = c % n;
-  float2 acc = make_float2(0.f, 0.f);
-  if (do_m2l) {
-    const float2 *m = mul + (size_t)rhs * mp + off_c;
-    const int oy = cy & 1, ox = cx & 1;
-    for (int dy = -2 - oy; dy <= 3 - oy; dy++) {
-      const int yy = cy + dy;
-      if (yy < 0 || yy >= n) continue;
-      for (int dx = -2 - ox; dx <= 3 - ox; dx++) {
-        const int xx = cx + dx;
-        if (xx < 0 || xx >= n) continue;
-        if (dy >= -1 && dy <= 1 && dx >= -1 && dx <= 1) continue;
-        cfma(acc, __ldg(&T[((dy + 3) * 7 + dx + 3) * ns + k]), m[(size_t)(yy * n + xx) * ns + k]);
+// M2L (kernels.cu:239-266, solve.cpp:133-148) as a 2-D stencil per sample.
+// The far list of a cluster is the 6x6 block of its parent's neighbours'
+// children minus its own 3x3 neighbourhood, clipped to the grid, so for a
+// cluster of parity (OY, OX) at row 2a+OY the sources are rows 2a-2 .. 2a+3
+// of the same columns window, and the 27 translation weights depend only on
+// the parity and the sample.  Each thread keeps its 27 weights and a 6x6
+// window of multipoles in registers and slides the window down a column of
+// eight same-parity clusters; a block covers 16 x 4 clusters x 32 samples
+// with the (16+4) x (4+4) halo staged in shared memory.
+constexpr int kM2lRows = 16, kM2lCols = 4, kM2lKC = 32;
+constexpr int kM2lHR = kM2lRows + 4, kM2lHC = kM2lCols + 4;
+
+template <int OY, int OX>
+__device__ __forceinline__ void m2l_column(const float2 (*hs)[kM2lHC][kM2lKC], const float2 *__restrict__ T, int ns,
+                                           int k, int kk, int b, int cy0, int cx0, int n, float2 *__restrict__ out) {
+  constexpr int NR0 = OY + 1, NC0 = OX + 1;  // first near row/column inside the window
+  float2 tw[6][6];
+#pragma unroll
+  for (int i = 0; i < 6; i++)
+#pragma unroll
+    for (int j = 0; j < 6; j++) {
+      const bool nearby = (i >= NR0 && i < NR0 + 3 && j >= NC0 && j < NC0 + 3);
+      tw[i][j] = (!nearby && k < ns) ? __ldg(&T[((i + 1 - OY) * 7 + (j + 1 - OX)) * ns + k]) : make_float2(0.f, 0.f);
+    }
+  float2 w[6][6];
+#pragma unroll
+  for (int i = 0; i < 6; i++)
+#pragma unroll
+    for (int j = 0; j < 6; j++) w[i][j] = hs[i][2 * b + j][kk];
+#pragma unroll
+  for (int a = 0; a < kM2lRows / 2; a++) {
+    if (a > 0) {
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 6; j++) w[i][j] = w[i + 2][j];
+#pragma unroll
+      for (int j = 0; j < 6; j++) {
+        w[4][j] = hs[2 * a + 4][2 * b + j][kk];
+        w[5][j] = hs[2 * a + 5][2 * b + j][kk];
       }
     }
+    float2 acc[3] = {};
+    int term = 0;
+#pragma unroll
+    for (int i = 0; i < 6; i++)
+#pragma unroll
+      for (int j = 0; j < 6; j++) {
+        const bool nearby = (i >= NR0 && i < NR0 + 3 && j >= NC0 && j < NC0 + 3);
+        if (nearby) continue;
+        cfma(acc[term % 3], tw[i][j], w[i][j]);
+        term++;
+      }
+    const int cy = cy0 + 2 * a + OY, cx = cx0 + 2 * b + OX;
+    if (cy < n && cx < n && k < ns) out[(size_t)(cy * n + cx) * ns + k] = cadd(acc[0], cadd(acc[1], acc[2]));
   }
-  if (do_l2l) {
-    const int np = n >> 1;
-    const float2 *lp = loc + (size_t)rhs * mp + off_p + (size_t)((cy >> 1) * np + (cx >> 1)) * ns_p;
-    const float2 *sh = shl_p + ((cy & 1) * 2 + (cx & 1)) * ns_p;
-    int idx = afirst[k];
-    float2 a2 = make_float2(0.f, 0.f);
-    for (int t = 0; t < awidth; t++) {
-      rfma(a2, __ldg(&aw[t * ns + k]), cmul(__ldg(&sh[idx]), lp[idx]));
-      if (++idx == ns_p) idx = 0;
+}
+
+__global__ void __launch_bounds__(256, 1) k_m2l(const float2 *__restrict__ mul, float2 *__restrict__ loc, size_t mp,
+                                                size_t off, int n, int ns, int nkc, int tiles_x,
+                                                const float2 *__restrict__ T, const int *__restrict__ active) {
+  __shared__ float2 hs[kM2lHR][kM2lHC][kM2lKC];
+  const int rhs = blockIdx.y;
+  if (inactive(active, rhs)) return;
+  const int kc = blockIdx.x % nkc, tile = blockIdx.x / nkc;
+  const int cy0 = (tile / tiles_x) * kM2lRows, cx0 = (tile % tiles_x) * kM2lCols, k0 = kc * kM2lKC;
+  const float2 *m = mul + (size_t)rhs * mp + off;
+  for (int e = threadIdx.x; e < kM2lHR * kM2lHC * kM2lKC; e += blockDim.x) {
+    const int kk = e % kM2lKC, hc = (e / kM2lKC) % kM2lHC, hr = e / (kM2lKC * kM2lHC);
+    const int cy = cy0 - 2 + hr, cx = cx0 - 2 + hc, k = k0 + kk;
+    float2 v = make_float2(0.f, 0.f);
+    if (cy >= 0 && cy < n && cx >= 0 && cx < n && k < ns) v = m[(size_t)(cy * n + cx) * ns + k];
+    hs[hr][hc][kk] = v;
+  }
+  __syncthreads();
+  const int kk = threadIdx.x & 31, par = (threadIdx.x >> 5) & 3, b = threadIdx.x >> 7, k = k0 + kk;
+  float2 *out = loc + (size_t)rhs * mp + off;
+  switch (par) {
+    case 0: m2l_column<0, 0>(hs, T, ns, k, kk, b, cy0, cx0, n, out); break;
+    case 1: m2l_column<0, 1>(hs, T, ns, k, kk, b, cy0, cx0, n, out); break;
+    case 2: m2l_column<1, 0>(hs, T, ns, k, kk, b, cy0, cx0, n, out); break;
+    default: m2l_column<1, 1>(hs, T, ns, k, kk, b, cy0, cx0, n, out); break;
+  }
+}
+
+// L2L (kernels.cu:137-238, solve.cpp:149-169 and 389-429): the parent's local
+// expansion, shifted to each child centre, anterpolated to the child rate and
+// added to (or written over) the child's local expansion.  The four shifted
+// parent rings are staged in shared memory when they fit.
+template <bool STAGE>
+__global__ void __launch_bounds__(128) k_l2l(float2 *__restrict__ loc, size_t mp, size_t off_p, size_t off_c, int n_p,
+                                             int ns_p, int ns_c, int nchunk, const int *__restrict__ afirst,
+                                             const float *__restrict__ aw, int awidth,
+                                             const float2 *__restrict__ shl_p, int accumulate,
+                                             const int *__restrict__ active) {
+  extern __shared__ float2 tmp[];
+  const int rhs = blockIdx.y;
+  if (inactive(active, rhs)) return;
+  const int pc = blockIdx.x / nchunk, chunk = blockIdx.x % nchunk;
+  const int py = pc / n_p, px = pc % n_p, n_c = 2 * n_p;
+  const float2 *lp = loc + (size_t)rhs * mp + off_p + (size_t)pc * ns_p;
+  if (STAGE) {
+    for (int e = threadIdx.x; e < 4 * ns_p; e += blockDim.x) tmp[e] = cmul(__ldg(&shl_p[e]), lp[e % ns_p]);
+    __syncthreads();
+  }
+  const int km = chunk * blockDim.x + threadIdx.x;
+  if (km >= ns_c) return;
+  int idx = afirst[km];
+  float2 acc[4] = {};
+  for (int t = 0; t < awidth; t++) {
+    const float w = __ldg(&aw[t * ns_c + km]);
+    if (STAGE) {
+#pragma unroll
+      for (int q = 0; q < 4; q++) rfma(acc[q], w, tmp[q * ns_p + idx]);
+    } else {
+      const float2 v = lp[idx];
+#pragma unroll
+      for (int q = 0; q < 4; q++) rfma(acc[q], w, cmul(__ldg(&shl_p[q * ns_p + idx]), v));
     }
-    acc = cadd(acc, a2);
+    if (++idx == ns_p) idx = 0;
   }
-  loc[(size_t)rhs * mp + off_c + (size_t)c * ns + k] = acc;
+  float2 *lc = loc + (size_t)rhs * mp + off_c;
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    float2 *d = lc + (size_t)((2 * py + (q >> 1)) * n_c + 2 * px + (q & 1)) * ns_c + km;
+    *d = accumulate ? cadd(*d, acc[q]) : acc[q];
+  }
 }
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -317,20 +416,45 @@ void launch_p2m(const DevPlan &P, const BatchArgs &B, float2 *mul, cudaStream_t 
 
 void launch_m2m(const DevPlan &P, int lvl, float2 *mul, int nrhs, const int *active, cudaStream_t st) {
   const DevLevel &p = P.lv[lvl], &c = P.lv[lvl + 1];
-  dim3 grid((p.ns + 127) / 128, p.n * p.n, nrhs);
+  const int nchunk = (p.ns + 127) / 128;
+  dim3 grid(nchunk * p.n * p.n, nrhs);
+  const size_t smem = (size_t)4 * c.ns * sizeof(float2);
   count_launch();
-  k_m2m<<<grid, 128, 0, st>>>(mul, P.mp, p.off, c.off, p.n, p.ns, c.ns, p.ifirst, p.iw, p.shm, P.ninter, active);
+  if (smem <= (size_t)kSmemStage) {
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_m2m<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_m2m<true><<<grid, 128, smem, st>>>(mul, P.mp, p.off, c.off, p.n, p.ns, c.ns, nchunk, p.ifirst, p.iw, p.shm,
+                                         P.ninter, active);
+  } else {
+    k_m2m<false><<<grid, 128, 0, st>>>(mul, P.mp, p.off, c.off, p.n, p.ns, c.ns, nchunk, p.ifirst, p.iw, p.shm,
+                                       P.ninter, active);
+  }
 }
 
-void launch_m2l_l2l(const DevPlan &P, int lvl, const float2 *mul, float2 *loc, int nrhs, const int *active,
-                    bool do_m2l, bool do_l2l, cudaStream_t st) {
+void launch_m2l(const DevPlan &P, int lvl, const float2 *mul, float2 *loc, int nrhs, const int *active,
+                cudaStream_t st) {
   const DevLevel &c = P.lv[lvl];
-  const DevLevel *p = lvl > 0 ? &P.lv[lvl - 1] : nullptr;
-  dim3 grid((c.ns + 127) / 128, c.n * c.n, nrhs);
+  const int nkc = (c.ns + kM2lKC - 1) / kM2lKC;
+  const int tiles_x = (c.n + kM2lCols - 1) / kM2lCols, tiles_y = (c.n + kM2lRows - 1) / kM2lRows;
+  dim3 grid(nkc * tiles_x * tiles_y, nrhs);
   count_launch();
-  k_m2l_l2l<<<grid, 128, 0, st>>>(mul, loc, P.mp, c.off, p ? p->off : 0, c.n, c.ns, p ? p->ns : 1, c.T, c.afirst,
-                                  c.aw, c.awidth, p ? p->shl : nullptr, do_m2l ? 1 : 0, (do_l2l && p) ? 1 : 0,
-                                  active);
+  k_m2l<<<grid, 256, 0, st>>>(mul, loc, P.mp, c.off, c.n, c.ns, nkc, tiles_x, c.T, active);
+}
+
+void launch_l2l(const DevPlan &P, int lvl, float2 *loc, int nrhs, const int *active, bool accumulate,
+                cudaStream_t st) {
+  const DevLevel &c = P.lv[lvl], &p = P.lv[lvl - 1];
+  const int nchunk = (c.ns + 127) / 128;
+  dim3 grid(nchunk * p.n * p.n, nrhs);
+  const size_t smem = (size_t)4 * p.ns * sizeof(float2);
+  count_launch();
+  if (smem <= (size_t)kSmemStage) {
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_l2l<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_l2l<true><<<grid, 128, smem, st>>>(loc, P.mp, p.off, c.off, p.n, p.ns, c.ns, nchunk, c.afirst, c.aw,
+                                         c.awidth, p.shl, accumulate ? 1 : 0, active);
+  } else {
+    k_l2l<false><<<grid, 128, 0, st>>>(loc, P.mp, p.off, c.off, p.n, p.ns, c.ns, nchunk, c.afirst, c.aw,
+                                       c.awidth, p.shl, accumulate ? 1 : 0, active);
+  }
 }
 
 int near_blocks_per_rhs(const DevPlan &P) {

@@ -343,7 +343,8 @@ isg_status run_matvec(isg_ctx *c, const float2 *x, const float2 *g, int64_t gs, 
     launch_p2m(P, B, c->mul, st);
   }
   for (int i = P.L - 2; i >= 2; i--) launch_m2m(P, i, c->mul, nrhs, active, st);
-  for (int i = 2; i < P.L; i++) launch_m2l_l2l(P, i, c->mul, c->loc, nrhs, active, true, i > 2, st);
+  for (int i = 2; i < P.L; i++) launch_m2l(P, i, c->mul, c->loc, nrhs, active, st);
+  for (int i = 3; i < P.L; i++) launch_l2l(P, i, c->loc, nrhs, active, true, st);
   NearArgs A;
   A.in = B;
   A.loc = c->loc;
