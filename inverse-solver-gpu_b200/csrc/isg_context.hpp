@@ -64,4 +64,6 @@ void tc_destroy(isg_ctx *c);
 bool tc_available(const isg_ctx *c);
 isg_status tc_p2m(isg_ctx *c, const BatchArgs &B, float2 *mul, cudaStream_t st);
 isg_status tc_near(isg_ctx *c, const NearArgs &A, cudaStream_t st);
+// Nonzero when a bounded wait inside a tensor-core kernel gave up.
+int tc_error(isg_ctx *c);
 }  // namespace isg

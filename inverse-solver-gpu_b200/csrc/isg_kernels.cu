@@ -2,6 +2,7 @@
 // P2M/M2M/M2L/L2L/L2P/P2P stages, re-designed for a batched, RHS-major layout
 // and raster cluster numbering).  The tensor-core leaf kernels live in
 // isg_tc.cu.
+#include <algorithm>
 #include <atomic>
 
 #include "isg_device.cuh"
@@ -61,80 +62,131 @@ __global__ void __launch_bounds__(128) k_p2m(const float2 *__restrict__ x, const
 }
 
 constexpr int kSmemStage = 200 * 1024;  // largest ring staged in shared memory
+constexpr int kStageBudget = 32 * 1024;  // per-block staging target for the small levels
+
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem, bool valid) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(valid ? 8 : 0));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+// Block-wide barrier usable from warp-uniform divergent paths (every warp
+// reaches it the same number of times).
+__device__ __forceinline__ void block_bar1() { asm volatile("bar.sync 1, %0;\n" ::"r"(blockDim.x)); }
 
 // M2M (kernels.cu:83-136, solve.cpp:93-112): parent sample km gathers the
 // 30-tap interpolation of each of its four children, shifts it to the parent
-// centre and sums.  The four children's rings are staged in shared memory
-// (STAGE) or read through L1 when they are too large (top levels only).
+// centre and sums.  A block covers `npb` parents whose children's rings are
+// staged in shared memory (STAGE), or reads through L1 when one parent's
+// children are too large to stage (top levels only).
 template <bool STAGE>
-__global__ void __launch_bounds__(128) k_m2m(float2 *__restrict__ mul, size_t mp, size_t off_p, size_t off_c, int n_p,
-                                             int ns_p, int ns_c, int nchunk, const int *__restrict__ ifirst,
+__global__ void __launch_bounds__(256) k_m2m(float2 *__restrict__ mul, size_t mp, size_t off_p, size_t off_c, int n_p,
+                                             int ns_p, int ns_c, int npb, const int *__restrict__ ifirst,
                                              const float *__restrict__ iw, const float2 *__restrict__ shm,
                                              int ninter, const int *__restrict__ active) {
   extern __shared__ float2 chs[];
   const int rhs = blockIdx.y;
   if (inactive(active, rhs)) return;
-  const int pc = blockIdx.x / nchunk, chunk = blockIdx.x % nchunk;
-  const int py = pc / n_p, px = pc % n_p, n_c = 2 * n_p;
+  const int nparent = n_p * n_p, n_c = 2 * n_p;
+  const int p0 = blockIdx.x * npb, np_here = min(npb, nparent - p0);
   const float2 *base = mul + (size_t)rhs * mp + off_c;
+  auto child = [&](int pc, int q) {
+    return (size_t)((2 * (pc / n_p) + (q >> 1)) * n_c + 2 * (pc % n_p) + (q & 1)) * ns_c;
+  };
   if (STAGE) {
-    for (int e = threadIdx.x; e < 4 * ns_c; e += blockDim.x) {
-      const int q = e / ns_c;
-      chs[e] = base[(size_t)((2 * py + (q >> 1)) * n_c + 2 * px + (q & 1)) * ns_c + e % ns_c];
+    for (int e = threadIdx.x; e < np_here * 4 * ns_c; e += blockDim.x) {
+      const int j = e % ns_c, q = (e / ns_c) & 3, pl = e / (4 * ns_c);
+      chs[e] = base[child(p0 + pl, q) + j];
     }
     __syncthreads();
   }
-  size_t coff[4];
+  for (int u = threadIdx.x; u < np_here * ns_p; u += blockDim.x) {
+    const int pl = u / ns_p, km = u % ns_p, pc = p0 + pl;
+    int idx = ifirst[km];
+    float2 acc[4] = {};
+    for (int t = 0; t < ninter; t++) {
+      const float w = __ldg(&iw[t * ns_p + km]);
 #pragma unroll
-  for (int q = 0; q < 4; q++) coff[q] = (size_t)((2 * py + (q >> 1)) * n_c + 2 * px + (q & 1)) * ns_c;
-  const int km = chunk * blockDim.x + threadIdx.x;
-  if (km >= ns_p) return;
-  int idx = ifirst[km];
-  float2 acc[4] = {};
-  for (int t = 0; t < ninter; t++) {
-    const float w = __ldg(&iw[t * ns_p + km]);
+      for (int q = 0; q < 4; q++) rfma(acc[q], w, STAGE ? chs[(pl * 4 + q) * ns_c + idx] : base[child(pc, q) + idx]);
+      if (++idx == ns_c) idx = 0;
+    }
+    float2 res = make_float2(0.f, 0.f);
 #pragma unroll
-    for (int q = 0; q < 4; q++) rfma(acc[q], w, STAGE ? chs[q * ns_c + idx] : base[coff[q] + idx]);
-    if (++idx == ns_c) idx = 0;
+    for (int q = 0; q < 4; q++) cfma(res, __ldg(&shm[q * ns_p + km]), acc[q]);
+    mul[(size_t)rhs * mp + off_p + (size_t)pc * ns_p + km] = res;
   }
-  float2 res = make_float2(0.f, 0.f);
-#pragma unroll
-  for (int q = 0; q < 4; q++) cfma(res, __ldg(&shm[q * ns_p + km]), acc[q]);
-  mul[(size_t)rhs * mp + off_p + (size_t)pc * ns_p + km] = res;
 }
 
 // M2L (kernels.cu:239-266, solve.cpp:133-148) as a 2-D stencil per sample.
 // The far list of a cluster is the 6x6 block of its parent's neighbours'
 // children minus its own 3x3 neighbourhood, clipped to the grid, so for a
 // cluster of parity (OY, OX) at row 2a+OY the sources are rows 2a-2 .. 2a+3
-// of the same columns window, and the 27 translation weights depend only on
-// the parity and the sample.  Each thread keeps its 27 weights and a 6x6
-// window of multipoles in registers and slides the window down a column of
-// eight same-parity clusters; a block covers 16 x 4 clusters x 32 samples
-// with the (16+4) x (4+4) halo staged in shared memory.
+// of a six-column window, and the 27 translation weights depend only on the
+// parity and the sample.  A block owns one chunk of 32 samples: each thread
+// keeps its 27 weights in registers for the whole launch and walks a list of
+// (tile of 16 x 4 clusters, RHS) items, sliding a 6x6 register window of
+// multipoles down a column of eight same-parity clusters.  The (16+4) x (4+4)
+// halo of the next item is fetched with cp.async while the current one is
+// computed.
 constexpr int kM2lRows = 16, kM2lCols = 4, kM2lKC = 32;
 constexpr int kM2lHR = kM2lRows + 4, kM2lHC = kM2lCols + 4;
+constexpr int kM2lHalo = kM2lHR * kM2lHC * kM2lKC;
+
+struct M2lArgs {
+  const float2 *mul;
+  float2 *loc;
+  size_t mp, off;
+  int n, ns, tiles_x, tiles, nitems;
+  const float2 *T;
+  const int *active;
+};
+
+__device__ __forceinline__ void m2l_issue(const M2lArgs &A, int item, int k0, float2 *buf) {
+  const int tile = item % A.tiles, rhs = item / A.tiles;
+  const int cy0 = (tile / A.tiles_x) * kM2lRows, cx0 = (tile % A.tiles_x) * kM2lCols;
+  const float2 *m = A.mul + (size_t)rhs * A.mp + A.off;
+  for (int e = threadIdx.x; e < kM2lHalo; e += blockDim.x) {
+    const int kk = e % kM2lKC, hc = (e / kM2lKC) % kM2lHC, hr = e / (kM2lKC * kM2lHC);
+    const int cy = cy0 - 2 + hr, cx = cx0 - 2 + hc, k = k0 + kk;
+    const bool ok = cy >= 0 && cy < A.n && cx >= 0 && cx < A.n && k < A.ns;
+    cp_async8(&buf[e], ok ? (const void *)&m[(size_t)(cy * A.n + cx) * A.ns + k] : (const void *)A.mul, ok);
+  }
+}
 
 template <int OY, int OX>
-__device__ __forceinline__ void m2l_column(const float2 (*hs)[kM2lHC][kM2lKC], const float2 *__restrict__ T, int ns,
-                                           int k, int kk, int b, int cy0, int cx0, int n, float2 *__restrict__ out) {
+__device__ __forceinline__ void m2l_worker(const M2lArgs &A, float2 *hbuf) {
   constexpr int NR0 = OY + 1, NC0 = OX + 1;  // first near row/column inside the window
+  const int kk = threadIdx.x & 31, b = threadIdx.x >> 7;
+  const int k0 = blockIdx.x * kM2lKC, k = k0 + kk;
   float2 tw[6][6];
 #pragma unroll
   for (int i = 0; i < 6; i++)
 #pragma unroll
     for (int j = 0; j < 6; j++) {
       const bool nearby = (i >= NR0 && i < NR0 + 3 && j >= NC0 && j < NC0 + 3);
-      tw[i][j] = (!nearby && k < ns) ? __ldg(&T[((i + 1 - OY) * 7 + (j + 1 - OX)) * ns + k]) : make_float2(0.f, 0.f);
+      tw[i][j] = (!nearby && k < A.ns) ? __ldg(&A.T[((i + 1 - OY) * 7 + (j + 1 - OX)) * A.ns + k])
+                                       : make_float2(0.f, 0.f);
     }
-  float2 w[6][6];
+  int buf = 0;
+  const int G = gridDim.y;
+  for (int item = blockIdx.y; item < A.nitems; item += G) {
+    if (item + G < A.nitems) m2l_issue(A, item + G, k0, hbuf + (buf ^ 1) * kM2lHalo);
+    cp_async_commit();
+    cp_async_wait1();
+    block_bar1();
+    const float2(*hs)[kM2lHC][kM2lKC] = (const float2(*)[kM2lHC][kM2lKC])(hbuf + buf * kM2lHalo);
+    const int tile = item % A.tiles, rhs = item / A.tiles;
+    const bool live = !(A.active && !A.active[rhs]);
+    const int cy0 = (tile / A.tiles_x) * kM2lRows, cx0 = (tile % A.tiles_x) * kM2lCols;
+    float2 *out = A.loc + (size_t)rhs * A.mp + A.off;
+    // Rows 0..3 of the first window; each step loads two new rows and slides.
+    float2 w[6][6];
 #pragma unroll
-  for (int i = 0; i < 6; i++)
+    for (int i = 0; i < 4; i++)
 #pragma unroll
-    for (int j = 0; j < 6; j++) w[i][j] = hs[i][2 * b + j][kk];
-#pragma unroll
-  for (int a = 0; a < kM2lRows / 2; a++) {
-    if (a > 0) {
+      for (int j = 0; j < 6; j++) w[i + 2][j] = hs[i][2 * b + j][kk];
+#pragma unroll 1
+    for (int a = 0; a < kM2lRows / 2; a++) {
 #pragma unroll
       for (int i = 0; i < 4; i++)
 #pragma unroll
@@ -144,91 +196,86 @@ __device__ __forceinline__ void m2l_column(const float2 (*hs)[kM2lHC][kM2lKC], c
         w[4][j] = hs[2 * a + 4][2 * b + j][kk];
         w[5][j] = hs[2 * a + 5][2 * b + j][kk];
       }
+      float2 acc[3] = {};
+      int term = 0;
+#pragma unroll
+      for (int i = 0; i < 6; i++)
+#pragma unroll
+        for (int j = 0; j < 6; j++) {
+          const bool nearby = (i >= NR0 && i < NR0 + 3 && j >= NC0 && j < NC0 + 3);
+          if (nearby) continue;
+          cfma(acc[term % 3], tw[i][j], w[i][j]);
+          term++;
+        }
+      const int cy = cy0 + 2 * a + OY, cx = cx0 + 2 * b + OX;
+      if (live && cy < A.n && cx < A.n && k < A.ns)
+        out[(size_t)(cy * A.n + cx) * A.ns + k] = cadd(acc[0], cadd(acc[1], acc[2]));
     }
-    float2 acc[3] = {};
-    int term = 0;
-#pragma unroll
-    for (int i = 0; i < 6; i++)
-#pragma unroll
-      for (int j = 0; j < 6; j++) {
-        const bool nearby = (i >= NR0 && i < NR0 + 3 && j >= NC0 && j < NC0 + 3);
-        if (nearby) continue;
-        cfma(acc[term % 3], tw[i][j], w[i][j]);
-        term++;
-      }
-    const int cy = cy0 + 2 * a + OY, cx = cx0 + 2 * b + OX;
-    if (cy < n && cx < n && k < ns) out[(size_t)(cy * n + cx) * ns + k] = cadd(acc[0], cadd(acc[1], acc[2]));
+    block_bar1();
+    buf ^= 1;
   }
 }
 
-__global__ void __launch_bounds__(256, 1) k_m2l(const float2 *__restrict__ mul, float2 *__restrict__ loc, size_t mp,
-                                                size_t off, int n, int ns, int nkc, int tiles_x,
-                                                const float2 *__restrict__ T, const int *__restrict__ active) {
-  __shared__ float2 hs[kM2lHR][kM2lHC][kM2lKC];
-  const int rhs = blockIdx.y;
-  if (inactive(active, rhs)) return;
-  const int kc = blockIdx.x % nkc, tile = blockIdx.x / nkc;
-  const int cy0 = (tile / tiles_x) * kM2lRows, cx0 = (tile % tiles_x) * kM2lCols, k0 = kc * kM2lKC;
-  const float2 *m = mul + (size_t)rhs * mp + off;
-  for (int e = threadIdx.x; e < kM2lHR * kM2lHC * kM2lKC; e += blockDim.x) {
-    const int kk = e % kM2lKC, hc = (e / kM2lKC) % kM2lHC, hr = e / (kM2lKC * kM2lHC);
-    const int cy = cy0 - 2 + hr, cx = cx0 - 2 + hc, k = k0 + kk;
-    float2 v = make_float2(0.f, 0.f);
-    if (cy >= 0 && cy < n && cx >= 0 && cx < n && k < ns) v = m[(size_t)(cy * n + cx) * ns + k];
-    hs[hr][hc][kk] = v;
-  }
-  __syncthreads();
-  const int kk = threadIdx.x & 31, par = (threadIdx.x >> 5) & 3, b = threadIdx.x >> 7, k = k0 + kk;
-  float2 *out = loc + (size_t)rhs * mp + off;
-  switch (par) {
-    case 0: m2l_column<0, 0>(hs, T, ns, k, kk, b, cy0, cx0, n, out); break;
-    case 1: m2l_column<0, 1>(hs, T, ns, k, kk, b, cy0, cx0, n, out); break;
-    case 2: m2l_column<1, 0>(hs, T, ns, k, kk, b, cy0, cx0, n, out); break;
-    default: m2l_column<1, 1>(hs, T, ns, k, kk, b, cy0, cx0, n, out); break;
+__global__ void __launch_bounds__(256, 1) k_m2l(M2lArgs A) {
+  extern __shared__ float2 hbuf[];
+  if (blockIdx.y < A.nitems) m2l_issue(A, blockIdx.y, blockIdx.x * kM2lKC, hbuf);
+  cp_async_commit();
+  switch ((threadIdx.x >> 5) & 3) {
+    case 0: m2l_worker<0, 0>(A, hbuf); break;
+    case 1: m2l_worker<0, 1>(A, hbuf); break;
+    case 2: m2l_worker<1, 0>(A, hbuf); break;
+    default: m2l_worker<1, 1>(A, hbuf); break;
   }
 }
 
 // L2L (kernels.cu:137-238, solve.cpp:149-169 and 389-429): the parent's local
 // expansion, shifted to each child centre, anterpolated to the child rate and
-// added to (or written over) the child's local expansion.  The four shifted
-// parent rings are staged in shared memory when they fit.
+// added to (or written over) the child's local expansion.  A block covers `npb`
+// parents whose four shifted rings are staged in shared memory, or reads
+// through L1 when one parent's rings are too large (top levels only).
 template <bool STAGE>
-__global__ void __launch_bounds__(128) k_l2l(float2 *__restrict__ loc, size_t mp, size_t off_p, size_t off_c, int n_p,
-                                             int ns_p, int ns_c, int nchunk, const int *__restrict__ afirst,
+__global__ void __launch_bounds__(256) k_l2l(float2 *__restrict__ loc, size_t mp, size_t off_p, size_t off_c, int n_p,
+                                             int ns_p, int ns_c, int npb, const int *__restrict__ afirst,
                                              const float *__restrict__ aw, int awidth,
                                              const float2 *__restrict__ shl_p, int accumulate,
                                              const int *__restrict__ active) {
   extern __shared__ float2 tmp[];
   const int rhs = blockIdx.y;
   if (inactive(active, rhs)) return;
-  const int pc = blockIdx.x / nchunk, chunk = blockIdx.x % nchunk;
-  const int py = pc / n_p, px = pc % n_p, n_c = 2 * n_p;
-  const float2 *lp = loc + (size_t)rhs * mp + off_p + (size_t)pc * ns_p;
+  const int nparent = n_p * n_p, n_c = 2 * n_p;
+  const int p0 = blockIdx.x * npb, np_here = min(npb, nparent - p0);
+  const float2 *lp0 = loc + (size_t)rhs * mp + off_p;
   if (STAGE) {
-    for (int e = threadIdx.x; e < 4 * ns_p; e += blockDim.x) tmp[e] = cmul(__ldg(&shl_p[e]), lp[e % ns_p]);
+    for (int e = threadIdx.x; e < np_here * 4 * ns_p; e += blockDim.x) {
+      const int j = e % ns_p, q = (e / ns_p) & 3, pl = e / (4 * ns_p);
+      tmp[e] = cmul(__ldg(&shl_p[q * ns_p + j]), lp0[(size_t)(p0 + pl) * ns_p + j]);
+    }
     __syncthreads();
   }
-  const int km = chunk * blockDim.x + threadIdx.x;
-  if (km >= ns_c) return;
-  int idx = afirst[km];
-  float2 acc[4] = {};
-  for (int t = 0; t < awidth; t++) {
-    const float w = __ldg(&aw[t * ns_c + km]);
-    if (STAGE) {
-#pragma unroll
-      for (int q = 0; q < 4; q++) rfma(acc[q], w, tmp[q * ns_p + idx]);
-    } else {
-      const float2 v = lp[idx];
-#pragma unroll
-      for (int q = 0; q < 4; q++) rfma(acc[q], w, cmul(__ldg(&shl_p[q * ns_p + idx]), v));
-    }
-    if (++idx == ns_p) idx = 0;
-  }
   float2 *lc = loc + (size_t)rhs * mp + off_c;
+  for (int u = threadIdx.x; u < np_here * ns_c; u += blockDim.x) {
+    const int pl = u / ns_c, km = u % ns_c, pc = p0 + pl;
+    const float2 *lp = lp0 + (size_t)pc * ns_p;
+    int idx = afirst[km];
+    float2 acc[4] = {};
+    for (int t = 0; t < awidth; t++) {
+      const float w = __ldg(&aw[t * ns_c + km]);
+      if (STAGE) {
 #pragma unroll
-  for (int q = 0; q < 4; q++) {
-    float2 *d = lc + (size_t)((2 * py + (q >> 1)) * n_c + 2 * px + (q & 1)) * ns_c + km;
-    *d = accumulate ? cadd(*d, acc[q]) : acc[q];
+        for (int q = 0; q < 4; q++) rfma(acc[q], w, tmp[(pl * 4 + q) * ns_p + idx]);
+      } else {
+        const float2 v = lp[idx];
+#pragma unroll
+        for (int q = 0; q < 4; q++) rfma(acc[q], w, cmul(__ldg(&shl_p[q * ns_p + idx]), v));
+      }
+      if (++idx == ns_p) idx = 0;
+    }
+    const int py = pc / n_p, px = pc % n_p;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      float2 *d = lc + (size_t)((2 * py + (q >> 1)) * n_c + 2 * px + (q & 1)) * ns_c + km;
+      *d = accumulate ? cadd(*d, acc[q]) : acc[q];
+    }
   }
 }
 
@@ -414,18 +461,27 @@ void launch_p2m(const DevPlan &P, const BatchArgs &B, float2 *mul, cudaStream_t 
                               mul + P.lv[P.L - 1].off, P.mp);
 }
 
+// Parents per block so that the staged rings stay near kStageBudget.
+static int parents_per_block(size_t ring_bytes, int nparent) {
+  const int npb = (int)std::max<size_t>(1, kStageBudget / std::max<size_t>(1, ring_bytes));
+  return std::min(npb, std::max(1, nparent));
+}
+
 void launch_m2m(const DevPlan &P, int lvl, float2 *mul, int nrhs, const int *active, cudaStream_t st) {
   const DevLevel &p = P.lv[lvl], &c = P.lv[lvl + 1];
-  const int nchunk = (p.ns + 127) / 128;
-  dim3 grid(nchunk * p.n * p.n, nrhs);
-  const size_t smem = (size_t)4 * c.ns * sizeof(float2);
+  const size_t ring = (size_t)4 * c.ns * sizeof(float2);
+  const int nparent = p.n * p.n;
   count_launch();
-  if (smem <= (size_t)kSmemStage) {
+  if (ring <= (size_t)kSmemStage) {
+    const int npb = parents_per_block(ring, nparent);
+    const size_t smem = ring * npb;
     if (smem > 48 * 1024) cudaFuncSetAttribute(k_m2m<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_m2m<true><<<grid, 128, smem, st>>>(mul, P.mp, p.off, c.off, p.n, p.ns, c.ns, nchunk, p.ifirst, p.iw, p.shm,
+    dim3 grid((nparent + npb - 1) / npb, nrhs);
+    k_m2m<true><<<grid, 256, smem, st>>>(mul, P.mp, p.off, c.off, p.n, p.ns, c.ns, npb, p.ifirst, p.iw, p.shm,
                                          P.ninter, active);
   } else {
-    k_m2m<false><<<grid, 128, 0, st>>>(mul, P.mp, p.off, c.off, p.n, p.ns, c.ns, nchunk, p.ifirst, p.iw, p.shm,
+    dim3 grid(nparent, nrhs);
+    k_m2m<false><<<grid, 256, 0, st>>>(mul, P.mp, p.off, c.off, p.n, p.ns, c.ns, 1, p.ifirst, p.iw, p.shm,
                                        P.ninter, active);
   }
 }
@@ -433,27 +489,44 @@ void launch_m2m(const DevPlan &P, int lvl, float2 *mul, int nrhs, const int *act
 void launch_m2l(const DevPlan &P, int lvl, const float2 *mul, float2 *loc, int nrhs, const int *active,
                 cudaStream_t st) {
   const DevLevel &c = P.lv[lvl];
+  M2lArgs A;
+  A.mul = mul;
+  A.loc = loc;
+  A.mp = P.mp;
+  A.off = c.off;
+  A.n = c.n;
+  A.ns = c.ns;
+  A.tiles_x = (c.n + kM2lCols - 1) / kM2lCols;
+  A.tiles = A.tiles_x * ((c.n + kM2lRows - 1) / kM2lRows);
+  A.nitems = A.tiles * nrhs;
+  A.T = c.T;
+  A.active = active;
   const int nkc = (c.ns + kM2lKC - 1) / kM2lKC;
-  const int tiles_x = (c.n + kM2lCols - 1) / kM2lCols, tiles_y = (c.n + kM2lRows - 1) / kM2lRows;
-  dim3 grid(nkc * tiles_x * tiles_y, nrhs);
+  // one resident block per SM: spread the items so every SM has a sample chunk
+  const int groups = std::max(1, std::min(A.nitems, (2 * 148 + nkc - 1) / nkc));
+  const size_t smem = 2 * (size_t)kM2lHalo * sizeof(float2);
+  cudaFuncSetAttribute(k_m2l, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   count_launch();
-  k_m2l<<<grid, 256, 0, st>>>(mul, loc, P.mp, c.off, c.n, c.ns, nkc, tiles_x, c.T, active);
+  k_m2l<<<dim3(nkc, groups), 256, smem, st>>>(A);
 }
 
 void launch_l2l(const DevPlan &P, int lvl, float2 *loc, int nrhs, const int *active, bool accumulate,
                 cudaStream_t st) {
   const DevLevel &c = P.lv[lvl], &p = P.lv[lvl - 1];
-  const int nchunk = (c.ns + 127) / 128;
-  dim3 grid(nchunk * p.n * p.n, nrhs);
-  const size_t smem = (size_t)4 * p.ns * sizeof(float2);
+  const size_t ring = (size_t)4 * p.ns * sizeof(float2);
+  const int nparent = p.n * p.n;
   count_launch();
-  if (smem <= (size_t)kSmemStage) {
+  if (ring <= (size_t)kSmemStage) {
+    const int npb = parents_per_block(ring, nparent);
+    const size_t smem = ring * npb;
     if (smem > 48 * 1024) cudaFuncSetAttribute(k_l2l<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_l2l<true><<<grid, 128, smem, st>>>(loc, P.mp, p.off, c.off, p.n, p.ns, c.ns, nchunk, c.afirst, c.aw,
-                                         c.awidth, p.shl, accumulate ? 1 : 0, active);
+    dim3 grid((nparent + npb - 1) / npb, nrhs);
+    k_l2l<true><<<grid, 256, smem, st>>>(loc, P.mp, p.off, c.off, p.n, p.ns, c.ns, npb, c.afirst, c.aw, c.awidth,
+                                         p.shl, accumulate ? 1 : 0, active);
   } else {
-    k_l2l<false><<<grid, 128, 0, st>>>(loc, P.mp, p.off, c.off, p.n, p.ns, c.ns, nchunk, c.afirst, c.aw,
-                                       c.awidth, p.shl, accumulate ? 1 : 0, active);
+    dim3 grid(nparent, nrhs);
+    k_l2l<false><<<grid, 256, 0, st>>>(loc, P.mp, p.off, c.off, p.n, p.ns, c.ns, 1, c.afirst, c.aw, c.awidth,
+                                       p.shl, accumulate ? 1 : 0, active);
   }
 }
 

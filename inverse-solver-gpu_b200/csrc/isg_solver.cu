@@ -427,6 +427,10 @@ isg_status run_bicgs(isg_ctx *c, float2 *x, const float2 *g, int64_t gs, const f
   std::vector<RhsState> hs(R);
   cudaMemcpyAsync(hs.data(), c->state, R * sizeof(RhsState), cudaMemcpyDeviceToHost, st);
   if ((e = cuda_check(c, cudaStreamSynchronize(st), "bicgs results")) != ISG_OK) return e;
+  if (engine == ISG_ENGINE_TENSOR && tc_error(c)) {
+    c->err = "a tensor-core kernel hit its wait limit";
+    return ISG_TIMEOUT;
+  }
   isg_status worst = ISG_OK;
   for (int r = 0; r < R; r++) {
     if (info) {

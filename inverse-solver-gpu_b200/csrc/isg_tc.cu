@@ -1,19 +1,702 @@
-// Tensor-core engine for the dense leaf stages (near field + L2P, P2M).
+// Tensor-core engine for the dense leaf stages of the MLFMA matvec on sm_100a.
+//
+// Near field + L2P (kernels.cu:32-81, 292-319; solve.cpp:170-216) and P2M
+// (kernels.cu:6-30; solve.cpp:80-92) are complex GEMMs with a shared,
+// translation-invariant operand.  Each runs as a real GEMM through the
+// embedding [re, im] x [[re, -im], [im, re]] on tcgen05 (kind::f16, FP32
+// accumulation in TMEM).  FP32 accuracy comes from splitting both operands
+// into FP16 pairs, v = hi + lo, after a power-of-two scaling of each tile into
+// the FP16 range, and summing hi*hi + hi*lo + lo*hi (the lo*lo term is below
+// FP32 rounding).
+//
+// Near-field CTA: a tile of 16 x 8 leaves of one RHS.  Its 18 x 10 halo of
+// leaves is stored once in shared memory in the K-major core-matrix layout
+// [halo row][16-byte K chunk][halo column], so the operand of each of the nine
+// neighbour slots is the same halo seen through a descriptor shifted by one
+// halo row / column.  The weights (9 slots x 128 x 128 reals, then the
+// L2P basis) stream through a 4-deep ring of 16 KB stages filled by bulk
+// async copies.  Warp 1 is the copy producer, thread 0 issues the MMAs, the
+// other warps load and convert operands and all warps run the epilogue.
+#include <cmath>
+#include <vector>
+
 #include "isg_context.hpp"
+#include "isg_tc.cuh"
 
 namespace isg {
 
-struct TcPlan {
-  int dummy = 0;
+namespace {
+
+using namespace tc;
+
+constexpr int kTY = 16, kTX = 8;                 // leaves per tile
+constexpr int kHR = kTY + 2, kHC = kTX + 2;      // halo
+constexpr int kLboA = kHC * 16;                  // 160
+constexpr int kSboA = 16 * kLboA;                // 2560 (one halo row: 16 K-chunks)
+constexpr int kRegion = kHR * kSboA;             // 46080 bytes per FP16 split
+constexpr int kStageBytes = 16384;               // hi [128 x 32] + lo [128 x 32]
+constexpr int kStageHalf = 8192;
+constexpr int kNB = 4;                           // ring depth
+constexpr int kNearStages = 36;                  // 9 slots x 4 K-chunks of 32 reals
+constexpr int kLocChunksMax = 20;                // K chunks (8 reals each) of the L2P operand
+constexpr int kSboL = kLocChunksMax * 128;       // 2560
+constexpr int kLoaders = 224;                    // warps 0, 2..7
+constexpr int kErrNearFull = 101, kErrNearEmpty = 102, kErrNearDone = 103, kErrP2m = 111;
+
+struct NearSmem {
+  static constexpr int hi = 0, lo = kRegion, stages = 2 * kRegion, bars = stages + kNB * kStageBytes;
+  static constexpr int misc = bars + 16 * 8;
+  static constexpr int total = misc + 256;
 };
 
-isg_status tc_setup(isg_ctx *) { return ISG_OK; }
+__device__ __forceinline__ int loader_id() {
+  const int w = threadIdx.x >> 5;
+  return w == 0 ? threadIdx.x : threadIdx.x - 32;
+}
+__device__ __forceinline__ void loaders_bar() { asm volatile("bar.sync 1, %0;\n" ::"n"(kLoaders)); }
+
+// max over the loader threads (named barrier 1)
+__device__ float loaders_max(float v, float *scratch) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) scratch[w] = v;
+  loaders_bar();
+  float m = 0.f;
+  for (int q = 0; q < 8; q++)
+    if (q != 1) m = fmaxf(m, scratch[q]);
+  loaders_bar();
+  return m;
+}
+
+__device__ __forceinline__ float2 transform(float2 v, float2 g, int mode) {
+  if (mode == IN_G) return cmul(g, v);
+  if (mode == IN_CONJ) return cconj(v);
+  return v;
+}
+
+__device__ __forceinline__ float cabs1(float2 v) { return fmaxf(fabsf(v.x), fabsf(v.y)); }
+
+// Stores 4 complex values as one 16-byte chunk of hi and one of lo.
+__device__ __forceinline__ void store_chunk(char *smem, int off, const float2 *v, float s) {
+  __align__(16) __half h[8], l[8];
+#pragma unroll
+  for (int p = 0; p < 4; p++) {
+    split_f16(v[p].x * s, h[2 * p], l[2 * p]);
+    split_f16(v[p].y * s, h[2 * p + 1], l[2 * p + 1]);
+  }
+  *(uint4 *)(smem + NearSmem::hi + off) = *(uint4 *)h;
+  *(uint4 *)(smem + NearSmem::lo + off) = *(uint4 *)l;
+}
+
+struct TcNearArgs {
+  const float2 *x, *g;
+  int64_t gstride;
+  int mode;
+  const int *active;
+  const float2 *loc_leaf;  // per-RHS stride mp
+  size_t mp;
+  int ns;
+  const uint8_t *B;  // stages: 36 near + nl2p basis
+  int nl2p;          // L2P stages
+  float inv_w, inv_b;  // 1 / weight scales
+  float2 *y;
+  int epi, red;
+  const float2 *dot_a;
+  double *part;
+  int nleaf, U, tiles_x, tiles;
+  int *err;
+};
+
+__global__ void __launch_bounds__(256, 1) k_tc_near(TcNearArgs A) {
+  extern __shared__ __align__(1024) char sm[];
+  const int rhs = blockIdx.y;
+  if (A.active && !A.active[rhs]) return;
+  uint64_t *full = (uint64_t *)(sm + NearSmem::bars);
+  uint64_t *empty = full + kNB;
+  uint64_t *done = empty + kNB;
+  uint32_t *tslot = (uint32_t *)(sm + NearSmem::misc);
+  float *fscr = (float *)(sm + NearSmem::misc + 16);      // [8]
+  float *scales = (float *)(sm + NearSmem::misc + 48);    // [2]
+  double *dscr = (double *)(sm + NearSmem::misc + 64);    // [8][3]
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int tile = blockIdx.x;
+  const int ty0 = (tile / A.tiles_x) * kTY, tx0 = (tile % A.tiles_x) * kTX;
+  const size_t rbase = (size_t)rhs * A.U;
+  const float2 *gr = A.g ? A.g + rhs * A.gstride : nullptr;
+  const int nstages = kNearStages + A.nl2p;
+
+  if (threadIdx.x == 0) {
+    for (int b = 0; b < kNB; b++) {
+      mbar_init(&full[b], 1);
+      mbar_init(&empty[b], 1);
+    }
+    mbar_init(done, 1);
+    fence_mbar_init();
+  }
+  if (warp == 0) tmem_alloc(tslot, 256);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+
+  if (warp == 1) {
+    // ---- producer: weight stages through the ring ----
+    if (lane == 0) {
+      for (int t = 0; t < nstages; t++) {
+        const int b = t % kNB;
+        if (t >= kNB && !mbar_wait(&empty[b], ((t / kNB) - 1) & 1, A.err, kErrNearEmpty)) break;
+        mbar_expect_tx(&full[b], kStageBytes);
+        bulk_g2s(sm + NearSmem::stages + b * kStageBytes, A.B + (size_t)t * kStageBytes, kStageBytes, &full[b]);
+      }
+    }
+  } else {
+    // ---- loaders: halo of the transformed input, FP16 hi/lo ----
+    const int li = loader_id();
+    constexpr int kItems = kHR * kHC * 16;  // (halo leaf, 4-pixel chunk)
+    constexpr int kPer = (kItems + kLoaders - 1) / kLoaders;
+    float2 v[kPer][4];
+    float mx = 0.f;
+#pragma unroll
+    for (int r = 0; r < kPer; r++) {
+      const int it = li + r * kLoaders;
+#pragma unroll
+      for (int p = 0; p < 4; p++) v[r][p] = make_float2(0.f, 0.f);
+      if (it < kItems) {
+        const int h = it >> 4, c = it & 15;
+        const int ly = ty0 - 1 + h / kHC, lx = tx0 - 1 + h % kHC;
+        if (ly >= 0 && ly < A.nleaf && lx >= 0 && lx < A.nleaf) {
+          const size_t i = (size_t)(ly * A.nleaf + lx) * kBB + 4 * c;
+          const float4 a0 = *(const float4 *)(A.x + rbase + i), a1 = *(const float4 *)(A.x + rbase + i + 2);
+          float4 g0 = make_float4(0.f, 0.f, 0.f, 0.f), g1 = g0;
+          if (A.mode == IN_G) {
+            g0 = *(const float4 *)(gr + i);
+            g1 = *(const float4 *)(gr + i + 2);
+          }
+          v[r][0] = transform(make_float2(a0.x, a0.y), make_float2(g0.x, g0.y), A.mode);
+          v[r][1] = transform(make_float2(a0.z, a0.w), make_float2(g0.z, g0.w), A.mode);
+          v[r][2] = transform(make_float2(a1.x, a1.y), make_float2(g1.x, g1.y), A.mode);
+          v[r][3] = transform(make_float2(a1.z, a1.w), make_float2(g1.z, g1.w), A.mode);
+#pragma unroll
+          for (int p = 0; p < 4; p++) mx = fmaxf(mx, cabs1(v[r][p]));
+        }
+      }
+    }
+    const float s1 = pow2_scale(loaders_max(mx, fscr));
+#pragma unroll
+    for (int r = 0; r < kPer; r++) {
+      const int it = li + r * kLoaders;
+      if (it < kItems) {
+        const int h = it >> 4, c = it & 15;
+        store_chunk(sm, (h / kHC) * kSboA + c * kLboA + (h % kHC) * 16, v[r], s1);
+      }
+    }
+    if (li == 0) scales[0] = s1;
+    fence_proxy_async();
+    loaders_bar();
+
+    // ---- MMA issue: near field into D1 = columns [0, 128) ----
+    const uint32_t idesc = idesc_f16_f32(128, 128);
+    const uint32_t sbase = smem_u32(sm);
+    if (threadIdx.x == 0) {
+      tc_fence_after();
+      for (int t = 0; t < kNearStages; t++) {
+        const int b = t % kNB;
+        if (!mbar_wait(&full[b], (t / kNB) & 1, A.err, kErrNearFull)) break;
+        const int s = t >> 2, c = t & 3, dr = s / 3 - 1, dc = s % 3 - 1;
+        const uint32_t abase = (1 + dr) * kSboA + (1 + dc) * 16;
+        const uint32_t bst = sbase + NearSmem::stages + b * kStageBytes;
+#pragma unroll
+        for (int ks = 0; ks < 2; ks++) {
+          const uint32_t aoff = abase + (uint32_t)(c * 4 + ks * 2) * kLboA;
+          const uint64_t ahi = smem_desc(sbase + NearSmem::hi + aoff, kLboA, kSboA);
+          const uint64_t alo = smem_desc(sbase + NearSmem::lo + aoff, kLboA, kSboA);
+          const uint64_t bhi = smem_desc(bst + ks * 256, 128, 512);
+          const uint64_t blo = smem_desc(bst + kStageHalf + ks * 256, 128, 512);
+          mma_f16(tmem, ahi, bhi, idesc, (t | ks) ? 1 : 0);
+          mma_f16(tmem, ahi, blo, idesc, 1);
+          mma_f16(tmem, alo, bhi, idesc, 1);
+        }
+        mma_commit(&empty[b]);
+      }
+      mma_commit(done);
+    }
+
+    // ---- L2P operand: leaf locals of the tile, once the near MMAs are done ----
+    constexpr int kLItems = 128 * kLocChunksMax;
+    constexpr int kLPer = (kLItems + kLoaders - 1) / kLoaders;
+    const int nchunk = (A.ns + 3) / 4;
+    float2 w[kLPer][4];
+    float mx2 = 0.f;
+    const float2 *lr = A.loc_leaf + (size_t)rhs * A.mp;
+#pragma unroll
+    for (int r = 0; r < kLPer; r++) {
+      const int it = li + r * kLoaders;
+#pragma unroll
+      for (int p = 0; p < 4; p++) w[r][p] = make_float2(0.f, 0.f);
+      if (it < kLItems) {
+        const int m = it / kLocChunksMax, c = it % kLocChunksMax;
+        const int ly = ty0 + m / kTX, lx = tx0 + m % kTX;
+        if (c < nchunk && ly < A.nleaf && lx < A.nleaf) {
+          const float2 *src = lr + (size_t)(ly * A.nleaf + lx) * A.ns + 4 * c;
+#pragma unroll
+          for (int p = 0; p < 4; p++)
+            if (4 * c + p < A.ns) w[r][p] = src[p];
+#pragma unroll
+          for (int p = 0; p < 4; p++) mx2 = fmaxf(mx2, cabs1(w[r][p]));
+        }
+      }
+    }
+    const float s2 = pow2_scale(loaders_max(mx2, fscr));
+    if (!mbar_wait(done, 0, A.err, kErrNearDone)) {
+      // leave the operand region untouched; the result is flagged
+    } else {
+#pragma unroll
+      for (int r = 0; r < kLPer; r++) {
+        const int it = li + r * kLoaders;
+        if (it < kLItems) {
+          const int m = it / kLocChunksMax, c = it % kLocChunksMax;
+          store_chunk(sm, (m >> 3) * kSboL + c * 128 + (m & 7) * 16, w[r], s2);
+        }
+      }
+    }
+    if (li == 0) scales[1] = s2;
+    fence_proxy_async();
+    loaders_bar();
+    if (threadIdx.x == 0) {
+      tc_fence_after();
+      for (int t = kNearStages; t < nstages; t++) {
+        const int b = t % kNB;
+        if (!mbar_wait(&full[b], (t / kNB) & 1, A.err, kErrNearFull)) break;
+        const int c = t - kNearStages;
+        const uint32_t bst = sbase + NearSmem::stages + b * kStageBytes;
+#pragma unroll
+        for (int ks = 0; ks < 2; ks++) {
+          const uint32_t aoff = (uint32_t)(c * 4 + ks * 2) * 128;
+          const uint64_t ahi = smem_desc(sbase + NearSmem::hi + aoff, 128, kSboL);
+          const uint64_t alo = smem_desc(sbase + NearSmem::lo + aoff, 128, kSboL);
+          const uint64_t bhi = smem_desc(bst + ks * 256, 128, 512);
+          const uint64_t blo = smem_desc(bst + kStageHalf + ks * 256, 128, 512);
+          mma_f16(tmem + 128, ahi, bhi, idesc, (c | ks) ? 1 : 0);
+          mma_f16(tmem + 128, ahi, blo, idesc, 1);
+          mma_f16(tmem + 128, alo, bhi, idesc, 1);
+        }
+        mma_commit(&empty[b]);
+      }
+      mma_commit(done);
+    }
+  }
+
+  // ---- epilogue (all warps) ----
+  const bool ok = mbar_wait(done, 1, A.err, kErrNearDone);
+  __syncthreads();
+  tc_fence_after();
+  const float inv1 = A.inv_w / scales[0], inv2 = A.inv_b / scales[1];
+  const int q = warp & 3, hh = warp >> 2;
+  const int m = 32 * q + lane;
+  const int ly = ty0 + m / kTX, lx = tx0 + m % kTX;
+  const bool valid = ok && ly < A.nleaf && lx < A.nleaf;
+  const size_t leafbase = rbase + (size_t)(ly * A.nleaf + lx) * kBB;
+  double r0 = 0, r1 = 0, r2 = 0;
+  for (int ch = 0; ch < 4; ch++) {
+    const int col = 64 * hh + 16 * ch;
+    float d1[16], d2[16];
+    tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + col, d1);
+    tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + 128 + col, d2);
+    if (!valid) continue;
+#pragma unroll
+    for (int p = 0; p < 8; p += 2) {
+      const int t0 = col / 2 + p;  // complex pixel
+      float2 o[2];
+#pragma unroll
+      for (int e = 0; e < 2; e++)
+        o[e] = make_float2(d1[2 * (p + e)] * inv1 + d2[2 * (p + e)] * inv2,
+                           d1[2 * (p + e) + 1] * inv1 + d2[2 * (p + e) + 1] * inv2);
+      const size_t i = leafbase + t0;
+      float2 xin[2] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+      if (A.epi == EPI_FWD || A.epi == EPI_ADJ || A.red == RED_TS) {
+        const float4 xv = *(const float4 *)(A.x + i);
+        xin[0] = make_float2(xv.x, xv.y);
+        xin[1] = make_float2(xv.z, xv.w);
+      }
+      if (A.epi == EPI_FWD) {
+        o[0] = csub(xin[0], o[0]);
+        o[1] = csub(xin[1], o[1]);
+      } else if (A.epi == EPI_ADJ) {
+        const float4 gv = *(const float4 *)(gr + (i - rbase));
+        o[0] = csub(xin[0], cconj(cmul(make_float2(gv.x, gv.y), o[0])));
+        o[1] = csub(xin[1], cconj(cmul(make_float2(gv.z, gv.w), o[1])));
+      } else if (A.epi == EPI_CONJ) {
+        o[0] = cconj(o[0]);
+        o[1] = cconj(o[1]);
+      }
+      *(float4 *)(A.y + i) = make_float4(o[0].x, o[0].y, o[1].x, o[1].y);
+      if (A.red == RED_DOT) {
+        const float4 av = *(const float4 *)(A.dot_a + i);
+        const float2 a0 = make_float2(av.x, av.y), a1 = make_float2(av.z, av.w);
+        r0 += (double)a0.x * o[0].x + (double)a0.y * o[0].y + (double)a1.x * o[1].x + (double)a1.y * o[1].y;
+        r1 += (double)a0.x * o[0].y - (double)a0.y * o[0].x + (double)a1.x * o[1].y - (double)a1.y * o[1].x;
+      } else if (A.red == RED_TS) {
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+          r0 += (double)o[e].x * xin[e].x + (double)o[e].y * xin[e].y;
+          r1 += (double)o[e].x * xin[e].y - (double)o[e].y * xin[e].x;
+          r2 += (double)o[e].x * o[e].x + (double)o[e].y * o[e].y;
+        }
+      }
+    }
+  }
+  if (A.red != RED_NONE) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      r0 += __shfl_xor_sync(0xffffffffu, r0, o);
+      r1 += __shfl_xor_sync(0xffffffffu, r1, o);
+      r2 += __shfl_xor_sync(0xffffffffu, r2, o);
+    }
+    if (lane == 0) {
+      dscr[warp * 3 + 0] = r0;
+      dscr[warp * 3 + 1] = r1;
+      dscr[warp * 3 + 2] = r2;
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (A.red != RED_NONE && threadIdx.x == 0) {
+    double s0 = 0, s1 = 0, s2 = 0;
+    for (int w2 = 0; w2 < 8; w2++) {
+      s0 += dscr[w2 * 3 + 0];
+      s1 += dscr[w2 * 3 + 1];
+      s2 += dscr[w2 * 3 + 2];
+    }
+    double *p = A.part + ((size_t)rhs * A.tiles + tile) * 4;
+    p[0] = s0;
+    p[1] = s1;
+    p[2] = s2;
+    p[3] = 0;
+  }
+  if (warp == 0) tmem_dealloc(tmem, 256);
+}
+
+// ---- P2M: 128 consecutive leaves of one RHS per CTA, N = 2 ns padded to 16 ----
+constexpr int kP2mA = 16 * 2048;  // one FP16 split of the [128 x 128] operand
+struct P2mSmem {
+  static constexpr int hi = 0, lo = kP2mA, b = 2 * kP2mA;
+};
+
+struct TcP2mArgs {
+  const float2 *x, *g;
+  int64_t gstride;
+  int mode;
+  const int *active;
+  const uint8_t *B;  // 4 stages of [npad x 32] hi then lo
+  int npad, stage_bytes;
+  float inv_c;
+  float2 *mul_leaf;
+  size_t mp;
+  int ns, nleaves, U;
+  int *err;
+};
+
+__global__ void __launch_bounds__(256, 1) k_tc_p2m(TcP2mArgs A) {
+  extern __shared__ __align__(1024) char sm[];
+  const int rhs = blockIdx.y;
+  if (A.active && !A.active[rhs]) return;
+  const int bbytes = 4 * A.stage_bytes;
+  uint64_t *bar = (uint64_t *)(sm + P2mSmem::b + bbytes);
+  uint64_t *done = bar + 1;
+  uint32_t *tslot = (uint32_t *)(bar + 2);
+  float *fscr = (float *)(bar + 3);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int leaf0 = blockIdx.x * 128;
+  const size_t rbase = (size_t)rhs * A.U;
+  const float2 *gr = A.g ? A.g + rhs * A.gstride : nullptr;
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    mbar_init(done, 1);
+    fence_mbar_init();
+  }
+  if (warp == 0) tmem_alloc(tslot, 256);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+  if (threadIdx.x == 0) {
+    mbar_expect_tx(bar, bbytes);
+    for (int c = 0; c < 4; c++)
+      bulk_g2s(sm + P2mSmem::b + c * A.stage_bytes, A.B + (size_t)c * A.stage_bytes, A.stage_bytes, bar);
+  }
+  // operand: 128 leaves x 16 chunks of 4 pixels
+  constexpr int kPer = 128 * 16 / 256;
+  float2 v[kPer][4];
+  float mx = 0.f;
+#pragma unroll
+  for (int r = 0; r < kPer; r++) {
+    const int it = threadIdx.x + r * 256;
+    const int m = it >> 4, c = it & 15, leaf = leaf0 + m;
+#pragma unroll
+    for (int p = 0; p < 4; p++) v[r][p] = make_float2(0.f, 0.f);
+    if (leaf < A.nleaves) {
+      const size_t i = (size_t)leaf * kBB + 4 * c;
+      const float4 a0 = *(const float4 *)(A.x + rbase + i), a1 = *(const float4 *)(A.x + rbase + i + 2);
+      float4 g0 = make_float4(0.f, 0.f, 0.f, 0.f), g1 = g0;
+      if (A.mode == IN_G) {
+        g0 = *(const float4 *)(gr + i);
+        g1 = *(const float4 *)(gr + i + 2);
+      }
+      v[r][0] = transform(make_float2(a0.x, a0.y), make_float2(g0.x, g0.y), A.mode);
+      v[r][1] = transform(make_float2(a0.z, a0.w), make_float2(g0.z, g0.w), A.mode);
+      v[r][2] = transform(make_float2(a1.x, a1.y), make_float2(g1.x, g1.y), A.mode);
+      v[r][3] = transform(make_float2(a1.z, a1.w), make_float2(g1.z, g1.w), A.mode);
+#pragma unroll
+      for (int p = 0; p < 4; p++) mx = fmaxf(mx, cabs1(v[r][p]));
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if (lane == 0) fscr[warp] = mx;
+  __syncthreads();
+  float m2 = 0.f;
+  for (int q = 0; q < 8; q++) m2 = fmaxf(m2, fscr[q]);
+  const float s = pow2_scale(m2);
+#pragma unroll
+  for (int r = 0; r < kPer; r++) {
+    const int it = threadIdx.x + r * 256;
+    const int m = it >> 4, c = it & 15;
+    __align__(16) __half h[8], l[8];
+#pragma unroll
+    for (int p = 0; p < 4; p++) {
+      split_f16(v[r][p].x * s, h[2 * p], l[2 * p]);
+      split_f16(v[r][p].y * s, h[2 * p + 1], l[2 * p + 1]);
+    }
+    const int off = (m >> 3) * 2048 + c * 128 + (m & 7) * 16;
+    *(uint4 *)(sm + P2mSmem::hi + off) = *(uint4 *)h;
+    *(uint4 *)(sm + P2mSmem::lo + off) = *(uint4 *)l;
+  }
+  fence_proxy_async();
+  __syncthreads();
+  const uint32_t sbase = smem_u32(sm);
+  if (threadIdx.x == 0) {
+    tc_fence_after();
+    if (mbar_wait(bar, 0, A.err, kErrP2m)) {
+      const uint32_t idesc = idesc_f16_f32(128, A.npad);
+      for (int c = 0; c < 4; c++)
+#pragma unroll
+        for (int ks = 0; ks < 2; ks++) {
+          const uint32_t aoff = (uint32_t)(c * 4 + ks * 2) * 128;
+          const uint64_t ahi = smem_desc(sbase + P2mSmem::hi + aoff, 128, 2048);
+          const uint64_t alo = smem_desc(sbase + P2mSmem::lo + aoff, 128, 2048);
+          const uint32_t bst = sbase + P2mSmem::b + c * A.stage_bytes + ks * 256;
+          const uint64_t bhi = smem_desc(bst, 128, 512);
+          const uint64_t blo = smem_desc(bst + A.stage_bytes / 2, 128, 512);
+          mma_f16(tmem, ahi, bhi, idesc, (c | ks) ? 1 : 0);
+          mma_f16(tmem, ahi, blo, idesc, 1);
+          mma_f16(tmem, alo, bhi, idesc, 1);
+        }
+    }
+    mma_commit(done);
+  }
+  const bool ok = mbar_wait(done, 0, A.err, kErrP2m);
+  __syncthreads();
+  tc_fence_after();
+  const float inv = A.inv_c / s;
+  const int q = warp & 3, hh = warp >> 2;
+  const int leaf = leaf0 + 32 * q + lane;
+  const int nchunks = A.npad / 16, c0 = hh ? (nchunks + 1) / 2 : 0, c1 = hh ? nchunks : (nchunks + 1) / 2;
+  float2 *out = A.mul_leaf + (size_t)rhs * A.mp + (size_t)leaf * A.ns;
+  for (int ch = c0; ch < c1; ch++) {
+    float d[16];
+    tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + 16 * ch, d);
+    if (!ok || leaf >= A.nleaves) continue;
+#pragma unroll
+    for (int p = 0; p < 8; p++) {
+      const int k = 8 * ch + p;
+      if (k < A.ns) out[k] = make_float2(d[2 * p] * inv, d[2 * p + 1] * inv);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, 256);
+}
+
+// ---- host: operand construction ----
+
+inline double pow2_scale_host(double maxabs) {
+  if (!(maxabs > 0)) return 1.0;
+  int e;
+  std::frexp(maxabs, &e);
+  return std::ldexp(1.0, 14 - e);
+}
+
+// Writes the [nrows x 32] K-major FP16 core-matrix block of reals(row, k0..k0+31)
+// as hi then lo (each nrows/8 groups x 4 chunks x 8 rows x 8 halves).
+template <class F>
+void pack_stage(std::vector<uint8_t> &buf, size_t at, int nrows, int k0, double scale, F real_at) {
+  const size_t half = (size_t)nrows * 32 * 2;
+  __half *hi = (__half *)(buf.data() + at), *lo = (__half *)(buf.data() + at + half);
+  for (int n = 0; n < nrows; n++)
+    for (int k = 0; k < 32; k++) {
+      const double v = real_at(n, k0 + k) * scale;
+      const __half h = __double2half(v);
+      const __half l = __double2half(v - (double)__half2float(h));
+      const size_t idx = ((size_t)(n / 8) * 4 + k / 8) * 64 + (n % 8) * 8 + (k % 8);
+      hi[idx] = h;
+      lo[idx] = l;
+    }
+}
+
+}  // namespace
+
+struct TcPlan {
+  uint8_t *nearB = nullptr;
+  int nl2p = 0;
+  float inv_w = 1, inv_b = 1;
+  uint8_t *p2mB = nullptr;
+  int npad = 0, p2m_stage = 0;
+  float inv_c = 1;
+  int *err = nullptr;
+  bool ok = false;
+};
+
+bool tc_available(const isg_ctx *c) { return c->tc && c->tc->ok; }
+
+isg_status tc_setup(isg_ctx *c) {
+  int dev = 0, major = 0, minor = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+  cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev);
+  const HostTables &T = c->T;
+  const int ns = T.nsamp[T.L - 1];
+  c->tc = new TcPlan();
+  TcPlan &P = *c->tc;
+  if (major != 10 || ns > 4 * kLocChunksMax || T.nleaf < 1) return ISG_OK;  // engine unavailable, SIMT remains
+  // near field: real embedding of near[slot][t][b]; row n = 2t + d, K = 2b + e
+  auto wreal = [&](int s, int n, int k) {
+    const cd w = T.near[((size_t)s * kBB + n / 2) * kBB + k / 2];
+    const int d = n & 1, e = k & 1;
+    return d == 0 ? (e == 0 ? w.real() : -w.imag()) : (e == 0 ? w.imag() : w.real());
+  };
+  auto breal = [&](int n, int k) {
+    if (k / 2 >= ns) return 0.0;
+    const cd w = T.basis[(size_t)(n / 2) * ns + k / 2];
+    const int d = n & 1, e = k & 1;
+    return d == 0 ? (e == 0 ? w.real() : -w.imag()) : (e == 0 ? w.imag() : w.real());
+  };
+  double mw = 0, mb = 0, mc = 0;
+  for (const cd &v : T.near) mw = std::max(mw, std::max(std::abs(v.real()), std::abs(v.imag())));
+  for (const cd &v : T.basis) mb = std::max(mb, std::max(std::abs(v.real()), std::abs(v.imag())));
+  for (const cd &v : T.coeff) mc = std::max(mc, std::max(std::abs(v.real()), std::abs(v.imag())));
+  const double sw = pow2_scale_host(mw), sb = pow2_scale_host(mb), sc = pow2_scale_host(mc);
+  const int kl = ((2 * ns + 31) / 32) * 32;  // L2P K padded to whole stages
+  P.nl2p = kl / 32;
+  std::vector<uint8_t> nb((size_t)(kNearStages + P.nl2p) * kStageBytes, 0);
+  for (int t = 0; t < kNearStages; t++)
+    pack_stage(nb, (size_t)t * kStageBytes, 128, (t & 3) * 32, sw, [&](int n, int k) { return wreal(t >> 2, n, k); });
+  for (int c2 = 0; c2 < P.nl2p; c2++)
+    pack_stage(nb, (size_t)(kNearStages + c2) * kStageBytes, 128, c2 * 32, sb, breal);
+  P.inv_w = (float)(1.0 / sw);
+  P.inv_b = (float)(1.0 / sb);
+  // P2M: row n = 2k + d over samples (padded to a multiple of 16), K = 2 pixel + e
+  P.npad = ((2 * ns + 15) / 16) * 16;
+  P.p2m_stage = P.npad * 32 * 2 * 2;
+  auto creal = [&](int n, int k) {
+    if (n / 2 >= ns) return 0.0;
+    const cd w = T.coeff[(size_t)(n / 2) * kBB + k / 2];
+    const int d = n & 1, e = k & 1;
+    return d == 0 ? (e == 0 ? w.real() : -w.imag()) : (e == 0 ? w.imag() : w.real());
+  };
+  std::vector<uint8_t> pb((size_t)4 * P.p2m_stage, 0);
+  for (int c2 = 0; c2 < 4; c2++) pack_stage(pb, (size_t)c2 * P.p2m_stage, P.npad, c2 * 32, sc, creal);
+  P.inv_c = (float)(1.0 / sc);
+  isg_status e;
+  if ((e = cuda_check(c, cudaMalloc(&P.nearB, nb.size()), "tc alloc")) != ISG_OK) return e;
+  if ((e = cuda_check(c, cudaMalloc(&P.p2mB, pb.size()), "tc alloc")) != ISG_OK) return e;
+  if ((e = cuda_check(c, cudaMalloc(&P.err, sizeof(int)), "tc alloc")) != ISG_OK) return e;
+  cudaMemcpy(P.nearB, nb.data(), nb.size(), cudaMemcpyHostToDevice);
+  cudaMemcpy(P.p2mB, pb.data(), pb.size(), cudaMemcpyHostToDevice);
+  cudaMemset(P.err, 0, sizeof(int));
+  cudaFuncSetAttribute(k_tc_near, cudaFuncAttributeMaxDynamicSharedMemorySize, NearSmem::total);
+  cudaFuncSetAttribute(k_tc_p2m, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       P2mSmem::b + 4 * P.p2m_stage + 64);
+  if ((e = cuda_check(c, cudaGetLastError(), "tc setup")) != ISG_OK) return e;
+  P.ok = true;
+  return ISG_OK;
+}
+
 void tc_destroy(isg_ctx *c) {
+  if (!c->tc) return;
+  cudaFree(c->tc->nearB);
+  cudaFree(c->tc->p2mB);
+  cudaFree(c->tc->err);
   delete c->tc;
   c->tc = nullptr;
 }
-bool tc_available(const isg_ctx *c) { return c->tc != nullptr; }
-isg_status tc_p2m(isg_ctx *, const BatchArgs &, float2 *, cudaStream_t) { return ISG_UNSUPPORTED; }
-isg_status tc_near(isg_ctx *, const NearArgs &, cudaStream_t) { return ISG_UNSUPPORTED; }
+
+int tc_error(isg_ctx *c) {
+  if (!tc_available(c)) return 0;
+  int h = 0;
+  cudaMemcpy(&h, c->tc->err, sizeof(int), cudaMemcpyDeviceToHost);
+  return h;
+}
+
+static bool aligned16(const void *p) { return ((uintptr_t)p & 15) == 0; }
+
+isg_status tc_near(isg_ctx *c, const NearArgs &N, cudaStream_t st) {
+  const DevPlan &P = c->P;
+  const TcPlan &T = *c->tc;
+  if (!aligned16(N.in.x) || (N.in.g && !aligned16(N.in.g)) || !aligned16(N.y) || (N.dot_a && !aligned16(N.dot_a)) ||
+      (N.in.gstride % 2) || N.epi == EPI_L2P_ONLY)
+    return ISG_UNSUPPORTED;
+  TcNearArgs A;
+  A.x = N.in.x;
+  A.g = N.in.g;
+  A.gstride = N.in.gstride;
+  A.mode = N.in.mode;
+  A.active = N.in.active;
+  A.loc_leaf = N.loc + P.lv[P.L - 1].off;
+  A.mp = P.mp;
+  A.ns = P.ns_leaf;
+  A.B = T.nearB;
+  A.nl2p = T.nl2p;
+  A.inv_w = T.inv_w;
+  A.inv_b = T.inv_b;
+  A.y = N.y;
+  A.epi = N.epi;
+  A.red = N.red;
+  A.dot_a = N.dot_a;
+  A.part = N.part;
+  A.nleaf = P.nleaf;
+  A.U = P.U;
+  A.tiles_x = (P.nleaf + kTX - 1) / kTX;
+  A.tiles = A.tiles_x * ((P.nleaf + kTY - 1) / kTY);
+  A.err = T.err;
+  count_launch();
+  k_tc_near<<<dim3(A.tiles, N.in.nrhs), 256, NearSmem::total, st>>>(A);
+  return cuda_check(c, cudaGetLastError(), "tc near launch");
+}
+
+isg_status tc_p2m(isg_ctx *c, const BatchArgs &B, float2 *mul, cudaStream_t st) {
+  const DevPlan &P = c->P;
+  const TcPlan &T = *c->tc;
+  if (!aligned16(B.x) || (B.g && !aligned16(B.g)) || (B.gstride % 2)) return ISG_UNSUPPORTED;
+  TcP2mArgs A;
+  A.x = B.x;
+  A.g = B.g;
+  A.gstride = B.gstride;
+  A.mode = B.mode;
+  A.active = B.active;
+  A.B = T.p2mB;
+  A.npad = T.npad;
+  A.stage_bytes = T.p2m_stage;
+  A.inv_c = T.inv_c;
+  A.mul_leaf = mul + P.lv[P.L - 1].off;
+  A.mp = P.mp;
+  A.ns = P.ns_leaf;
+  A.nleaves = P.nleaf * P.nleaf;
+  A.U = P.U;
+  A.err = T.err;
+  count_launch();
+  k_tc_p2m<<<dim3((A.nleaves + 127) / 128, B.nrhs), 256, P2mSmem::b + 4 * T.p2m_stage + 64, st>>>(A);
+  return cuda_check(c, cudaGetLastError(), "tc p2m launch");
+}
 
 }  // namespace isg

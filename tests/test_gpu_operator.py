@@ -31,7 +31,10 @@ def case(request):
     return d, s
 
 
-@pytest.mark.parametrize("engine", [isg.ENGINE_SIMT])
+ENGINES = [isg.ENGINE_SIMT, isg.ENGINE_TENSOR]
+
+
+@pytest.mark.parametrize("engine", ENGINES)
 def test_mlfma_matches_reference(case, engine):
     d, s = case
     x = torch_dev(d["x"])
@@ -45,12 +48,13 @@ def test_mlfma_against_dense_rows(case):
     assert rel(r[d["dense_rows"]], d["dense"]) < 3e-5
 
 
-def test_matvec_forward_and_adjoint(case):
+@pytest.mark.parametrize("engine", ENGINES)
+def test_matvec_forward_and_adjoint(case, engine):
     d, s = case
     o = Oracle(int(d["level"]), numrx=int(d["numrx"]))
     x, g = d["x"], d["g"]
     for h in (False, True):
-        y = host(s.matvec(torch_dev(x), torch_dev(g), hermitian=h))
+        y = host(s.matvec(torch_dev(x), torch_dev(g), hermitian=h, engine=engine))
         assert rel(y, o.matvec(x, g, h)) < TOL
 
 
@@ -109,3 +113,25 @@ def test_smallest_grid_level3():
     assert rel(host(s.mlfma(torch_dev(x))), o.mlfma(x)) < TOL
     g = disk_contrast(o.pos(), radius=0.8)
     assert rel(host(s.matvec(torch_dev(x), torch_dev(g), hermitian=True)), o.matvec(x, g, True)) < TOL
+
+
+@pytest.mark.parametrize("level", [3, 6, 7])
+def test_tensor_engine_matches_simt(level):
+    """3xFP16 tcgen05 leaf stages agree with complex-FP32 SIMT on random batches,
+    including the tile edges of grids smaller than one 16 x 8 leaf tile."""
+    s = isg.Solver(level, max_rhs=3)
+    rng = np.random.default_rng(level)
+    U = s.numunk
+    X = rng.standard_normal((3, U)) + 1j * rng.standard_normal((3, U))
+    X[1] *= 1e-3  # per-tile scaling must follow the magnitude
+    G = (rng.standard_normal(U) + 1j * rng.standard_normal(U)) * 10
+    xs, gs = torch_dev(X), torch_dev(G)
+    for h in (False, True):
+        a = host(s.matvec(xs, gs, hermitian=h, engine=isg.ENGINE_SIMT, order=isg.ORDER_BLOCKED))
+        b = host(s.matvec(xs, gs, hermitian=h, engine=isg.ENGINE_TENSOR, order=isg.ORDER_BLOCKED))
+        for j in range(3):
+            assert rel(b[j], a[j]) < 5e-6, (h, j, rel(b[j], a[j]))
+    a = host(s.mlfma(xs, engine=isg.ENGINE_SIMT))
+    b = host(s.mlfma(xs, engine=isg.ENGINE_TENSOR))
+    for j in range(3):
+        assert rel(b[j], a[j]) < 5e-6

@@ -24,15 +24,16 @@ def host(t):
     return t.detach().cpu().numpy().astype(np.complex128)
 
 
+@pytest.mark.parametrize("engine", [isg.ENGINE_SIMT, isg.ENGINE_TENSOR])
 @pytest.mark.parametrize("name", ["golden_l4.npz", "golden_l5.npz"])
 @pytest.mark.parametrize("hermitian", [False, True])
-def test_bicgs_matches_reference(name, hermitian):
+def test_bicgs_matches_reference(name, hermitian, engine):
     d = dict(np.load(os.path.join(GOLDEN, name)))
     s = isg.Solver(int(d["level"]), numrx=int(d["numrx"]))
     o = Oracle(int(d["level"]), numrx=int(d["numrx"]))
     g, b = d["g"], d["b"]
     x = torch_dev(np.zeros_like(b))
-    info = s.bicgs(x, torch_dev(g), torch_dev(b), hermitian=hermitian, tol=1e-5)[0]
+    info = s.bicgs(x, torch_dev(g), torch_dev(b), hermitian=hermitian, tol=1e-5, engine=engine)[0]
     assert info["status"] == 0, info
     assert info["true_residual"] <= 1e-5
     ref_iters = int(d["bicgs_adj_iters" if hermitian else "bicgs_fwd_iters"])
