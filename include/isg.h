@@ -148,6 +148,42 @@ isg_status isg_aggregate(isg_ctx *ctx, const void *x, void *rx, int nrhs, int or
  * solve.cpp:356-456), all levels on the device. */
 isg_status isg_aggregateh(isg_ctx *ctx, void *x, const void *rx, int nrhs, int order, isg_stream stream);
 
+/* ---- inversion (distorted-Born / Polak-Ribiere nonlinear CG, mom.cpp:222-399) ---- */
+typedef struct isg_dbim_opts {
+  int iterations;        /* Polak-Ribiere iterations (mom.cpp:277 runs 3) */
+  double regular;        /* Tikhonov weight; adds regular^2 chi per transmitter (mom.cpp:32,268-269) */
+  int start_from_chi;    /* 0: chi = 0 and total field = incident (mom.cpp:225-229);
+                            1: start from the caller's chi (the reference's commented restart, mom.cpp:230-245) */
+  isg_solve_opts solve;  /* inner BiCGSTAB options (tol: mom.cpp:21) */
+} isg_dbim_opts;
+
+typedef struct isg_dbim_record {
+  double misfit;         /* sum |mesd|^2 / sum |mes|^2            (setup_born.cpp:239-240) */
+  double object_error;   /* sum |chi - chi_true|^2 / sum |chi_true|^2, or -1 without chi_true */
+  double reg_cost;       /* sum |regular chi|^2 / sum |mes|^2 */
+  double grad_norm;      /* sum |gradient|^2 */
+  double object_norm;    /* sum |chi|^2 */
+  double alpha;          /* step length of the iteration (mom.cpp:315); 0 in record 0 */
+  double beta_re, beta_im; /* Polak-Ribiere coefficient (mom.cpp:394) */
+  int64_t solves;        /* BiCGSTAB solves so far */
+  int64_t iterations;    /* BiCGSTAB iterations so far */
+} isg_dbim_record;
+
+void isg_default_dbim_opts(isg_dbim_opts *o);
+/* Synthetic measurements (setup_born.cpp:139-149): per transmitter a forward
+ * solve with g = k0^2 chi, then the far-field pattern of g u.  inc: ntx
+ * complex64 fields in `order`; chi: complex128 contrast eps_r - 1 in `order`;
+ * mes: ntx x numrx complex64.  noise > 0 adds complex Gaussian noise of
+ * standard deviation noise * ||mes|| / sqrt(2 ntx numrx) per real component. */
+isg_status isg_measure(isg_ctx *ctx, int ntx, const void *inc, const double *chi, int order, double noise,
+                       uint64_t seed, const isg_solve_opts *solve, void *mes, isg_stream stream);
+/* The inversion loop: gradient by adjoint solves, Born-linearised step
+ * length, contrast update, total-field re-solve, Polak-Ribiere direction, all
+ * transmitters batched (chunks of max_rhs).  chi (complex128, in/out) and
+ * chi_true (optional) are in `order`; hist receives iterations + 1 records. */
+isg_status isg_dbim(isg_ctx *ctx, int ntx, const void *inc, const void *mes, const double *chi_true, double *chi,
+                    int order, const isg_dbim_opts *opts, isg_dbim_record *hist, isg_stream stream);
+
 /* ---- measurement ---- */
 /* Number of CUDA kernels this library has launched in the process so far. */
 int64_t isg_kernel_launches(void);

@@ -20,6 +20,36 @@ isg_status cuda_check(isg_ctx *c, cudaError_t e, const char *what) {
   return ISG_CUDA_ERROR;
 }
 
+const int *order_perm(const isg_ctx *c, int order) {
+  return order == ISG_ORDER_TREE ? c->P.perm_tree : (order == ISG_ORDER_RASTER ? c->P.perm_raster : nullptr);
+}
+
+// solve.cpp:249-355: P2M, M2M up to the root, interpolation to the receivers.
+isg_status run_aggregate(isg_ctx *c, const float2 *xb, float2 *rx, int nrhs, cudaStream_t st) {
+  BatchArgs B;
+  B.x = xb;
+  B.nrhs = nrhs;
+  launch_p2m(c->P, B, c->mul, st);
+  for (int i = c->P.L - 2; i >= 0; i--) launch_m2m(c->P, i, c->mul, nrhs, nullptr, st);
+  launch_rx_interp(c->P, c->mul, rx, nrhs, st);
+  return cuda_check(c, cudaGetLastError(), "aggregate");
+}
+
+// solve.cpp:356-456: anterpolation from the receivers times (-4i) numrx res^2,
+// L2L down to the leaves (overwriting), L2P.
+isg_status run_aggregateh(isg_ctx *c, float2 *xb, const float2 *rx, int nrhs, cudaStream_t st) {
+  const float scale = (float)(-4.0 * c->T.numrx * c->T.res * c->T.res);
+  launch_rx_anterp(c->P, rx, c->loc, nrhs, make_float2(0.f, scale), st);
+  for (int i = 1; i < c->P.L; i++) launch_l2l(c->P, i, c->loc, nrhs, nullptr, false, st);
+  NearArgs A;
+  A.in.nrhs = nrhs;
+  A.loc = c->loc;
+  A.y = xb;
+  A.epi = EPI_L2P_ONLY;
+  launch_near(c->P, A, st);
+  return cuda_check(c, cudaGetLastError(), "aggregateh");
+}
+
 }  // namespace isg
 
 namespace {
@@ -418,13 +448,7 @@ isg_status isg_aggregate(isg_ctx *c, const void *x, void *rx, int nrhs, int orde
   if (e != ISG_OK) return e;
   if (!x || !rx || bad_order(order) || (e = check_batch(c, nrhs)) != ISG_OK) return ISG_BAD_ARG;
   cudaStream_t st = pick(c, stream);
-  BatchArgs B;
-  B.x = to_blocked(c, x, c->wx, nrhs, order, st);
-  B.nrhs = nrhs;
-  launch_p2m(c->P, B, c->mul, st);
-  for (int i = c->P.L - 2; i >= 0; i--) launch_m2m(c->P, i, c->mul, nrhs, nullptr, st);
-  launch_rx_interp(c->P, c->mul, (float2 *)rx, nrhs, st);
-  return cuda_check(c, cudaGetLastError(), "aggregate");
+  return run_aggregate(c, to_blocked(c, x, c->wx, nrhs, order, st), (float2 *)rx, nrhs, st);
 }
 
 isg_status isg_aggregateh(isg_ctx *c, void *x, const void *rx, int nrhs, int order, isg_stream stream) {
@@ -432,16 +456,9 @@ isg_status isg_aggregateh(isg_ctx *c, void *x, const void *rx, int nrhs, int ord
   if (e != ISG_OK) return e;
   if (!x || !rx || bad_order(order) || (e = check_batch(c, nrhs)) != ISG_OK) return ISG_BAD_ARG;
   cudaStream_t st = pick(c, stream);
-  const float scale = (float)(-4.0 * c->T.numrx * c->T.res * c->T.res);
-  launch_rx_anterp(c->P, (const float2 *)rx, c->loc, nrhs, make_float2(0.f, scale), st);
-  for (int i = 1; i < c->P.L; i++) launch_l2l(c->P, i, c->loc, nrhs, nullptr, false, st);
-  NearArgs A;
-  A.in.nrhs = nrhs;
-  A.loc = c->loc;
-  A.y = order == ISG_ORDER_BLOCKED ? (float2 *)x : c->wy;
-  A.epi = EPI_L2P_ONLY;
-  launch_near(c->P, A, st);
-  from_blocked(c, A.y, x, nrhs, order, st);
+  float2 *y = order == ISG_ORDER_BLOCKED ? (float2 *)x : c->wy;
+  if ((e = run_aggregateh(c, y, (const float2 *)rx, nrhs, st)) != ISG_OK) return e;
+  from_blocked(c, y, x, nrhs, order, st);
   return cuda_check(c, cudaGetLastError(), "aggregateh");
 }
 

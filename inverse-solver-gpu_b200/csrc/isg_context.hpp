@@ -58,12 +58,18 @@ isg_status run_matvec(isg_ctx *c, const float2 *x, const float2 *g, int64_t gs, 
 isg_status run_bicgs(isg_ctx *c, float2 *x, const float2 *g, int64_t gs, const float2 *b, int nrhs, int hermitian,
                      const isg_solve_opts *o, isg_solve_info *info, cudaStream_t st);
 isg_status cuda_check(isg_ctx *c, cudaError_t e, const char *what);
+// Receiver projection and back-projection on blocked vectors (isg_capi.cu).
+isg_status run_aggregate(isg_ctx *c, const float2 *xb, float2 *rx, int nrhs, cudaStream_t st);
+isg_status run_aggregateh(isg_ctx *c, float2 *xb, const float2 *rx, int nrhs, cudaStream_t st);
+const int *order_perm(const isg_ctx *c, int order);
 // Tensor-core engine (isg_tc.cu).
 isg_status tc_setup(isg_ctx *c);
 void tc_destroy(isg_ctx *c);
 bool tc_available(const isg_ctx *c);
 isg_status tc_p2m(isg_ctx *c, const BatchArgs &B, float2 *mul, cudaStream_t st);
 isg_status tc_near(isg_ctx *c, const NearArgs &A, cudaStream_t st);
+// Per-RHS partial sums written by tc_near (one per tile).
+int tc_near_blocks(const isg_ctx *c);
 // Nonzero when a bounded wait inside a tensor-core kernel gave up.
 int tc_error(isg_ctx *c);
 }  // namespace isg

@@ -153,9 +153,37 @@ __device__ __forceinline__ void m2l_issue(const M2lArgs &A, int item, int k0, fl
   }
 }
 
+// One window step: rows of the 6x6 window live in six register slots that
+// rotate by two per step (ROT = step mod 3), so no registers are moved.
+template <int OY, int OX, int ROT>
+__device__ __forceinline__ void m2l_step(const float2 (*hs)[kM2lHC][kM2lKC], float2 (&w)[6][6],
+                                         const float2 (&tw)[6][6], int a, int b, int kk, int cy0, int cx0,
+                                         bool live, const M2lArgs &A, int k, float2 *out) {
+  constexpr int NR0 = OY + 1, NC0 = OX + 1;  // first near row/column inside the window
+#pragma unroll
+  for (int j = 0; j < 6; j++) {
+    w[(4 + 2 * ROT) % 6][j] = hs[2 * a + 4][2 * b + j][kk];
+    w[(5 + 2 * ROT) % 6][j] = hs[2 * a + 5][2 * b + j][kk];
+  }
+  float2 acc[3] = {};
+  int term = 0;
+#pragma unroll
+  for (int i = 0; i < 6; i++)
+#pragma unroll
+    for (int j = 0; j < 6; j++) {
+      const bool nearby = (i >= NR0 && i < NR0 + 3 && j >= NC0 && j < NC0 + 3);
+      if (nearby) continue;
+      cfma(acc[term % 3], tw[i][j], w[(i + 2 * ROT) % 6][j]);
+      term++;
+    }
+  const int cy = cy0 + 2 * a + OY, cx = cx0 + 2 * b + OX;
+  if (live && cy < A.n && cx < A.n && k < A.ns)
+    out[(size_t)(cy * A.n + cx) * A.ns + k] = cadd(acc[0], cadd(acc[1], acc[2]));
+}
+
 template <int OY, int OX>
 __device__ __forceinline__ void m2l_worker(const M2lArgs &A, float2 *hbuf) {
-  constexpr int NR0 = OY + 1, NC0 = OX + 1;  // first near row/column inside the window
+  constexpr int NR0 = OY + 1, NC0 = OX + 1;
   const int kk = threadIdx.x & 31, b = threadIdx.x >> 7;
   const int k0 = blockIdx.x * kM2lKC, k = k0 + kk;
   float2 tw[6][6];
@@ -179,38 +207,20 @@ __device__ __forceinline__ void m2l_worker(const M2lArgs &A, float2 *hbuf) {
     const bool live = !(A.active && !A.active[rhs]);
     const int cy0 = (tile / A.tiles_x) * kM2lRows, cx0 = (tile % A.tiles_x) * kM2lCols;
     float2 *out = A.loc + (size_t)rhs * A.mp + A.off;
-    // Rows 0..3 of the first window; each step loads two new rows and slides.
     float2 w[6][6];
 #pragma unroll
     for (int i = 0; i < 4; i++)
 #pragma unroll
-      for (int j = 0; j < 6; j++) w[i + 2][j] = hs[i][2 * b + j][kk];
+      for (int j = 0; j < 6; j++) w[i][j] = hs[i][2 * b + j][kk];
+    static_assert(kM2lRows / 2 == 8, "window walk is unrolled for eight steps");
 #pragma unroll 1
-    for (int a = 0; a < kM2lRows / 2; a++) {
-#pragma unroll
-      for (int i = 0; i < 4; i++)
-#pragma unroll
-        for (int j = 0; j < 6; j++) w[i][j] = w[i + 2][j];
-#pragma unroll
-      for (int j = 0; j < 6; j++) {
-        w[4][j] = hs[2 * a + 4][2 * b + j][kk];
-        w[5][j] = hs[2 * a + 5][2 * b + j][kk];
-      }
-      float2 acc[3] = {};
-      int term = 0;
-#pragma unroll
-      for (int i = 0; i < 6; i++)
-#pragma unroll
-        for (int j = 0; j < 6; j++) {
-          const bool nearby = (i >= NR0 && i < NR0 + 3 && j >= NC0 && j < NC0 + 3);
-          if (nearby) continue;
-          cfma(acc[term % 3], tw[i][j], w[i][j]);
-          term++;
-        }
-      const int cy = cy0 + 2 * a + OY, cx = cx0 + 2 * b + OX;
-      if (live && cy < A.n && cx < A.n && k < A.ns)
-        out[(size_t)(cy * A.n + cx) * A.ns + k] = cadd(acc[0], cadd(acc[1], acc[2]));
+    for (int a = 0; a < 6; a += 3) {
+      m2l_step<OY, OX, 0>(hs, w, tw, a, b, kk, cy0, cx0, live, A, k, out);
+      m2l_step<OY, OX, 1>(hs, w, tw, a + 1, b, kk, cy0, cx0, live, A, k, out);
+      m2l_step<OY, OX, 2>(hs, w, tw, a + 2, b, kk, cy0, cx0, live, A, k, out);
     }
+    m2l_step<OY, OX, 0>(hs, w, tw, 6, b, kk, cy0, cx0, live, A, k, out);
+    m2l_step<OY, OX, 1>(hs, w, tw, 7, b, kk, cy0, cx0, live, A, k, out);
     block_bar1();
     buf ^= 1;
   }

@@ -363,9 +363,9 @@ isg_status run_bicgs(isg_ctx *c, float2 *x, const float2 *g, int64_t gs, const f
   const int U = c->P.U;
   const int kind = hermitian ? OP_ADJ : OP_FWD;
   const int nbv = c->vec_blocks;
-  const int nbn = near_blocks_per_rhs(c->P);
   const double tol = o->tol;
   const int engine = o->engine;
+  const int nbn = (engine == ISG_ENGINE_TENSOR && tc_available(c)) ? tc_near_blocks(c) : near_blocks_per_rhs(c->P);
   const int zero_guess = (o->guess == ISG_GUESS_ZERO);
   isg_status e;
   dim3 vgrid(nbv, R);

@@ -631,6 +631,11 @@ void tc_destroy(isg_ctx *c) {
   c->tc = nullptr;
 }
 
+int tc_near_blocks(const isg_ctx *c) {
+  const int tx = (c->P.nleaf + kTX - 1) / kTX, ty = (c->P.nleaf + kTY - 1) / kTY;
+  return tx * ty;
+}
+
 int tc_error(isg_ctx *c) {
   if (!tc_available(c)) return 0;
   int h = 0;

@@ -54,6 +54,21 @@ class SolveInfo(ctypes.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class DbimOpts(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("regular", ctypes.c_double), ("start_from_chi", ctypes.c_int),
+                ("solve", SolveOpts)]
+
+
+class DbimRecord(ctypes.Structure):
+    _fields_ = [("misfit", ctypes.c_double), ("object_error", ctypes.c_double), ("reg_cost", ctypes.c_double),
+                ("grad_norm", ctypes.c_double), ("object_norm", ctypes.c_double), ("alpha", ctypes.c_double),
+                ("beta_re", ctypes.c_double), ("beta_im", ctypes.c_double), ("solves", ctypes.c_int64),
+                ("iterations", ctypes.c_int64)]
+
+    def as_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 class Phantom(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int), ("count", ctypes.c_int), ("axis_min", ctypes.c_double),
                 ("axis_max", ctypes.c_double), ("eps_min", ctypes.c_double), ("eps_max", ctypes.c_double),
@@ -83,6 +98,9 @@ SIGNATURES = {
     "isg_bicgs": (_I, [_P, _P, _P, _L, _P, _I, _I, _I, ctypes.POINTER(SolveOpts), ctypes.POINTER(SolveInfo), _P]),
     "isg_aggregate": (_I, [_P, _P, _P, _I, _I, _P]),
     "isg_aggregateh": (_I, [_P, _P, _P, _I, _I, _P]),
+    "isg_default_dbim_opts": (None, [ctypes.POINTER(DbimOpts)]),
+    "isg_measure": (_I, [_P, _I, _P, _P, _I, _D, ctypes.c_uint64, ctypes.POINTER(SolveOpts), _P, _P]),
+    "isg_dbim": (_I, [_P, _I, _P, _P, _P, _P, _I, ctypes.POINTER(DbimOpts), ctypes.POINTER(DbimRecord), _P]),
     "isg_kernel_launches": (ctypes.c_int64, []),
     "isg_time_stages": (_I, [_P, _I, _I, _I, _P]),
     "isg_make_phantom": (_I, [_P, ctypes.POINTER(Phantom), _P]),
@@ -266,6 +284,34 @@ class Solver:
         out = np.zeros(5)
         self._check(lib().isg_time_stages(self._h, nrhs, engine, reps, out.ctypes.data), "time_stages")
         return dict(zip(("p2m", "m2m", "m2l_l2l", "near", "total"), out.tolist()))
+
+    # ---- inversion ----
+    def measure(self, inc, chi, noise: float = 0.0, seed: int = 0, order: int = ORDER_TREE, stream=None, **solve):
+        """Synthetic far-field data of contrast chi (setup_born.cpp:139-149): (ntx, numrx) complex64."""
+        import torch
+        ntx = 1 if inc.dim() == 1 else inc.shape[0]
+        mes = torch.empty((ntx, self.numrx), dtype=torch.complex64, device=inc.device)
+        so = default_solve_opts(**{"tol": 1e-4, **solve})
+        self._check(lib().isg_measure(self._h, ntx, _ptr(inc), _ptr(chi), order, noise, seed, ctypes.byref(so),
+                                      _ptr(mes), _stream(stream)), "measure")
+        return mes
+
+    def dbim(self, inc, mes, chi=None, chi_true=None, iterations: int = 3, regular: float = 0.0,
+             order: int = ORDER_TREE, start_from_chi: bool = False, stream=None, **solve):
+        """The reference's inversion loop (mom.cpp:222-399); returns (chi, history records)."""
+        import torch
+        ntx = 1 if inc.dim() == 1 else inc.shape[0]
+        if chi is None:
+            chi = torch.zeros(self.numunk, dtype=torch.complex128, device=inc.device)
+        o = DbimOpts()
+        lib().isg_default_dbim_opts(ctypes.byref(o))
+        o.iterations, o.regular, o.start_from_chi = iterations, regular, int(start_from_chi)
+        for k, v in solve.items():
+            setattr(o.solve, k, v)
+        hist = (DbimRecord * (iterations + 1))()
+        self._check(lib().isg_dbim(self._h, ntx, _ptr(inc), _ptr(mes), _ptr(chi_true), _ptr(chi), order,
+                                   ctypes.byref(o), hist, _stream(stream)), "dbim")
+        return chi, [h.as_dict() for h in hist]
 
     def reorder(self, x, frm: int, to: int, out=None, stream=None):
         out = self._empty_like(x) if out is None else out

@@ -660,7 +660,12 @@ int orc_bicgs(orc_ctx *c, double complex *x, const double complex *g, const doub
       alpha = rho / inner(rt, v, U);
       for (int n = 0; n < U; n++) s[n] = r[n] - alpha * v[n];
       orc_matvec(c, s, g, t, hermitian);
-      omega = inner(t, s, U) / norm2(t, U);
+      /* bicgs.cpp:153, with the guard of the linked GPU solver (bicgs_gpu.cu:
+       * 373-376) for t = s = 0, which the reference's -ffast-math CPU build
+       * also resolves to a finite omega */
+      double complex ts = inner(t, s, U);
+      double tt = norm2(t, U);
+      omega = (cabs(ts) < 1e-200 && tt < 1e-200) ? 1.0 : ts / tt;
       for (int n = 0; n < U; n++) {
         x[n] = x[n] + alpha * p[n] + omega * s[n];
         r[n] = s[n] - omega * t[n];
@@ -704,4 +709,144 @@ void orc_aggregateh(orc_ctx *c, double complex *x, const double complex *rx) {
   }
   for (int i = 0; i < L - 1; i++) l2l(c, i, 1);
   l2p(c, x);
+}
+
+/* One write_error record (setup_born.cpp:593-664). */
+static void dbim_record(const orc_ctx *c, int ntx, const double complex *mesd, const double complex *od,
+                        const double complex *o, const double complex *otrue, double regular, double mesnorm,
+                        double objnorm, double *rec) {
+  int U = c->U;
+  double err = 0, errd = 0, obj = 0, objn = 0, errm = 0;
+  for (int m = 0; m < ntx * c->numrx; m++) err += creal(mesd[m] * conj(mesd[m]));
+  for (int n = 0; n < U; n++) {
+    errd += creal(od[n] * conj(od[n]));
+    double complex ro = regular * o[n];
+    obj += creal(ro * conj(ro));
+    objn += creal(o[n] * conj(o[n]));
+    double complex d = o[n] - otrue[n];
+    errm += creal(d * conj(d));
+  }
+  rec[0] = err / mesnorm;
+  rec[1] = errm / objnorm;
+  rec[2] = obj / mesnorm;
+  rec[3] = errd;
+  rec[4] = objn;
+}
+
+/* mom.cpp:247-271 (and 338-362): gradient od of the misfit at contrast o. */
+static void dbim_gradient(orc_ctx *c, int ntx, const double complex *o, const double complex *tot,
+                          const double complex *mesd, double regular, double tol, int maxit, double complex *od) {
+  int U = c->U;
+  double k2 = c->k0 * c->k0;
+  double complex *y = malloc(U * sizeof(double complex)), *cc = malloc(U * sizeof(double complex));
+  double complex *g = malloc(U * sizeof(double complex)), *x = malloc(U * sizeof(double complex));
+  for (int n = 0; n < U; n++) od[n] = 0;
+  for (int i = 0; i < ntx; i++) {
+    orc_aggregateh(c, y, &mesd[i * c->numrx]);
+    for (int n = 0; n < U; n++) {
+      cc[n] = conj(o[n] * k2) * y[n];
+      g[n] = o[n] * k2;
+      x[n] = 0;
+    }
+    orc_bicgs(c, x, g, cc, 1, tol, maxit, NULL);
+    orc_mlfmah(c, x, cc);
+    for (int n = 0; n < U; n++) {
+      y[n] += cc[n];
+      od[n] += conj(tot[(size_t)i * U + n]) * y[n];
+      od[n] += regular * regular * o[n];
+    }
+  }
+  free(y);
+  free(cc);
+  free(g);
+  free(x);
+}
+
+int orc_dbim(orc_ctx *c, int ntx, const double complex *inc, const double complex *chi_true, int iterations,
+             double regular, double tol, int maxit, double complex *o, double *hist, double *alpha,
+             double complex *beta) {
+  int U = c->U, nr = c->numrx;
+  double k2 = c->k0 * c->k0;
+  size_t fb = (size_t)ntx * U * sizeof(double complex), mb = (size_t)ntx * nr * sizeof(double complex);
+  double complex *tot = malloc(fb), *mes = malloc(mb), *mesd = malloc(mb), *rhs = malloc(mb);
+  double complex *od = malloc(U * sizeof(double complex)), *ot = malloc(U * sizeof(double complex));
+  double complex *save = malloc(U * sizeof(double complex)), *g = malloc(U * sizeof(double complex));
+  double complex *x = malloc(U * sizeof(double complex)), *y = malloc(U * sizeof(double complex));
+  double complex *cc = malloc(U * sizeof(double complex));
+  /* setup_born.cpp:139-149: measurements of the true contrast */
+  for (int n = 0; n < U; n++) g[n] = chi_true[n] * k2;
+  for (int i = 0; i < ntx; i++) {
+    for (int n = 0; n < U; n++) x[n] = 0;
+    orc_bicgs(c, x, g, &inc[(size_t)i * U], 0, tol, maxit, NULL);
+    for (int n = 0; n < U; n++) x[n] *= g[n];
+    orc_aggregate(c, x, &mes[i * nr]);
+  }
+  double objnorm = 0, mesnorm = 0;
+  for (int n = 0; n < U; n++) objnorm += creal(chi_true[n] * conj(chi_true[n]));
+  for (int m = 0; m < ntx * nr; m++) mesnorm += creal(mes[m] * conj(mes[m]));
+  /* mom.cpp:224-229: no object, total field = incident */
+  for (int n = 0; n < U; n++) o[n] = 0;
+  memcpy(tot, inc, fb);
+  for (int m = 0; m < ntx * nr; m++) mesd[m] = -mes[m];
+  dbim_gradient(c, ntx, o, tot, mesd, regular, tol, maxit, od);
+  dbim_record(c, ntx, mesd, od, o, chi_true, regular, mesnorm, objnorm, &hist[0]);
+  memcpy(ot, od, U * sizeof(double complex));
+  for (int it = 0; it < iterations; it++) {
+    /* mom.cpp:280-316: Born-linearised step length */
+    for (int i = 0; i < ntx; i++) {
+      for (int n = 0; n < U; n++) y[n] = tot[(size_t)i * U + n] * ot[n] * k2;
+      orc_mlfma(c, y, cc);
+      for (int n = 0; n < U; n++) {
+        x[n] = 0;
+        g[n] = o[n] * k2;
+      }
+      orc_bicgs(c, x, g, cc, 0, tol, maxit, NULL);
+      for (int n = 0; n < U; n++) y[n] += o[n] * k2 * x[n];
+      orc_aggregate(c, y, &rhs[i * nr]);
+    }
+    double complex t1 = 0;
+    double t2 = 0;
+    for (int m = 0; m < ntx * nr; m++) {
+      t1 += conj(mesd[m]) * rhs[m];
+      t2 += creal(rhs[m] * conj(rhs[m]));
+    }
+    double a = creal(t1) / t2;
+    alpha[it] = a;
+    /* mom.cpp:318-336: step, then re-solve the total fields */
+    for (int n = 0; n < U; n++) o[n] -= a * ot[n];
+    for (int n = 0; n < U; n++) g[n] = o[n] * k2;
+    for (int i = 0; i < ntx; i++) {
+      double complex *ti = &tot[(size_t)i * U];
+      for (int n = 0; n < U; n++) ti[n] = 0;
+      orc_bicgs(c, ti, g, &inc[(size_t)i * U], 0, tol, maxit, NULL);
+      for (int n = 0; n < U; n++) x[n] = ti[n] * o[n] * k2;
+      orc_aggregate(c, x, &rhs[i * nr]);
+      for (int m = 0; m < nr; m++) mesd[i * nr + m] = rhs[i * nr + m] - mes[i * nr + m];
+    }
+    memcpy(save, od, U * sizeof(double complex));
+    dbim_gradient(c, ntx, o, tot, mesd, regular, tol, maxit, od);
+    dbim_record(c, ntx, mesd, od, o, chi_true, regular, mesnorm, objnorm, &hist[5 * (it + 1)]);
+    /* mom.cpp:383-399: Polak-Ribiere direction */
+    double complex n1 = 0;
+    double n2 = 0;
+    for (int n = 0; n < U; n++) {
+      n1 += od[n] * conj(od[n] - save[n]);
+      n2 += creal(save[n] * conj(save[n]));
+    }
+    double complex b = n1 / n2;
+    beta[it] = b;
+    for (int n = 0; n < U; n++) ot[n] = od[n] + b * ot[n];
+  }
+  free(tot);
+  free(mes);
+  free(mesd);
+  free(rhs);
+  free(od);
+  free(ot);
+  free(save);
+  free(g);
+  free(x);
+  free(y);
+  free(cc);
+  return 0;
 }

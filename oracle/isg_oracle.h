@@ -54,6 +54,17 @@ int orc_bicgs(orc_ctx *c, double complex *x, const double complex *g, const doub
 void orc_aggregate(orc_ctx *c, const double complex *x, double complex *rx);
 void orc_aggregateh(orc_ctx *c, double complex *x, const double complex *rx);
 
+/* The reference's inversion driver: synthetic measurements of chi_true
+ * (setup_born.cpp:139-168), then the gradient (mom.cpp:247-271) and
+ * `iterations` Polak-Ribiere steps (mom.cpp:277-399) from chi = 0.  inc holds
+ * ntx incident fields, chi and chi_true are contrasts (eps_r - 1), all in tree
+ * order.  hist receives 5 numbers per record (write_error, setup_born.cpp:
+ * 239-240: misfit, object error, regularisation cost, gradient norm, object
+ * norm), iterations + 1 records; alpha and beta one per iteration. */
+int orc_dbim(orc_ctx *c, int ntx, const double complex *inc, const double complex *chi_true, int iterations,
+             double regular, double tol, int maxit, double complex *chi, double *hist, double *alpha,
+             double complex *beta);
+
 #ifdef __cplusplus
 }
 #endif

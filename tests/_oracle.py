@@ -218,3 +218,20 @@ def disk_contrast(pos: np.ndarray, k0: float = 2 * np.pi, radius: float = 2.0, c
 def plane_wave(pos: np.ndarray, angle: float, k0: float = 2 * np.pi) -> np.ndarray:
     """exp(i k0 d.r) (setup_born.cpp:62-65)."""
     return np.exp(1j * k0 * (np.cos(angle) * pos.real + np.sin(angle) * pos.imag))
+
+
+def oracle_dbim(o: "Oracle", inc: np.ndarray, chi_true: np.ndarray, iterations: int, regular: float = 0.0,
+                tol: float = 1e-4, maxit: int = 300):
+    """orc_dbim: the reference's measurement + Polak-Ribiere inversion loop in FP64 (tree order)."""
+    L = o.L
+    L.orc_dbim.argtypes = [_P, _I, _P, _P, _I, _D, _D, _I, _P, _P, _P, _P]
+    ntx = inc.shape[0]
+    inc = np.ascontiguousarray(inc, np.complex128)
+    chi_true = np.ascontiguousarray(chi_true, np.complex128)
+    chi = np.zeros(o.U, np.complex128)
+    hist = np.zeros((iterations + 1, 5))
+    alpha = np.zeros(iterations)
+    beta = np.zeros(iterations, np.complex128)
+    L.orc_dbim(o.h, ntx, _arr(inc), _arr(chi_true), iterations, regular, tol, maxit, _arr(chi), _arr(hist),
+               _arr(alpha), _arr(beta))
+    return chi, hist, alpha, beta
