@@ -19,6 +19,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 OUT = os.path.join(HERE, "isg", "libisg.so")
+REFAPI_SRC = os.path.join(HERE, "refapi", "isg_refapi.cpp")
+REFAPI_OUT = os.path.join(HERE, "isg", "libisg_ref.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr",
@@ -71,7 +73,23 @@ def build(force: bool = False, jobs: int = 8, verbose_ptxas: bool = False) -> st
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    build_refapi(force)
     return OUT
+
+
+def build_refapi(force: bool = False) -> str:
+    """libisg_ref.so: the reference's routine names over libisg.so.  Its globals
+    (res, level, ...) stay undefined until the caller's driver links it."""
+    inputs = [REFAPI_SRC, OUT, os.path.join(ROOT, "include", "isg_refapi.h"), os.path.join(ROOT, "include", "isg.h")]
+    if force or stale(REFAPI_OUT, inputs):
+        cuda_inc = os.path.join(os.path.dirname(os.path.dirname(nvcc())), "include")
+        cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-I" + cuda_inc, "-o", REFAPI_OUT, REFAPI_SRC,
+               "-L" + os.path.dirname(OUT), "-lisg", "-L" + os.path.join(os.path.dirname(cuda_inc), "lib64"),
+               "-lcudart", "-Wl,-rpath,$ORIGIN"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"libisg_ref.so failed:\n{r.stdout}\n{r.stderr}")
+    return REFAPI_OUT
 
 
 if __name__ == "__main__":

@@ -65,3 +65,20 @@ def test_unknown_table_is_bad_arg():
     s = isg.Solver(4)
     with pytest.raises(isg.IsgError):
         s.host_table("no_such_table")
+
+
+def test_refapi_library_exports_the_reference_names():
+    """libisg_ref.so defines every routine of include/isg_refapi.h under the
+    reference's own C++ names and leaves the driver's globals undefined."""
+    import subprocess
+    lib = os.path.join(ROOT, "inverse-solver-gpu_b200", "isg", "libisg_ref.so")
+    out = subprocess.run(["nm", "-D", "-C", lib], capture_output=True, text=True, check=True).stdout
+    defined = {ln.split(" T ", 1)[1].strip() for ln in out.splitlines() if " T " in ln}
+    c = "std::complex<double>*"
+    want = ["setup_mlfma()", "setup_gpu()", "setup_bicgs()", f"bicgs({c}, {c}, {c}, bool)",
+            f"matvec({c}, {c}, {c}, bool)", f"mlfma({c}, {c})", f"mlfmah({c}, {c})", f"aggregate({c}, {c})",
+            f"aggregateh({c}, {c})"]
+    assert not [w for w in want if w not in defined], defined
+    undefined = {ln.split()[-1] for ln in out.splitlines() if " U " in ln}
+    for g in ("res", "box", "level", "k0", "numunk", "numrx", "toli", "iti", "pos", "unkmap"):
+        assert g in undefined, g
