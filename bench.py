@@ -220,7 +220,7 @@ def main():
     b = torch.from_numpy(b_np.astype(np.complex64)).to(dev)
     x = torch.zeros_like(b)
     stream = torch.cuda.Stream(dev)
-    engine = {"simt": isg.ENGINE_SIMT, "tensor": isg.ENGINE_TENSOR, "auto": isg.ENGINE_SIMT}[args.engine]
+    engine = {"simt": isg.ENGINE_SIMT, "tensor": isg.ENGINE_TENSOR, "auto": isg.ENGINE_TENSOR}[args.engine]
     opts = isg.default_solve_opts(tol=TOL, maxit=300, engine=engine, check_every=2)
 
     def step():
