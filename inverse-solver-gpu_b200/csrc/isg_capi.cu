@@ -305,6 +305,7 @@ isg_status isg_setup_gpu(isg_ctx *c) {
   if ((e = cuda_check(c, cudaMemset(c->mul, 0, R * P.mp * sizeof(float2)), "memset"))) return e;
   if ((e = cuda_check(c, cudaMemset(c->loc, 0, R * P.mp * sizeof(float2)), "memset"))) return e;
   if ((e = tc_setup(c)) != ISG_OK) return e;
+  if ((e = band_setup(c)) != ISG_OK) return e;
   c->gpu_ready = true;
   return cuda_check(c, cudaDeviceSynchronize(), "setup sync");
 }
@@ -314,6 +315,7 @@ void isg_destroy(isg_ctx *c) {
   if (c->gpu_ready || !c->dev_allocs.empty()) {
     cudaSetDevice(c->opts.device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    band_destroy(c);
     tc_destroy(c);
     for (void *p : c->dev_allocs) cudaFree(p);
     if (c->h_count) cudaFreeHost(c->h_count);
@@ -495,10 +497,13 @@ isg_status isg_time_stages(isg_ctx *c, int nrhs, int engine, int reps, double *m
     cudaEventRecord(ev[0], st);
     if (tc) tc_p2m(c, B, c->mul, st); else launch_p2m(P, B, c->mul, st);
     cudaEventRecord(ev[1], st);
-    for (int i = P.L - 2; i >= 2; i--) launch_m2m(P, i, c->mul, nrhs, nullptr, st);
+    isg_status be = ISG_OK;
+    for (int i = P.L - 2; i >= 2; i--)
+      if (!(tc && band_m2m(c, i, c->mul, nrhs, nullptr, st, &be))) launch_m2m(P, i, c->mul, nrhs, nullptr, st);
     cudaEventRecord(ev[2], st);
     for (int i = 2; i < P.L; i++) launch_m2l(P, i, c->mul, c->loc, nrhs, nullptr, st);
-    for (int i = 3; i < P.L; i++) launch_l2l(P, i, c->loc, nrhs, nullptr, true, st);
+    for (int i = 3; i < P.L; i++)
+      if (!(tc && band_l2l(c, i, c->loc, nrhs, nullptr, true, st, &be))) launch_l2l(P, i, c->loc, nrhs, nullptr, true, st);
     cudaEventRecord(ev[3], st);
     if (tc) tc_near(c, A, st); else launch_near(P, A, st);
     cudaEventRecord(ev[4], st);

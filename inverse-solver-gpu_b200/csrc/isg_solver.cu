@@ -342,9 +342,14 @@ isg_status run_matvec(isg_ctx *c, const float2 *x, const float2 *g, int64_t gs, 
   } else {
     launch_p2m(P, B, c->mul, st);
   }
-  for (int i = P.L - 2; i >= 2; i--) launch_m2m(P, i, c->mul, nrhs, active, st);
+  isg_status be = ISG_OK;
+  for (int i = P.L - 2; i >= 2; i--)
+    if (!(tc && band_m2m(c, i, c->mul, nrhs, active, st, &be))) launch_m2m(P, i, c->mul, nrhs, active, st);
+  if (be != ISG_OK) return be;
   for (int i = 2; i < P.L; i++) launch_m2l(P, i, c->mul, c->loc, nrhs, active, st);
-  for (int i = 3; i < P.L; i++) launch_l2l(P, i, c->loc, nrhs, active, true, st);
+  for (int i = 3; i < P.L; i++)
+    if (!(tc && band_l2l(c, i, c->loc, nrhs, active, true, st, &be))) launch_l2l(P, i, c->loc, nrhs, active, true, st);
+  if (be != ISG_OK) return be;
   NearArgs A;
   A.in = B;
   A.loc = c->loc;

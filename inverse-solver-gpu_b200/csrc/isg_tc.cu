@@ -559,6 +559,12 @@ struct TcPlan {
 
 bool tc_available(const isg_ctx *c) { return c->tc && c->tc->ok; }
 
+}  // namespace isg
+
+int *isg_ctx::tc_err_flag() const { return tc ? tc->err : nullptr; }
+
+namespace isg {
+
 isg_status tc_setup(isg_ctx *c) {
   int dev = 0, major = 0, minor = 0;
   cudaGetDevice(&dev);

@@ -1,0 +1,389 @@
+// M2M and L2L on the tensor cores as banded GEMMs over every ring of a level.
+//
+// Interpolation (M2M, kernels.cu:83-136, solve.cpp:93-112) and anterpolation
+// (L2L, kernels.cu:137-238, solve.cpp:149-169) apply one real banded matrix
+// per level to complex rings: D[sample][ring] = sum_j W[sample][j] ring[j].
+// Output samples are tiled by 128 (the MMA M); for each tile the weights are
+// restricted to the circular window of input samples its rows touch (a few
+// dozen more than 128 x the rate ratio), precomputed on the host as FP16 hi/lo
+// K-chunks of 64 in the core-matrix layout and brought in by bulk copies.  The
+// CTA's 256 MMA columns are 32 parents x 4 children x (re, im) of one level of
+// one or more RHS; ring values are split into FP16 hi/lo after a power-of-two
+// scale per CTA (3 products, FP32 accumulation in TMEM).  The child shift
+// phases are folded into the epilogue (M2M: sum over the four children) or into
+// the operand (L2L: shifted parent ring), exactly as in the reference.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "isg_context.hpp"
+#include "isg_tc.cuh"
+
+namespace isg {
+
+namespace {
+
+using namespace tc;
+
+constexpr int kCols = 256;        // MMA N: 32 parents x 4 children x (re, im)
+constexpr int kParents = 32;
+constexpr int kKC = 64;           // K chunk
+constexpr int kAHalf = 128 * kKC * 2;    // 16 KB: one FP16 split of an A chunk
+constexpr int kBHalf = kCols * kKC * 2;  // 32 KB
+constexpr int kSmem = 2 * kAHalf + 2 * kBHalf + 128;
+constexpr int kErrBand = 121;
+
+enum BandMode { BAND_M2M = 0, BAND_L2L_ADD = 1, BAND_L2L_SET = 2 };
+
+struct BandArgs {
+  int mode;
+  const float2 *src;  // M2M: child-level multipoles; L2L: parent-level locals (level base)
+  float2 *dst;        // M2M: parent-level multipoles; L2L: child-level locals (level base)
+  size_t mp;
+  int n_p, ns_in, ns_out;
+  const float2 *shift;  // M2M: shiftmul of the parent level; L2L: shiftloc of the parent level, [4][ns_p]
+  const uint8_t *A;     // K-chunks of this transition (hi then lo, 32 KB each)
+  const int *kw0, *nchunk, *chunk0;  // per M-tile: window start (-1: whole ring), chunks, first chunk
+  float inv_a;
+  int nparents, ncols;  // ncols = parents x RHS
+  const int *active;
+  int *err;
+};
+
+__device__ __forceinline__ float2 band_in(const BandArgs &A, int ring, int kk, int kw0) {
+  const int pl = ring >> 2, q = ring & 3, gp = blockIdx.x * kParents + pl;
+  if (gp >= A.ncols) return make_float2(0.f, 0.f);
+  const int rhs = gp / A.nparents, P = gp % A.nparents;
+  if (A.active && !A.active[rhs]) return make_float2(0.f, 0.f);
+  int j;
+  if (kw0 < 0) {
+    if (kk >= A.ns_in) return make_float2(0.f, 0.f);
+    j = kk;
+  } else {
+    j = kw0 + kk;
+    if (j >= A.ns_in) j -= A.ns_in;
+    if (j >= A.ns_in) j %= A.ns_in;
+  }
+  const float2 *base = A.src + (size_t)rhs * A.mp;
+  if (A.mode == BAND_M2M) {
+    const int py = P / A.n_p, px = P % A.n_p, nc = 2 * A.n_p;
+    return base[(size_t)((2 * py + (q >> 1)) * nc + 2 * px + (q & 1)) * A.ns_in + j];
+  }
+  return cmul(__ldg(&A.shift[q * A.ns_in + j]), base[(size_t)P * A.ns_in + j]);
+}
+
+__global__ void __launch_bounds__(256, 2) k_tc_band(BandArgs A) {
+  extern __shared__ __align__(1024) char sm[];
+  char *ahi = sm, *alo = sm + kAHalf, *bhi = sm + 2 * kAHalf, *blo = bhi + kBHalf;
+  uint64_t *abar = (uint64_t *)(blo + kBHalf);
+  uint64_t *mbar = abar + 1;
+  uint32_t *tslot = (uint32_t *)(abar + 2);
+  float *fscr = (float *)(abar + 3);  // [8]
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int mt = blockIdx.y, m0 = mt * 128;
+  const int kw0 = A.kw0[mt], nch = A.nchunk[mt];
+  const uint8_t *Achunks = A.A + (size_t)A.chunk0[mt] * 2 * kAHalf;
+  const int kwtot = nch * kKC;
+
+  // per-CTA power-of-two scale of the ring values in the window
+  float mx = 0.f;
+  for (int e = threadIdx.x; e < 128 * kwtot; e += blockDim.x) {
+    const float2 v = band_in(A, e / kwtot, e % kwtot, kw0);
+    mx = fmaxf(mx, fmaxf(fabsf(v.x), fabsf(v.y)));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if (lane == 0) fscr[warp] = mx;
+  if (threadIdx.x == 0) {
+    mbar_init(abar, 1);
+    mbar_init(mbar, 1);
+    fence_mbar_init();
+  }
+  if (warp == 0) tmem_alloc(tslot, 256);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+  float m2 = 0.f;
+  for (int w = 0; w < 8; w++) m2 = fmaxf(m2, fscr[w]);
+  const float s = pow2_scale(m2);
+  const uint32_t idesc = idesc_f16_f32(128, kCols);
+  const uint32_t sbase = smem_u32(sm);
+  bool ok = true;
+
+  for (int ch = 0; ch < nch; ch++) {
+    if (threadIdx.x == 0) {
+      mbar_expect_tx(abar, 2 * kAHalf);
+      bulk_g2s(ahi, Achunks + (size_t)ch * 2 * kAHalf, 2 * kAHalf, abar);
+    }
+    // B chunk: ring r gives rows 2r (re) and 2r + 1 (im); item = (ring, 8-sample group)
+    for (int it = threadIdx.x; it < 128 * (kKC / 8); it += blockDim.x) {
+      const int r = it >> 3, g8 = it & 7;
+      __align__(16) __half hr[8], lr[8], hi8[8], li8[8];
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        const float2 v = band_in(A, r, ch * kKC + g8 * 8 + k, kw0);
+        split_f16(v.x * s, hr[k], lr[k]);
+        split_f16(v.y * s, hi8[k], li8[k]);
+      }
+      const int n0 = 2 * r, n1 = 2 * r + 1;
+      const int o0 = ((n0 >> 3) * (kKC / 8) + g8) * 128 + (n0 & 7) * 16;
+      const int o1 = ((n1 >> 3) * (kKC / 8) + g8) * 128 + (n1 & 7) * 16;
+      *(uint4 *)(bhi + o0) = *(uint4 *)hr;
+      *(uint4 *)(blo + o0) = *(uint4 *)lr;
+      *(uint4 *)(bhi + o1) = *(uint4 *)hi8;
+      *(uint4 *)(blo + o1) = *(uint4 *)li8;
+    }
+    fence_proxy_async();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      tc_fence_after();
+      if (mbar_wait(abar, ch & 1, A.err, kErrBand)) {
+#pragma unroll
+        for (int ks = 0; ks < kKC / 16; ks++) {
+          const uint64_t ah = smem_desc(sbase + ks * 256, 128, (kKC / 8) * 128);
+          const uint64_t al = smem_desc(sbase + kAHalf + ks * 256, 128, (kKC / 8) * 128);
+          const uint64_t bh = smem_desc(sbase + 2 * kAHalf + ks * 256, 128, (kKC / 8) * 128);
+          const uint64_t bl = smem_desc(sbase + 2 * kAHalf + kBHalf + ks * 256, 128, (kKC / 8) * 128);
+          mma_f16(tmem, ah, bh, idesc, (ch | ks) ? 1 : 0);
+          mma_f16(tmem, ah, bl, idesc, 1);
+          mma_f16(tmem, al, bh, idesc, 1);
+        }
+      }
+      mma_commit(mbar);
+    }
+    ok = mbar_wait(mbar, ch & 1, A.err, kErrBand) && ok;
+    __syncthreads();
+  }
+
+  // ---- epilogue ----
+  tc_fence_after();
+  const float inv = A.inv_a / s;
+  const int qd = warp & 3, h = warp >> 2;
+  const int km = m0 + 32 * qd + lane;
+  const bool row_ok = ok && km < A.ns_out;
+  for (int pp = 0; pp < 8; pp++) {
+    float d[16];
+    tmem_ld16(tmem + ((uint32_t)(32 * qd) << 16) + 128 * h + 16 * pp, d);
+    if (!row_ok) continue;
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      const int pl = 16 * h + 2 * pp + u, gp = blockIdx.x * kParents + pl;
+      if (gp >= A.ncols) continue;
+      const int rhs = gp / A.nparents, P = gp % A.nparents;
+      if (A.active && !A.active[rhs]) continue;
+      float2 *base = A.dst + (size_t)rhs * A.mp;
+      const float *dv = d + 8 * u;
+      if (A.mode == BAND_M2M) {
+        float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+          cfma(acc, __ldg(&A.shift[q * A.ns_out + km]), make_float2(dv[2 * q] * inv, dv[2 * q + 1] * inv));
+        base[(size_t)P * A.ns_out + km] = acc;
+      } else {
+        const int py = P / A.n_p, px = P % A.n_p, nc = 2 * A.n_p;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          float2 *o = base + (size_t)((2 * py + (q >> 1)) * nc + 2 * px + (q & 1)) * A.ns_out + km;
+          const float2 v = make_float2(dv[2 * q] * inv, dv[2 * q + 1] * inv);
+          *o = A.mode == BAND_L2L_ADD ? cadd(*o, v) : v;
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, 256);
+}
+
+// One level transition: weight chunks and per-tile windows.
+struct Transition {
+  int mtiles = 0;
+  int *kw0 = nullptr, *nchunk = nullptr, *chunk0 = nullptr;  // device
+  uint8_t *A = nullptr;                                      // device
+  float inv_a = 1;
+  bool ok = false;
+};
+
+// Packs reals(row, k0 .. k0+63) of a [128 x K] block as FP16 hi then lo in the
+// K-major core-matrix layout (SBO = 8 chunks x 128 B, LBO = 128 B).
+template <class F>
+void pack_chunk(std::vector<uint8_t> &buf, size_t at, int k0, double scale, F real_at) {
+  __half *hi = (__half *)(buf.data() + at), *lo = (__half *)(buf.data() + at + kAHalf);
+  for (int n = 0; n < 128; n++)
+    for (int k = 0; k < kKC; k++) {
+      const double v = real_at(n, k0 + k) * scale;
+      const __half h = __double2half(v);
+      const __half l = __double2half(v - (double)__half2float(h));
+      const size_t idx = ((size_t)(n / 8) * (kKC / 8) + k / 8) * 64 + (n % 8) * 8 + (k % 8);
+      hi[idx] = h;
+      lo[idx] = l;
+    }
+}
+
+}  // namespace
+
+struct BandPlan {
+  Transition m2m[kMaxLevels];  // indexed by parent level
+  Transition l2l[kMaxLevels];  // indexed by child level
+  std::vector<void *> allocs;
+};
+
+// Builds one transition from rows of taps (index into the input ring, weight).
+static isg_status build_transition(isg_ctx *c, Transition &T, int ns_out, int ns_in,
+                                   const std::vector<std::vector<std::pair<int, double>>> &rows) {
+  double mw = 0;
+  for (auto &r : rows)
+    for (auto &t : r) mw = std::max(mw, std::abs(t.second));
+  int e2;
+  std::frexp(mw > 0 ? mw : 1.0, &e2);
+  const double sa = std::ldexp(1.0, 14 - e2);
+  T.mtiles = (ns_out + 127) / 128;
+  std::vector<int> kw0(T.mtiles), nch(T.mtiles), ch0(T.mtiles);
+  std::vector<uint8_t> buf;
+  int chunks = 0;
+  for (int mt = 0; mt < T.mtiles; mt++) {
+    std::vector<char> used(ns_in, 0);
+    for (int m = mt * 128; m < std::min(ns_out, mt * 128 + 128); m++)
+      for (auto &t : rows[m])
+        if (t.second != 0.0) used[t.first] = 1;
+    // shortest circular arc covering every used sample
+    int start = 0, len = ns_in, best_gap = 0, nused = 0;
+    for (int j = 0; j < ns_in; j++) nused += used[j];
+    if (nused > 0 && nused < ns_in) {
+      int first = -1;
+      for (int j = 0; j < ns_in; j++)
+        if (used[j]) {
+          first = j;
+          break;
+        }
+      int prev = first;
+      for (int step = 1; step <= ns_in; step++) {
+        const int j = (first + step) % ns_in;
+        if (!used[j]) continue;
+        const int gap = (j - prev + ns_in) % ns_in - 1;
+        if (gap > best_gap) {
+          best_gap = gap;
+          start = j;
+        }
+        prev = j;
+        if (j == first) break;
+      }
+      len = ns_in - best_gap;
+    }
+    const bool whole = len >= ns_in - 8;
+    kw0[mt] = whole ? -1 : start;
+    const int span = whole ? ns_in : len;
+    nch[mt] = (span + kKC - 1) / kKC;
+    ch0[mt] = chunks;
+    std::vector<double> dense((size_t)128 * nch[mt] * kKC, 0.0);
+    for (int m = mt * 128; m < std::min(ns_out, mt * 128 + 128); m++)
+      for (auto &t : rows[m]) {
+        const int kk = whole ? t.first : (t.first - start + ns_in) % ns_in;
+        if (kk < nch[mt] * kKC) dense[(size_t)(m - mt * 128) * nch[mt] * kKC + kk] += t.second;
+      }
+    buf.resize(buf.size() + (size_t)nch[mt] * 2 * kAHalf, 0);
+    for (int ch = 0; ch < nch[mt]; ch++)
+      pack_chunk(buf, (size_t)(chunks + ch) * 2 * kAHalf, ch * kKC, sa,
+                 [&](int n, int k) { return dense[(size_t)n * nch[mt] * kKC + k]; });
+    chunks += nch[mt];
+  }
+  isg_status e;
+  if ((e = cuda_check(c, cudaMalloc(&T.A, buf.size()), "band alloc")) != ISG_OK) return e;
+  if ((e = cuda_check(c, cudaMalloc(&T.kw0, T.mtiles * sizeof(int)), "band alloc")) != ISG_OK) return e;
+  if ((e = cuda_check(c, cudaMalloc(&T.nchunk, T.mtiles * sizeof(int)), "band alloc")) != ISG_OK) return e;
+  if ((e = cuda_check(c, cudaMalloc(&T.chunk0, T.mtiles * sizeof(int)), "band alloc")) != ISG_OK) return e;
+  cudaMemcpy(T.A, buf.data(), buf.size(), cudaMemcpyHostToDevice);
+  cudaMemcpy(T.kw0, kw0.data(), T.mtiles * sizeof(int), cudaMemcpyHostToDevice);
+  cudaMemcpy(T.nchunk, nch.data(), T.mtiles * sizeof(int), cudaMemcpyHostToDevice);
+  cudaMemcpy(T.chunk0, ch0.data(), T.mtiles * sizeof(int), cudaMemcpyHostToDevice);
+  T.inv_a = (float)(1.0 / sa);
+  T.ok = true;
+  return ISG_OK;
+}
+
+isg_status band_setup(isg_ctx *c) {
+  c->band = new BandPlan();
+  if (!tc_available(c)) return ISG_OK;
+  const HostTables &H = c->T;
+  const int L = H.L, ni = H.ninter, W = 2 * ni;
+  isg_status e;
+  for (int i = 2; i <= L - 2; i++) {  // M2M into parent level i
+    const int nsp = H.nsamp[i], nsc = H.nsamp[i + 1];
+    std::vector<std::vector<std::pair<int, double>>> rows(nsp);
+    for (int k = 0; k < nsp; k++)
+      for (int t = 0; t < ni; t++)
+        rows[k].push_back({H.intind[i][(size_t)k * ni + t], H.interp[i][(size_t)k * ni + t]});
+    if ((e = build_transition(c, c->band->m2m[i], nsp, nsc, rows)) != ISG_OK) return e;
+  }
+  for (int i = 3; i <= L - 1; i++) {  // L2L into child level i
+    const int nsc = H.nsamp[i], nsp = H.nsamp[i - 1];
+    std::vector<std::vector<std::pair<int, double>>> rows(nsc);
+    for (int k = 0; k < nsc; k++)
+      for (int t = 0; t < W; t++) {
+        const double w = H.anterp[i][(size_t)k * W + t];
+        if (w != 0.0) rows[k].push_back({H.antind[i][(size_t)k * W + t], w});
+      }
+    if ((e = build_transition(c, c->band->l2l[i], nsc, nsp, rows)) != ISG_OK) return e;
+  }
+  return cuda_check(c, cudaFuncSetAttribute(k_tc_band, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem),
+                    "band attr");
+}
+
+void band_destroy(isg_ctx *c) {
+  if (!c->band) return;
+  for (int i = 0; i < kMaxLevels; i++)
+    for (Transition *T : {&c->band->m2m[i], &c->band->l2l[i]}) {
+      cudaFree(T->A);
+      cudaFree(T->kw0);
+      cudaFree(T->nchunk);
+      cudaFree(T->chunk0);
+    }
+  delete c->band;
+  c->band = nullptr;
+}
+
+static isg_status band_launch(isg_ctx *c, const Transition &T, int mode, const float2 *src, float2 *dst, int n_p,
+                              int ns_in, int ns_out, const float2 *shift, int nrhs, const int *active,
+                              cudaStream_t st) {
+  BandArgs A;
+  A.mode = mode;
+  A.src = src;
+  A.dst = dst;
+  A.mp = c->P.mp;
+  A.n_p = n_p;
+  A.ns_in = ns_in;
+  A.ns_out = ns_out;
+  A.shift = shift;
+  A.A = T.A;
+  A.kw0 = T.kw0;
+  A.nchunk = T.nchunk;
+  A.chunk0 = T.chunk0;
+  A.inv_a = T.inv_a;
+  A.nparents = n_p * n_p;
+  A.ncols = A.nparents * nrhs;
+  A.active = active;
+  A.err = c->tc_err_flag();
+  count_launch();
+  k_tc_band<<<dim3((A.ncols + kParents - 1) / kParents, T.mtiles), 256, kSmem, st>>>(A);
+  return cuda_check(c, cudaGetLastError(), "band launch");
+}
+
+bool band_m2m(isg_ctx *c, int lvl, float2 *mul, int nrhs, const int *active, cudaStream_t st, isg_status *e) {
+  if (!c->band || lvl >= kMaxLevels || !c->band->m2m[lvl].ok) return false;
+  const DevLevel &p = c->P.lv[lvl], &ch = c->P.lv[lvl + 1];
+  *e = band_launch(c, c->band->m2m[lvl], BAND_M2M, mul + ch.off, mul + p.off, p.n, ch.ns, p.ns, p.shm, nrhs, active,
+                   st);
+  return true;
+}
+
+bool band_l2l(isg_ctx *c, int lvl, float2 *loc, int nrhs, const int *active, bool accumulate, cudaStream_t st,
+              isg_status *e) {
+  if (!c->band || lvl >= kMaxLevels || !c->band->l2l[lvl].ok) return false;
+  const DevLevel &ch = c->P.lv[lvl], &p = c->P.lv[lvl - 1];
+  *e = band_launch(c, c->band->l2l[lvl], accumulate ? BAND_L2L_ADD : BAND_L2L_SET, loc + p.off, loc + ch.off, p.n,
+                   p.ns, ch.ns, p.shl, nrhs, active, st);
+  return true;
+}
+
+}  // namespace isg
