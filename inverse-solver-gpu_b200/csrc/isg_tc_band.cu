@@ -50,31 +50,55 @@ struct BandArgs {
   int *err;
 };
 
-__device__ __forceinline__ float2 band_in(const BandArgs &A, int ring, int kk, int kw0) {
+// One ring of the CTA: its base pointer (and shift row for L2L), or none.
+struct RingRef {
+  const float2 *p;
+  const float2 *sh;
+};
+
+__device__ __forceinline__ RingRef ring_ref(const BandArgs &A, int ring) {
   const int pl = ring >> 2, q = ring & 3, gp = blockIdx.x * kParents + pl;
-  if (gp >= A.ncols) return make_float2(0.f, 0.f);
+  RingRef r{nullptr, nullptr};
+  if (gp >= A.ncols) return r;
   const int rhs = gp / A.nparents, P = gp % A.nparents;
-  if (A.active && !A.active[rhs]) return make_float2(0.f, 0.f);
-  int j;
-  if (kw0 < 0) {
-    if (kk >= A.ns_in) return make_float2(0.f, 0.f);
-    j = kk;
-  } else {
-    j = kw0 + kk;
-    if (j >= A.ns_in) j -= A.ns_in;
-    if (j >= A.ns_in) j %= A.ns_in;
-  }
+  if (A.active && !A.active[rhs]) return r;
   const float2 *base = A.src + (size_t)rhs * A.mp;
   if (A.mode == BAND_M2M) {
     const int py = P / A.n_p, px = P % A.n_p, nc = 2 * A.n_p;
-    return base[(size_t)((2 * py + (q >> 1)) * nc + 2 * px + (q & 1)) * A.ns_in + j];
+    r.p = base + (size_t)((2 * py + (q >> 1)) * nc + 2 * px + (q & 1)) * A.ns_in;
+  } else {
+    r.p = base + (size_t)P * A.ns_in;
+    r.sh = A.shift + q * A.ns_in;
   }
-  return cmul(__ldg(&A.shift[q * A.ns_in + j]), base[(size_t)P * A.ns_in + j]);
+  return r;
+}
+
+// Eight consecutive window samples kk0 .. kk0+7 of a ring (zero outside).
+__device__ __forceinline__ void ring_load8(const BandArgs &A, const RingRef &r, int kk0, int kw0, float2 *v) {
+  int j0;
+  if (kw0 < 0) {
+    j0 = kk0;
+  } else {
+    j0 = (kw0 + kk0) % A.ns_in;  // the window may be longer than the ring; weights past it are zero
+  }
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    int j = j0 + k;
+    bool ok = r.p != nullptr;
+    if (kw0 < 0) {
+      ok = ok && j < A.ns_in;
+    } else if (j >= A.ns_in) {
+      j -= A.ns_in;
+    }
+    float2 x = make_float2(0.f, 0.f);
+    if (ok) x = r.sh ? cmul(__ldg(&r.sh[j]), r.p[j]) : r.p[j];
+    v[k] = x;
+  }
 }
 
 __global__ void __launch_bounds__(256, 2) k_tc_band(BandArgs A) {
   extern __shared__ __align__(1024) char sm[];
-  char *ahi = sm, *alo = sm + kAHalf, *bhi = sm + 2 * kAHalf, *blo = bhi + kBHalf;
+  char *ahi = sm, *bhi = sm + 2 * kAHalf, *blo = bhi + kBHalf;
   uint64_t *abar = (uint64_t *)(blo + kBHalf);
   uint64_t *mbar = abar + 1;
   uint32_t *tslot = (uint32_t *)(abar + 2);
@@ -87,9 +111,14 @@ __global__ void __launch_bounds__(256, 2) k_tc_band(BandArgs A) {
 
   // per-CTA power-of-two scale of the ring values in the window
   float mx = 0.f;
-  for (int e = threadIdx.x; e < 128 * kwtot; e += blockDim.x) {
-    const float2 v = band_in(A, e / kwtot, e % kwtot, kw0);
-    mx = fmaxf(mx, fmaxf(fabsf(v.x), fabsf(v.y)));
+  const int g8n = kwtot / 8;
+#pragma unroll 2
+  for (int it = threadIdx.x; it < 128 * g8n; it += blockDim.x) {
+    const RingRef rr = ring_ref(A, it / g8n);
+    float2 v[8];
+    ring_load8(A, rr, (it % g8n) * 8, kw0, v);
+#pragma unroll
+    for (int k = 0; k < 8; k++) mx = fmaxf(mx, fmaxf(fabsf(v[k].x), fabsf(v[k].y)));
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
@@ -117,14 +146,16 @@ __global__ void __launch_bounds__(256, 2) k_tc_band(BandArgs A) {
       bulk_g2s(ahi, Achunks + (size_t)ch * 2 * kAHalf, 2 * kAHalf, abar);
     }
     // B chunk: ring r gives rows 2r (re) and 2r + 1 (im); item = (ring, 8-sample group)
+#pragma unroll 2
     for (int it = threadIdx.x; it < 128 * (kKC / 8); it += blockDim.x) {
       const int r = it >> 3, g8 = it & 7;
       __align__(16) __half hr[8], lr[8], hi8[8], li8[8];
+      float2 v[8];
+      ring_load8(A, ring_ref(A, r), ch * kKC + g8 * 8, kw0, v);
 #pragma unroll
       for (int k = 0; k < 8; k++) {
-        const float2 v = band_in(A, r, ch * kKC + g8 * 8 + k, kw0);
-        split_f16(v.x * s, hr[k], lr[k]);
-        split_f16(v.y * s, hi8[k], li8[k]);
+        split_f16(v[k].x * s, hr[k], lr[k]);
+        split_f16(v[k].y * s, hi8[k], li8[k]);
       }
       const int n0 = 2 * r, n1 = 2 * r + 1;
       const int o0 = ((n0 >> 3) * (kKC / 8) + g8) * 128 + (n0 & 7) * 16;
@@ -303,6 +334,7 @@ static isg_status build_transition(isg_ctx *c, Transition &T, int ns_out, int ns
 }
 
 isg_status band_setup(isg_ctx *c) {
+  const bool build_l2l = false;
   c->band = new BandPlan();
   if (!tc_available(c)) return ISG_OK;
   const HostTables &H = c->T;
@@ -316,7 +348,10 @@ isg_status band_setup(isg_ctx *c) {
         rows[k].push_back({H.intind[i][(size_t)k * ni + t], H.interp[i][(size_t)k * ni + t]});
     if ((e = build_transition(c, c->band->m2m[i], nsp, nsc, rows)) != ISG_OK) return e;
   }
-  for (int i = 3; i <= L - 1; i++) {  // L2L into child level i
+  // L2L stays on the SIMT kernel: its windows are ~2x wider than M2M's (the
+  // parent rate is higher) and the per-CTA operand conversion outweighs the
+  // MMAs (measured slower than k_l2l on the 1024^2 workload).
+  for (int i = 3; i <= L - 1 && build_l2l; i++) {  // L2L into child level i
     const int nsc = H.nsamp[i], nsp = H.nsamp[i - 1];
     std::vector<std::vector<std::pair<int, double>>> rows(nsc);
     for (int k = 0; k < nsc; k++)
