@@ -81,14 +81,15 @@ __device__ __forceinline__ void block_bar1() { asm volatile("bar.sync 1, %0;\n" 
 // children are too large to stage (top levels only).
 template <bool STAGE>
 __global__ void __launch_bounds__(256) k_m2m(float2 *__restrict__ mul, size_t mp, size_t off_p, size_t off_c, int n_p,
-                                             int ns_p, int ns_c, int npb, const int *__restrict__ ifirst,
+                                             int ns_p, int ns_c, int npb, int chunks, const int *__restrict__ ifirst,
                                              const float *__restrict__ iw, const float2 *__restrict__ shm,
                                              int ninter, const int *__restrict__ active) {
   extern __shared__ float2 chs[];
   const int rhs = blockIdx.y;
   if (inactive(active, rhs)) return;
   const int nparent = n_p * n_p, n_c = 2 * n_p;
-  const int p0 = blockIdx.x * npb, np_here = min(npb, nparent - p0);
+  const int pb = blockIdx.x / chunks, chunk = blockIdx.x % chunks;
+  const int p0 = pb * npb, np_here = min(npb, nparent - p0);
   const float2 *base = mul + (size_t)rhs * mp + off_c;
   auto child = [&](int pc, int q) {
     return (size_t)((2 * (pc / n_p) + (q >> 1)) * n_c + 2 * (pc % n_p) + (q & 1)) * ns_c;
@@ -100,7 +101,8 @@ __global__ void __launch_bounds__(256) k_m2m(float2 *__restrict__ mul, size_t mp
     }
     __syncthreads();
   }
-  for (int u = threadIdx.x; u < np_here * ns_p; u += blockDim.x) {
+  const int per = (np_here * ns_p + chunks - 1) / chunks, u_hi = min(np_here * ns_p, (chunk + 1) * per);
+  for (int u = chunk * per + threadIdx.x; u < u_hi; u += blockDim.x) {
     const int pl = u / ns_p, km = u % ns_p, pc = p0 + pl;
     int idx = ifirst[km];
     float2 acc[4] = {};
@@ -245,7 +247,7 @@ __global__ void __launch_bounds__(256, 1) k_m2l(M2lArgs A) {
 // through L1 when one parent's rings are too large (top levels only).
 template <bool STAGE>
 __global__ void __launch_bounds__(256) k_l2l(float2 *__restrict__ loc, size_t mp, size_t off_p, size_t off_c, int n_p,
-                                             int ns_p, int ns_c, int npb, const int *__restrict__ afirst,
+                                             int ns_p, int ns_c, int npb, int chunks, const int *__restrict__ afirst,
                                              const float *__restrict__ aw, int awidth,
                                              const float2 *__restrict__ shl_p, int accumulate,
                                              const int *__restrict__ active) {
@@ -253,7 +255,8 @@ __global__ void __launch_bounds__(256) k_l2l(float2 *__restrict__ loc, size_t mp
   const int rhs = blockIdx.y;
   if (inactive(active, rhs)) return;
   const int nparent = n_p * n_p, n_c = 2 * n_p;
-  const int p0 = blockIdx.x * npb, np_here = min(npb, nparent - p0);
+  const int pb = blockIdx.x / chunks, chunk = blockIdx.x % chunks;
+  const int p0 = pb * npb, np_here = min(npb, nparent - p0);
   const float2 *lp0 = loc + (size_t)rhs * mp + off_p;
   if (STAGE) {
     for (int e = threadIdx.x; e < np_here * 4 * ns_p; e += blockDim.x) {
@@ -263,7 +266,8 @@ __global__ void __launch_bounds__(256) k_l2l(float2 *__restrict__ loc, size_t mp
     __syncthreads();
   }
   float2 *lc = loc + (size_t)rhs * mp + off_c;
-  for (int u = threadIdx.x; u < np_here * ns_c; u += blockDim.x) {
+  const int per = (np_here * ns_c + chunks - 1) / chunks, u_hi = min(np_here * ns_c, (chunk + 1) * per);
+  for (int u = chunk * per + threadIdx.x; u < u_hi; u += blockDim.x) {
     const int pl = u / ns_c, km = u % ns_c, pc = p0 + pl;
     const float2 *lp = lp0 + (size_t)pc * ns_p;
     int idx = afirst[km];
@@ -477,21 +481,31 @@ static int parents_per_block(size_t ring_bytes, int nparent) {
   return std::min(npb, std::max(1, nparent));
 }
 
+// Splits each block's outputs over several blocks when the level has too few
+// parents to fill the GPU (the top levels, and any level at small batches).
+static int output_chunks(int blocks, int nrhs, int npb, int ns_out) {
+  const int want = 2 * 148;
+  if (npb != 1 || blocks * nrhs >= want) return 1;
+  return std::max(1, std::min((ns_out + 127) / 128, (want + blocks * nrhs - 1) / (blocks * nrhs)));
+}
+
 void launch_m2m(const DevPlan &P, int lvl, float2 *mul, int nrhs, const int *active, cudaStream_t st) {
   const DevLevel &p = P.lv[lvl], &c = P.lv[lvl + 1];
   const size_t ring = (size_t)4 * c.ns * sizeof(float2);
   const int nparent = p.n * p.n;
   count_launch();
   if (ring <= (size_t)kSmemStage) {
-    const int npb = parents_per_block(ring, nparent);
+    const int npb = parents_per_block(ring, nparent), blocks = (nparent + npb - 1) / npb;
+    const int chunks = output_chunks(blocks, nrhs, npb, p.ns);
     const size_t smem = ring * npb;
     if (smem > 48 * 1024) cudaFuncSetAttribute(k_m2m<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    dim3 grid((nparent + npb - 1) / npb, nrhs);
-    k_m2m<true><<<grid, 256, smem, st>>>(mul, P.mp, p.off, c.off, p.n, p.ns, c.ns, npb, p.ifirst, p.iw, p.shm,
-                                         P.ninter, active);
+    dim3 grid(blocks * chunks, nrhs);
+    k_m2m<true><<<grid, 256, smem, st>>>(mul, P.mp, p.off, c.off, p.n, p.ns, c.ns, npb, chunks, p.ifirst, p.iw,
+                                         p.shm, P.ninter, active);
   } else {
-    dim3 grid(nparent, nrhs);
-    k_m2m<false><<<grid, 256, 0, st>>>(mul, P.mp, p.off, c.off, p.n, p.ns, c.ns, 1, p.ifirst, p.iw, p.shm,
+    const int chunks = output_chunks(nparent, nrhs, 1, p.ns);
+    dim3 grid(nparent * chunks, nrhs);
+    k_m2m<false><<<grid, 256, 0, st>>>(mul, P.mp, p.off, c.off, p.n, p.ns, c.ns, 1, chunks, p.ifirst, p.iw, p.shm,
                                        P.ninter, active);
   }
 }
@@ -527,16 +541,18 @@ void launch_l2l(const DevPlan &P, int lvl, float2 *loc, int nrhs, const int *act
   const int nparent = p.n * p.n;
   count_launch();
   if (ring <= (size_t)kSmemStage) {
-    const int npb = parents_per_block(ring, nparent);
+    const int npb = parents_per_block(ring, nparent), blocks = (nparent + npb - 1) / npb;
+    const int chunks = output_chunks(blocks, nrhs, npb, c.ns);
     const size_t smem = ring * npb;
     if (smem > 48 * 1024) cudaFuncSetAttribute(k_l2l<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    dim3 grid((nparent + npb - 1) / npb, nrhs);
-    k_l2l<true><<<grid, 256, smem, st>>>(loc, P.mp, p.off, c.off, p.n, p.ns, c.ns, npb, c.afirst, c.aw, c.awidth,
-                                         p.shl, accumulate ? 1 : 0, active);
+    dim3 grid(blocks * chunks, nrhs);
+    k_l2l<true><<<grid, 256, smem, st>>>(loc, P.mp, p.off, c.off, p.n, p.ns, c.ns, npb, chunks, c.afirst, c.aw,
+                                         c.awidth, p.shl, accumulate ? 1 : 0, active);
   } else {
-    dim3 grid(nparent, nrhs);
-    k_l2l<false><<<grid, 256, 0, st>>>(loc, P.mp, p.off, c.off, p.n, p.ns, c.ns, 1, c.afirst, c.aw, c.awidth,
-                                       p.shl, accumulate ? 1 : 0, active);
+    const int chunks = output_chunks(nparent, nrhs, 1, c.ns);
+    dim3 grid(nparent * chunks, nrhs);
+    k_l2l<false><<<grid, 256, 0, st>>>(loc, P.mp, p.off, c.off, p.n, p.ns, c.ns, 1, chunks, c.afirst, c.aw,
+                                       c.awidth, p.shl, accumulate ? 1 : 0, active);
   }
 }
 
