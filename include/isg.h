@@ -148,6 +148,24 @@ isg_status isg_aggregate(isg_ctx *ctx, const void *x, void *rx, int nrhs, int or
  * solve.cpp:356-456), all levels on the device. */
 isg_status isg_aggregateh(isg_ctx *ctx, void *x, const void *rx, int nrhs, int order, isg_stream stream);
 
+/* Size of the device array isg_aggregate_noalloc works in (one per device). */
+#define ISG_STATIC_SCRATCH_BYTES (64u << 20)
+/* Same result as isg_aggregate, but allocates nothing: no cudaMalloc (which
+ * can synchronise the whole device), no use of the context's workspaces.  For
+ * callers that must not allocate at that point, e.g. a driver whose HBM is
+ * fully committed to solve workspaces, or a loop that cannot afford an
+ * allocator's device-wide synchronisation.  No counterpart in the reference.
+ *  - isg_setup_gpu(ctx) must have run (ISG_BAD_ARG otherwise).
+ *  - Works in a fixed array of ISG_STATIC_SCRATCH_BYTES inside libisg.so:
+ *    nrhs * (multipole samples per RHS, plus numunk unless order is
+ *    ISG_ORDER_BLOCKED) * 8 bytes must fit, else ISG_BAD_ARG with the limit in
+ *    isg_last_error (level 8: 2 RHS in tree/raster order, 4 in blocked order).
+ *  - The first call on each device looks the array's address up
+ *    (cudaGetSymbolAddress); make that first call before any stream capture.
+ *  - One array per device per process: calls that overlap in time on the same
+ *    device (other streams, threads or contexts) race on it. */
+isg_status isg_aggregate_noalloc(isg_ctx *ctx, const void *x, void *rx, int nrhs, int order, isg_stream stream);
+
 /* ---- inversion (distorted-Born / Polak-Ribiere nonlinear CG, mom.cpp:222-399) ---- */
 typedef struct isg_dbim_opts {
   int iterations;        /* Polak-Ribiere iterations (mom.cpp:277 runs 3) */

@@ -98,6 +98,7 @@ SIGNATURES = {
     "isg_bicgs": (_I, [_P, _P, _P, _L, _P, _I, _I, _I, ctypes.POINTER(SolveOpts), ctypes.POINTER(SolveInfo), _P]),
     "isg_aggregate": (_I, [_P, _P, _P, _I, _I, _P]),
     "isg_aggregateh": (_I, [_P, _P, _P, _I, _I, _P]),
+    "isg_aggregate_noalloc": (_I, [_P, _P, _P, _I, _I, _P]),
     "isg_default_dbim_opts": (None, [ctypes.POINTER(DbimOpts)]),
     "isg_measure": (_I, [_P, _I, _P, _P, _I, _D, ctypes.c_uint64, ctypes.POINTER(SolveOpts), _P, _P]),
     "isg_dbim": (_I, [_P, _I, _P, _P, _P, _P, _I, ctypes.POINTER(DbimOpts), ctypes.POINTER(DbimRecord), _P]),
