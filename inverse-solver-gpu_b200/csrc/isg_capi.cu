@@ -40,7 +40,7 @@ isg_status run_aggregate(isg_ctx *c, const float2 *xb, float2 *rx, int nrhs, cud
 isg_status run_aggregateh(isg_ctx *c, float2 *xb, const float2 *rx, int nrhs, cudaStream_t st) {
   const float scale = (float)(-4.0 * c->T.numrx * c->T.res * c->T.res);
   launch_rx_anterp(c->P, rx, c->loc, nrhs, make_float2(0.f, scale), st);
-  for (int i = 1; i < c->P.L; i++) launch_l2l(c->P, i, c->loc, nrhs, nullptr, false, st);
+  for (int i = 1; i < c->P.L; i++) launch_l2l(c->P, i, c->loc, nrhs, nullptr, st);
   NearArgs A;
   A.in.nrhs = nrhs;
   A.loc = c->loc;
@@ -63,6 +63,47 @@ isg_status upload(isg_ctx *c, T **dst, const std::vector<T> &src) {
   *dst = (T *)p;
   if (!src.empty()) e = cuda_check(c, cudaMemcpy(p, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
   return e;
+}
+
+// Tiles of `out` output samples of a banded resampling whose output sample k
+// reads input (idx[k * stride] + t) mod ns_in with weight wt[k * stride + t],
+// t < width (the kernels' circular tap walk).
+isg_status upload_tile_band(isg_ctx *c, TileBand *tb, const std::vector<int> &idx, const std::vector<double> &wt,
+                            int stride, int width, int ns_out, int ns_in, int out) {
+  const int tiles = (ns_out + out - 1) / out;
+  std::vector<int> a0(tiles), wl(tiles);
+  auto rel = [&](int t, int k, int u) { return ((idx[(size_t)k * stride] + u - a0[t]) % ns_in + ns_in) % ns_in; };
+  int wmax = 1;
+  for (int t = 0; t < tiles; t++) {
+    a0[t] = idx[(size_t)t * out * stride];
+    int len = 1;
+    for (int k = t * out; k < std::min(ns_out, (t + 1) * out); k++)
+      for (int u = 0; u < width; u++) len = std::max(len, rel(t, k, u) + 1);
+    wl[t] = len;
+    wmax = std::max(wmax, len);
+  }
+  std::vector<float> w((size_t)tiles * wmax * out, 0.f);
+  for (int t = 0; t < tiles; t++)
+    for (int k = t * out; k < std::min(ns_out, (t + 1) * out); k++)
+      for (int u = 0; u < width; u++)
+        w[((size_t)t * wmax + rel(t, k, u)) * out + (k - t * out)] += (float)wt[(size_t)k * stride + u];
+  tb->tiles = tiles;
+  tb->wmax = wmax;
+  tb->out = out;
+  isg_status e;
+  if ((e = upload(c, &tb->w, w)) || (e = upload(c, &tb->a0, a0)) || (e = upload(c, &tb->wl, wl))) return e;
+  return ISG_OK;
+}
+
+// [4][ns] -> [ns][4]
+std::vector<float2> transpose4(const std::vector<cd> &v, int ns) {
+  std::vector<float2> o((size_t)4 * ns);
+  for (int q = 0; q < 4; q++)
+    for (int k = 0; k < ns; k++) {
+      const cd z = v[(size_t)q * ns + k];
+      o[(size_t)k * 4 + q] = make_float2((float)z.real(), (float)z.imag());
+    }
+  return o;
 }
 
 template <class T>
@@ -256,6 +297,10 @@ isg_status isg_setup_gpu(isg_ctx *c) {
       if ((e = upload(c, &d.ifirst, f)) || (e = upload(c, &d.iw, w)) || (e = upload(c, &d.shm, sm)) ||
           (e = upload(c, &d.shl, sl)))
         return e;
+      if ((e = upload_tile_band(c, &d.mt, T.intind[i], T.interp[i], ni, ni, d.ns, T.nsamp[i + 1], 2 * kTileOut)) ||
+          (e = upload(c, &d.shmT, transpose4(T.shiftmul[i], d.ns))) ||
+          (e = upload(c, &d.shlT, transpose4(T.shiftloc[i], d.ns))))
+        return e;
     }
     if (i >= 1) {
       d.awidth = T.antcount[i];
@@ -266,6 +311,8 @@ isg_status isg_setup_gpu(isg_ctx *c) {
         for (int t = 0; t < d.awidth; t++) w[(size_t)t * d.ns + k] = (float)T.anterp[i][(size_t)k * W + t];
       }
       if ((e = upload(c, &d.afirst, f)) || (e = upload(c, &d.aw, w))) return e;
+      if ((e = upload_tile_band(c, &d.at, T.antind[i], T.anterp[i], W, d.awidth, d.ns, T.nsamp[i - 1], 2 * kTileOut)))
+        return e;
     }
     if (i >= 2) {
       std::vector<float2> tr(T.trans[i].size());
@@ -501,9 +548,10 @@ isg_status isg_time_stages(isg_ctx *c, int nrhs, int engine, int reps, double *m
     for (int i = P.L - 2; i >= 2; i--)
       if (!(tc && band_m2m(c, i, c->mul, nrhs, nullptr, st, &be))) launch_m2m(P, i, c->mul, nrhs, nullptr, st);
     cudaEventRecord(ev[2], st);
-    for (int i = 2; i < P.L; i++) launch_m2l(P, i, c->mul, c->loc, nrhs, nullptr, st);
-    for (int i = 3; i < P.L; i++)
-      if (!(tc && band_l2l(c, i, c->loc, nrhs, nullptr, true, st, &be))) launch_l2l(P, i, c->loc, nrhs, nullptr, true, st);
+    for (int i = 2; i < P.L; i++) {
+      if (i >= 3) launch_l2l(P, i, c->loc, nrhs, nullptr, st);
+      launch_m2l(P, i, c->mul, c->loc, nrhs, nullptr, i >= 3, st);
+    }
     cudaEventRecord(ev[3], st);
     if (tc) tc_near(c, A, st); else launch_near(P, A, st);
     cudaEventRecord(ev[4], st);

@@ -23,7 +23,7 @@ struct RhsState {
 };
 
 struct TcPlan;    // tensor-core leaf stage tables (isg_tc.cu)
-struct BandPlan;  // tensor-core M2M/L2L tables (isg_tc_band.cu)
+struct BandPlan;  // tensor-core M2M tables (isg_tc_band.cu)
 
 }  // namespace isg
 
@@ -75,11 +75,9 @@ isg_status tc_near(isg_ctx *c, const NearArgs &A, cudaStream_t st);
 int tc_near_blocks(const isg_ctx *c);
 // Nonzero when a bounded wait inside a tensor-core kernel gave up.
 int tc_error(isg_ctx *c);
-// Tensor-core M2M into parent level lvl / L2L into child level lvl; false when
+// Tensor-core M2M into parent level lvl; false when
 // the transition has no tensor-core tables (the caller uses the SIMT kernel).
 isg_status band_setup(isg_ctx *c);
 void band_destroy(isg_ctx *c);
 bool band_m2m(isg_ctx *c, int lvl, float2 *mul, int nrhs, const int *active, cudaStream_t st, isg_status *e);
-bool band_l2l(isg_ctx *c, int lvl, float2 *loc, int nrhs, const int *active, bool accumulate, cudaStream_t st,
-              isg_status *e);
 }  // namespace isg

@@ -12,6 +12,18 @@ constexpr int kMaxLevels = 12;
 constexpr int kBox = 8;
 constexpr int kBB = 64;  // pixels per leaf
 
+// A banded resampling (interpolation or anterpolation) cut into tiles of `out`
+// consecutive output samples (a multiple of kTileOut, the outputs one thread
+// accumulates): tile t reads the circular window of wl[t] input samples
+// starting at a0[t], with weights w[t][jj][i] (jj < wmax, zero padded)
+// relative to that window.
+constexpr int kTileOut = 8;
+struct TileBand {
+  float *w = nullptr;  // [tiles][wmax][out]
+  int *a0 = nullptr, *wl = nullptr;
+  int tiles = 0, wmax = 0, out = kTileOut;
+};
+
 // Per-level device tables.  Level numbering is the reference's (0 = root).
 struct DevLevel {
   int n = 0;        // clusters per side (2^level)
@@ -27,6 +39,10 @@ struct DevLevel {
   float *aw = nullptr;     // [awidth][ns]
   int awidth = 0;
   float2 *T = nullptr;     // [49][ns] translation operators (level >= 2)
+  TileBand mt;             // interpolation into this level (M2M), tiled
+  TileBand at;             // anterpolation into this level (L2L), tiled
+  float2 *shmT = nullptr;  // [ns][4] shm transposed
+  float2 *shlT = nullptr;  // [ns][4] shl transposed
 };
 
 struct DevPlan {
@@ -98,12 +114,11 @@ int64_t launch_count();
 // ---- launchers (isg_kernels.cu) ----
 void launch_p2m(const DevPlan &P, const BatchArgs &B, float2 *mul, cudaStream_t st);
 void launch_m2m(const DevPlan &P, int lvl, float2 *mul, int nrhs, const int *active, cudaStream_t st);
-// M2L into level lvl (overwrites its local expansions).
-void launch_m2l(const DevPlan &P, int lvl, const float2 *mul, float2 *loc, int nrhs, const int *active,
+// M2L into level lvl: written over its local expansions, or added to them.
+void launch_m2l(const DevPlan &P, int lvl, const float2 *mul, float2 *loc, int nrhs, const int *active, bool accumulate,
                 cudaStream_t st);
-// L2L from level lvl-1 into level lvl, added to or written over its locals.
-void launch_l2l(const DevPlan &P, int lvl, float2 *loc, int nrhs, const int *active, bool accumulate,
-                cudaStream_t st);
+// L2L from level lvl-1 into level lvl, written over its locals.
+void launch_l2l(const DevPlan &P, int lvl, float2 *loc, int nrhs, const int *active, cudaStream_t st);
 // y = epilogue(L2P(loc_leaf) + near(x)); optional FP64 partials per block.
 struct NearArgs {
   BatchArgs in;

@@ -61,237 +61,312 @@ __global__ void __launch_bounds__(128) k_p2m(const float2 *__restrict__ x, const
   }
 }
 
-constexpr int kSmemStage = 200 * 1024;  // largest ring staged in shared memory
-constexpr int kStageBudget = 32 * 1024;  // per-block staging target for the small levels
 
 __device__ __forceinline__ void cp_async8(void *smem, const void *gmem, bool valid) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(valid ? 8 : 0));
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
-// Block-wide barrier usable from warp-uniform divergent paths (every warp
-// reaches it the same number of times).
-__device__ __forceinline__ void block_bar1() { asm volatile("bar.sync 1, %0;\n" ::"r"(blockDim.x)); }
-
-// M2M (kernels.cu:83-136, solve.cpp:93-112): parent sample km gathers the
-// 30-tap interpolation of each of its four children, shifts it to the parent
-// centre and sums.  A block covers `npb` parents whose children's rings are
-// staged in shared memory (STAGE), or reads through L1 when one parent's
-// children are too large to stage (top levels only).
-template <bool STAGE>
-__global__ void __launch_bounds__(256) k_m2m(float2 *__restrict__ mul, size_t mp, size_t off_p, size_t off_c, int n_p,
-                                             int ns_p, int ns_c, int npb, int chunks, const int *__restrict__ ifirst,
-                                             const float *__restrict__ iw, const float2 *__restrict__ shm,
-                                             int ninter, const int *__restrict__ active) {
-  extern __shared__ float2 chs[];
-  const int rhs = blockIdx.y;
-  if (inactive(active, rhs)) return;
-  const int nparent = n_p * n_p, n_c = 2 * n_p;
-  const int pb = blockIdx.x / chunks, chunk = blockIdx.x % chunks;
-  const int p0 = pb * npb, np_here = min(npb, nparent - p0);
-  const float2 *base = mul + (size_t)rhs * mp + off_c;
-  auto child = [&](int pc, int q) {
-    return (size_t)((2 * (pc / n_p) + (q >> 1)) * n_c + 2 * (pc % n_p) + (q & 1)) * ns_c;
-  };
-  if (STAGE) {
-    for (int e = threadIdx.x; e < np_here * 4 * ns_c; e += blockDim.x) {
-      const int j = e % ns_c, q = (e / ns_c) & 3, pl = e / (4 * ns_c);
-      chs[e] = base[child(p0 + pl, q) + j];
-    }
-    __syncthreads();
-  }
-  const int per = (np_here * ns_p + chunks - 1) / chunks, u_hi = min(np_here * ns_p, (chunk + 1) * per);
-  for (int u = chunk * per + threadIdx.x; u < u_hi; u += blockDim.x) {
-    const int pl = u / ns_p, km = u % ns_p, pc = p0 + pl;
-    int idx = ifirst[km];
-    float2 acc[4] = {};
-    for (int t = 0; t < ninter; t++) {
-      const float w = __ldg(&iw[t * ns_p + km]);
-#pragma unroll
-      for (int q = 0; q < 4; q++) rfma(acc[q], w, STAGE ? chs[(pl * 4 + q) * ns_c + idx] : base[child(pc, q) + idx]);
-      if (++idx == ns_c) idx = 0;
-    }
-    float2 res = make_float2(0.f, 0.f);
-#pragma unroll
-    for (int q = 0; q < 4; q++) cfma(res, __ldg(&shm[q * ns_p + km]), acc[q]);
-    mul[(size_t)rhs * mp + off_p + (size_t)pc * ns_p + km] = res;
-  }
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
 }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // M2L (kernels.cu:239-266, solve.cpp:133-148) as a 2-D stencil per sample.
 // The far list of a cluster is the 6x6 block of its parent's neighbours'
-// children minus its own 3x3 neighbourhood, clipped to the grid, so for a
-// cluster of parity (OY, OX) at row 2a+OY the sources are rows 2a-2 .. 2a+3
-// of a six-column window, and the 27 translation weights depend only on the
-// parity and the sample.  A block owns one chunk of 32 samples: each thread
-// keeps its 27 weights in registers for the whole launch and walks a list of
-// (tile of 16 x 4 clusters, RHS) items, sliding a 6x6 register window of
-// multipoles down a column of eight same-parity clusters.  The (16+4) x (4+4)
-// halo of the next item is fetched with cp.async while the current one is
-// computed.
-constexpr int kM2lRows = 16, kM2lCols = 4, kM2lKC = 32;
-constexpr int kM2lHR = kM2lRows + 4, kM2lHC = kM2lCols + 4;
-constexpr int kM2lHalo = kM2lHR * kM2lHC * kM2lKC;
-
+// children minus its own 3x3 neighbourhood, clipped to the grid, so the four
+// siblings of a 2x2 group at rows 2a, 2a+1 all draw on rows 2a-2 .. 2a+3 of
+// the same six-column window, each with 27 of the 40 translation weights
+// T[(dy+3)*7+dx+3][k] whose offset is not inside the 3x3.  A thread owns one
+// sample k of one column of sibling groups: it keeps the 40 weights in
+// registers, slides the 6x6 window of multipoles down `ty` groups (two new
+// rows per step, read straight from L1/L2 and prefetched one step ahead) and
+// writes (or adds to, after L2L) the four siblings' locals per step: 108
+// complex FMAs per 12 loads.
+// Consecutive threads take consecutive samples, so every load and store is
+// coalesced along the cluster's samples.
 struct M2lArgs {
   const float2 *mul;
   float2 *loc;
   size_t mp, off;
-  int n, ns, tiles_x, tiles, nitems;
+  int n, ns, ty, accumulate;
   const float2 *T;
   const int *active;
 };
 
-__device__ __forceinline__ void m2l_issue(const M2lArgs &A, int item, int k0, float2 *buf) {
-  const int tile = item % A.tiles, rhs = item / A.tiles;
-  const int cy0 = (tile / A.tiles_x) * kM2lRows, cx0 = (tile % A.tiles_x) * kM2lCols;
-  const float2 *m = A.mul + (size_t)rhs * A.mp + A.off;
-  for (int e = threadIdx.x; e < kM2lHalo; e += blockDim.x) {
-    const int kk = e % kM2lKC, hc = (e / kM2lKC) % kM2lHC, hr = e / (kM2lKC * kM2lHC);
-    const int cy = cy0 - 2 + hr, cx = cx0 - 2 + hc, k = k0 + kk;
-    const bool ok = cy >= 0 && cy < A.n && cx >= 0 && cx < A.n && k < A.ns;
-    cp_async8(&buf[e], ok ? (const void *)&m[(size_t)(cy * A.n + cx) * A.ns + k] : (const void *)A.mul, ok);
-  }
-}
-
-// One window step: rows of the 6x6 window live in six register slots that
-// rotate by two per step (ROT = step mod 3), so no registers are moved.
-template <int OY, int OX, int ROT>
-__device__ __forceinline__ void m2l_step(const float2 (*hs)[kM2lHC][kM2lKC], float2 (&w)[6][6],
-                                         const float2 (&tw)[6][6], int a, int b, int kk, int cy0, int cx0,
-                                         bool live, const M2lArgs &A, int k, float2 *out) {
-  constexpr int NR0 = OY + 1, NC0 = OX + 1;  // first near row/column inside the window
+__global__ void __launch_bounds__(128, 2) k_m2l(M2lArgs A) {
+  const int rhs = blockIdx.z;
+  if (A.active && !A.active[rhs]) return;
+  const int half = A.n >> 1, ns = A.ns;
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= half * ns) return;
+  const int b = f / ns, k = f - b * ns;
+  const int a0 = blockIdx.y * A.ty, a1 = min(a0 + A.ty, half);
+  float2 tw[7][7];
+#pragma unroll
+  for (int dy = 0; dy < 7; dy++)
+#pragma unroll
+    for (int dx = 0; dx < 7; dx++)
+      tw[dy][dx] = (dy >= 2 && dy <= 4 && dx >= 2 && dx <= 4) ? make_float2(0.f, 0.f)
+                                                              : __ldg(&A.T[(dy * 7 + dx) * ns + k]);
+  const float2 *m = A.mul + (size_t)rhs * A.mp + A.off + k;
+  float2 *out = A.loc + (size_t)rhs * A.mp + A.off + k;
+  const size_t row_stride = (size_t)A.n * ns;
+  int cofs[6];
+  bool cok[6];
 #pragma unroll
   for (int j = 0; j < 6; j++) {
-    w[(4 + 2 * ROT) % 6][j] = hs[2 * a + 4][2 * b + j][kk];
-    w[(5 + 2 * ROT) % 6][j] = hs[2 * a + 5][2 * b + j][kk];
+    const int col = 2 * b - 2 + j;
+    cok[j] = col >= 0 && col < A.n;
+    cofs[j] = col * ns;
   }
-  float2 acc[3] = {};
-  int term = 0;
+  auto load_row = [&](int row, float2 (&dst)[6]) {
+    const bool rok = row >= 0 && row < A.n;
+    const float2 *rp = m + (ptrdiff_t)(rok ? row : 0) * (ptrdiff_t)row_stride;
 #pragma unroll
-  for (int i = 0; i < 6; i++)
+    for (int j = 0; j < 6; j++) dst[j] = (rok && cok[j]) ? __ldg(rp + cofs[j]) : make_float2(0.f, 0.f);
+  };
+  // the sibling group's current locals (added to when accumulating), one step ahead
+  auto load_old = [&](int a, float2 (&dst)[2][2]) {
+#pragma unroll
+    for (int oy = 0; oy < 2; oy++)
+#pragma unroll
+      for (int ox = 0; ox < 2; ox++)
+        dst[oy][ox] = A.accumulate ? out[(ptrdiff_t)(2 * a + oy) * (ptrdiff_t)row_stride + (2 * b + ox) * ns]
+                                   : make_float2(0.f, 0.f);
+  };
+  float2 w[6][6], pre[2][6], old[2][2];
+#pragma unroll
+  for (int i = 0; i < 4; i++) load_row(2 * a0 - 2 + i, w[i]);
+  load_row(2 * a0 + 2, pre[0]);
+  load_row(2 * a0 + 3, pre[1]);
+  load_old(a0, old);
+#pragma unroll 1
+  for (int a = a0; a < a1; a++) {
 #pragma unroll
     for (int j = 0; j < 6; j++) {
-      const bool nearby = (i >= NR0 && i < NR0 + 3 && j >= NC0 && j < NC0 + 3);
-      if (nearby) continue;
-      cfma(acc[term % 3], tw[i][j], w[(i + 2 * ROT) % 6][j]);
-      term++;
+      w[4][j] = pre[0][j];
+      w[5][j] = pre[1][j];
     }
-  const int cy = cy0 + 2 * a + OY, cx = cx0 + 2 * b + OX;
-  if (live && cy < A.n && cx < A.n && k < A.ns)
-    out[(size_t)(cy * A.n + cx) * A.ns + k] = cadd(acc[0], cadd(acc[1], acc[2]));
-}
-
-template <int OY, int OX>
-__device__ __forceinline__ void m2l_worker(const M2lArgs &A, float2 *hbuf) {
-  constexpr int NR0 = OY + 1, NC0 = OX + 1;
-  const int kk = threadIdx.x & 31, b = threadIdx.x >> 7;
-  const int k0 = blockIdx.x * kM2lKC, k = k0 + kk;
-  float2 tw[6][6];
+    float2 acc[2][2];
 #pragma unroll
-  for (int i = 0; i < 6; i++)
+    for (int oy = 0; oy < 2; oy++)
 #pragma unroll
-    for (int j = 0; j < 6; j++) {
-      const bool nearby = (i >= NR0 && i < NR0 + 3 && j >= NC0 && j < NC0 + 3);
-      tw[i][j] = (!nearby && k < A.ns) ? __ldg(&A.T[((i + 1 - OY) * 7 + (j + 1 - OX)) * A.ns + k])
-                                       : make_float2(0.f, 0.f);
+      for (int ox = 0; ox < 2; ox++) acc[oy][ox] = old[oy][ox];
+    if (a + 1 < a1) {
+      load_row(2 * a + 4, pre[0]);
+      load_row(2 * a + 5, pre[1]);
+      load_old(a + 1, old);
     }
-  int buf = 0;
-  const int G = gridDim.y;
-  for (int item = blockIdx.y; item < A.nitems; item += G) {
-    if (item + G < A.nitems) m2l_issue(A, item + G, k0, hbuf + (buf ^ 1) * kM2lHalo);
-    cp_async_commit();
-    cp_async_wait1();
-    block_bar1();
-    const float2(*hs)[kM2lHC][kM2lKC] = (const float2(*)[kM2lHC][kM2lKC])(hbuf + buf * kM2lHalo);
-    const int tile = item % A.tiles, rhs = item / A.tiles;
-    const bool live = !(A.active && !A.active[rhs]);
-    const int cy0 = (tile / A.tiles_x) * kM2lRows, cx0 = (tile % A.tiles_x) * kM2lCols;
-    float2 *out = A.loc + (size_t)rhs * A.mp + A.off;
-    float2 w[6][6];
+#pragma unroll
+    for (int i = 0; i < 6; i++)
+#pragma unroll
+      for (int j = 0; j < 6; j++)
+#pragma unroll
+        for (int oy = 0; oy < 2; oy++)
+#pragma unroll
+          for (int ox = 0; ox < 2; ox++) {
+            const int dy = i - 2 - oy, dx = j - 2 - ox;  // source minus target
+            if (dy >= -1 && dy <= 1 && dx >= -1 && dx <= 1) continue;
+            cfma(acc[oy][ox], tw[dy + 3][dx + 3], w[i][j]);
+          }
+#pragma unroll
+    for (int oy = 0; oy < 2; oy++)
+#pragma unroll
+      for (int ox = 0; ox < 2; ox++)
+        out[(ptrdiff_t)(2 * a + oy) * (ptrdiff_t)row_stride + (2 * b + ox) * ns] = acc[oy][ox];
 #pragma unroll
     for (int i = 0; i < 4; i++)
 #pragma unroll
-      for (int j = 0; j < 6; j++) w[i][j] = hs[i][2 * b + j][kk];
-    static_assert(kM2lRows / 2 == 8, "window walk is unrolled for eight steps");
-#pragma unroll 1
-    for (int a = 0; a < 6; a += 3) {
-      m2l_step<OY, OX, 0>(hs, w, tw, a, b, kk, cy0, cx0, live, A, k, out);
-      m2l_step<OY, OX, 1>(hs, w, tw, a + 1, b, kk, cy0, cx0, live, A, k, out);
-      m2l_step<OY, OX, 2>(hs, w, tw, a + 2, b, kk, cy0, cx0, live, A, k, out);
-    }
-    m2l_step<OY, OX, 0>(hs, w, tw, 6, b, kk, cy0, cx0, live, A, k, out);
-    m2l_step<OY, OX, 1>(hs, w, tw, 7, b, kk, cy0, cx0, live, A, k, out);
-    block_bar1();
-    buf ^= 1;
+      for (int j = 0; j < 6; j++) w[i][j] = w[i + 2][j];
   }
 }
 
-__global__ void __launch_bounds__(256, 1) k_m2l(M2lArgs A) {
-  extern __shared__ float2 hbuf[];
-  if (blockIdx.y < A.nitems) m2l_issue(A, blockIdx.y, blockIdx.x * kM2lKC, hbuf);
-  cp_async_commit();
-  switch ((threadIdx.x >> 5) & 3) {
-    case 0: m2l_worker<0, 0>(A, hbuf); break;
-    case 1: m2l_worker<0, 1>(A, hbuf); break;
-    case 2: m2l_worker<1, 0>(A, hbuf); break;
-    default: m2l_worker<1, 1>(A, hbuf); break;
+// Tiled M2M / L2L.  A column is one (RHS, parent) pair.  A block takes `cols`
+// columns and one tile of tb.out output samples; tb.out / kTileOut threads per
+// column each accumulate kTileOut of them.  The block stages the tile's input
+// window of every ring it reads in shared memory ([window sample][ring],
+// padded against bank conflicts) with cp.async, after one thread per ring has
+// worked out the ring's address.  Each thread then walks the window once with
+// its kTileOut x 4 accumulators live: the band weights (and the L2L shift
+// phases) are the same for every thread of the block, so each staged value
+// feeds 32 (M2M) or 36 (L2L) FMAs from registers.  Outputs go back through
+// shared memory so that every ring is written in runs of tb.out samples.
+struct TileArgs {
+  const float2 *src;
+  float2 *dst;
+  size_t mp, off_in, off_out;
+  int n_p, ns_in, ns_out, nparent, ncols, cols;
+  TileBand tb;
+  const float2 *shT;  // [ns][4]: L2L shiftloc of the parent level, M2M shiftmul of the parent level
+  const int *active;
+};
+
+// Shared-memory carve-up of one tiled block (float2 units, 16-byte aligned parts).
+struct TileSmem {
+  size_t win, w, sh, src, dst, total;
+  __host__ __device__ TileSmem(int wmax, int ld, int out, int nsrc, int ndst, size_t out_tile) {
+    auto up2 = [](size_t x) { return (x + 1) & ~(size_t)1; };
+    win = 0;
+    w = up2(((size_t)wmax * ld > out_tile ? (size_t)wmax * ld : out_tile));
+    sh = w + up2((size_t)wmax * out / 2);
+    src = sh + (size_t)wmax * 4;
+    dst = src + nsrc;
+    total = dst + ndst;
+  }
+};
+
+__device__ __forceinline__ const float2 *ring_ptr(const TileArgs &A, const float2 *base, size_t off, int gc, int q,
+                                                  int level_n, int ns) {
+  if (gc >= A.ncols) return nullptr;
+  const int rhs = gc / A.nparent, P = gc - rhs * A.nparent;
+  if (inactive(A.active, rhs)) return nullptr;
+  size_t cl = P;
+  if (q >= 0) {
+    const int py = P / A.n_p, px = P - py * A.n_p;
+    cl = (size_t)(2 * py + (q >> 1)) * level_n + 2 * px + (q & 1);
+  }
+  return base + (size_t)rhs * A.mp + off + cl * ns;
+}
+
+// L2L into the children of each column's parent: z = parent local, four
+// shifted copies shl[q][j] z[j], anterpolated by the tile's band weights and
+// written over the children's locals.
+__global__ void __launch_bounds__(128) k_l2l_tile(TileArgs A) {
+  extern __shared__ float2 sm[];
+  const int cols = A.cols, TO = A.tb.out, tile = blockIdx.y, c0 = blockIdx.x * cols;
+  const int a0 = A.tb.a0[tile], wl = A.tb.wl[tile], ld = cols + 1;
+  const TileSmem L(A.tb.wmax, ld, TO, cols, 4 * cols, (size_t)4 * TO * ld);
+  const float2 **sp = (const float2 **)(sm + L.src);
+  float2 **dp = (float2 **)(sm + L.dst);
+  float4 *sw = (float4 *)(sm + L.w);
+  float4 *ss = (float4 *)(sm + L.sh);
+  for (int t = threadIdx.x; t < 4 * cols; t += blockDim.x) {
+    if (t < cols) sp[t] = ring_ptr(A, A.src, A.off_in, c0 + t, -1, A.n_p, A.ns_in);
+    dp[t] = (float2 *)ring_ptr(A, A.dst, A.off_out, c0 + (t >> 2), t & 3, 2 * A.n_p, A.ns_out);
+  }
+  {
+    const float4 *wt = (const float4 *)(A.tb.w + (size_t)tile * A.tb.wmax * TO);
+    for (int e = threadIdx.x; e < wl * TO / 4; e += blockDim.x) cp_async16(sw + e, wt + e);
+    const float4 *sh = (const float4 *)A.shT;
+    for (int e = threadIdx.x; e < 2 * wl; e += blockDim.x) {
+      int j = a0 + (e >> 1);
+      if (j >= A.ns_in) j -= A.ns_in;
+      cp_async16(ss + e, sh + 2 * j + (e & 1));
+    }
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int r = warp; r < cols; r += nw) {
+    const float2 *ring = sp[r];
+    for (int jj = lane; jj < wl; jj += 32) {
+      int j = a0 + jj;
+      if (j >= A.ns_in) j -= A.ns_in;
+      cp_async8(&sm[jj * ld + r], ring ? ring + j : A.src, ring != nullptr);
+    }
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  const int col = threadIdx.x % cols, sub = threadIdx.x / cols;
+  float2 acc[kTileOut][4] = {};
+  const int wstep = TO / 4;
+#pragma unroll 2
+  for (int jj = 0; jj < wl; jj++) {
+    const float2 z = sm[jj * ld + col];
+    const float4 s01 = ss[2 * jj], s23 = ss[2 * jj + 1];
+    const float2 v[4] = {cmul(make_float2(s01.x, s01.y), z), cmul(make_float2(s01.z, s01.w), z),
+                         cmul(make_float2(s23.x, s23.y), z), cmul(make_float2(s23.z, s23.w), z)};
+    const float4 w0 = sw[jj * wstep + 2 * sub], w1 = sw[jj * wstep + 2 * sub + 1];
+    const float wv[kTileOut] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+#pragma unroll
+    for (int i = 0; i < kTileOut; i++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) rfma(acc[i][q], wv[i], v[q]);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < 4; q++)
+#pragma unroll
+    for (int i = 0; i < kTileOut; i++) sm[(q * TO + sub * kTileOut + i) * ld + col] = acc[i][q];
+  __syncthreads();
+  for (int e = threadIdx.x; e < cols * 4 * TO; e += blockDim.x) {
+    const int i = e % TO, cq = e / TO, km = tile * TO + i;
+    float2 *d = dp[cq];
+    if (d && km < A.ns_out) d[km] = sm[((cq & 3) * TO + i) * ld + (cq >> 2)];
   }
 }
 
-// L2L (kernels.cu:137-238, solve.cpp:149-169 and 389-429): the parent's local
-// expansion, shifted to each child centre, anterpolated to the child rate and
-// added to (or written over) the child's local expansion.  A block covers `npb`
-// parents whose four shifted rings are staged in shared memory, or reads
-// through L1 when one parent's rings are too large (top levels only).
-template <bool STAGE>
-__global__ void __launch_bounds__(256) k_l2l(float2 *__restrict__ loc, size_t mp, size_t off_p, size_t off_c, int n_p,
-                                             int ns_p, int ns_c, int npb, int chunks, const int *__restrict__ afirst,
-                                             const float *__restrict__ aw, int awidth,
-                                             const float2 *__restrict__ shl_p, int accumulate,
-                                             const int *__restrict__ active) {
-  extern __shared__ float2 tmp[];
-  const int rhs = blockIdx.y;
-  if (inactive(active, rhs)) return;
-  const int nparent = n_p * n_p, n_c = 2 * n_p;
-  const int pb = blockIdx.x / chunks, chunk = blockIdx.x % chunks;
-  const int p0 = pb * npb, np_here = min(npb, nparent - p0);
-  const float2 *lp0 = loc + (size_t)rhs * mp + off_p;
-  if (STAGE) {
-    for (int e = threadIdx.x; e < np_here * 4 * ns_p; e += blockDim.x) {
-      const int j = e % ns_p, q = (e / ns_p) & 3, pl = e / (4 * ns_p);
-      tmp[e] = cmul(__ldg(&shl_p[q * ns_p + j]), lp0[(size_t)(p0 + pl) * ns_p + j]);
-    }
-    __syncthreads();
+// M2M into each column's parent: the four children's rings interpolated by the
+// tile's band weights, then shifted by shm[q][k] and summed.
+__global__ void __launch_bounds__(128) k_m2m_tile(TileArgs A) {
+  extern __shared__ float2 sm[];
+  const int cols = A.cols, TO = A.tb.out, tile = blockIdx.y, c0 = blockIdx.x * cols;
+  const int a0 = A.tb.a0[tile], wl = A.tb.wl[tile], ld = 4 * cols + 1;
+  const TileSmem L(A.tb.wmax, ld, TO, 4 * cols, cols, (size_t)TO * (cols + 1));
+  const float2 **sp = (const float2 **)(sm + L.src);
+  float2 **dp = (float2 **)(sm + L.dst);
+  float4 *sw = (float4 *)(sm + L.w);
+  const int n_c = 2 * A.n_p;
+  for (int t = threadIdx.x; t < 4 * cols; t += blockDim.x) {
+    sp[t] = ring_ptr(A, A.src, A.off_in, c0 + (t >> 2), t & 3, n_c, A.ns_in);
+    if (t < cols) dp[t] = (float2 *)ring_ptr(A, A.dst, A.off_out, c0 + t, -1, A.n_p, A.ns_out);
   }
-  float2 *lc = loc + (size_t)rhs * mp + off_c;
-  const int per = (np_here * ns_c + chunks - 1) / chunks, u_hi = min(np_here * ns_c, (chunk + 1) * per);
-  for (int u = chunk * per + threadIdx.x; u < u_hi; u += blockDim.x) {
-    const int pl = u / ns_c, km = u % ns_c, pc = p0 + pl;
-    const float2 *lp = lp0 + (size_t)pc * ns_p;
-    int idx = afirst[km];
-    float2 acc[4] = {};
-    for (int t = 0; t < awidth; t++) {
-      const float w = __ldg(&aw[t * ns_c + km]);
-      if (STAGE) {
-#pragma unroll
-        for (int q = 0; q < 4; q++) rfma(acc[q], w, tmp[(pl * 4 + q) * ns_p + idx]);
-      } else {
-        const float2 v = lp[idx];
-#pragma unroll
-        for (int q = 0; q < 4; q++) rfma(acc[q], w, cmul(__ldg(&shl_p[q * ns_p + idx]), v));
-      }
-      if (++idx == ns_p) idx = 0;
+  {
+    const float4 *wt = (const float4 *)(A.tb.w + (size_t)tile * A.tb.wmax * TO);
+    for (int e = threadIdx.x; e < wl * TO / 4; e += blockDim.x) cp_async16(sw + e, wt + e);
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int r = warp; r < 4 * cols; r += nw) {
+    const float2 *ring = sp[r];
+    float2 *dst = sm + (r & 3) * cols + (r >> 2);
+    for (int jj = lane; jj < wl; jj += 32) {
+      int j = a0 + jj;
+      if (j >= A.ns_in) j -= A.ns_in;
+      cp_async8(dst + jj * ld, ring ? ring + j : A.src, ring != nullptr);
     }
-    const int py = pc / n_p, px = pc % n_p;
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  const int col = threadIdx.x % cols, sub = threadIdx.x / cols;
+  float2 acc[kTileOut][4] = {};
+  const int wstep = TO / 4;
+#pragma unroll 2
+  for (int jj = 0; jj < wl; jj++) {
+    float2 v[4];
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-      float2 *d = lc + (size_t)((2 * py + (q >> 1)) * n_c + 2 * px + (q & 1)) * ns_c + km;
-      *d = accumulate ? cadd(*d, acc[q]) : acc[q];
-    }
+    for (int q = 0; q < 4; q++) v[q] = sm[jj * ld + q * cols + col];
+    const float4 w0 = sw[jj * wstep + 2 * sub], w1 = sw[jj * wstep + 2 * sub + 1];
+    const float wv[kTileOut] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+#pragma unroll
+    for (int i = 0; i < kTileOut; i++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) rfma(acc[i][q], wv[i], v[q]);
+  }
+  const float4 *sh = (const float4 *)A.shT;
+  float2 res[kTileOut];
+#pragma unroll
+  for (int i = 0; i < kTileOut; i++) {
+    const int k = min(tile * TO + sub * kTileOut + i, A.ns_out - 1);
+    const float4 s01 = __ldg(sh + 2 * k), s23 = __ldg(sh + 2 * k + 1);
+    res[i] = make_float2(0.f, 0.f);
+    cfma(res[i], make_float2(s01.x, s01.y), acc[i][0]);
+    cfma(res[i], make_float2(s01.z, s01.w), acc[i][1]);
+    cfma(res[i], make_float2(s23.x, s23.y), acc[i][2]);
+    cfma(res[i], make_float2(s23.z, s23.w), acc[i][3]);
+  }
+  __syncthreads();
+  const int ldo = cols + 1;
+#pragma unroll
+  for (int i = 0; i < kTileOut; i++) sm[(sub * kTileOut + i) * ldo + col] = res[i];
+  __syncthreads();
+  for (int e = threadIdx.x; e < cols * TO; e += blockDim.x) {
+    const int i = e % TO, cl = e / TO, kp = tile * TO + i;
+    float2 *d = dp[cl];
+    if (d && kp < A.ns_out) d[kp] = sm[i * ldo + cl];
   }
 }
+
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -475,42 +550,38 @@ void launch_p2m(const DevPlan &P, const BatchArgs &B, float2 *mul, cudaStream_t 
                               mul + P.lv[P.L - 1].off, P.mp);
 }
 
-// Parents per block so that the staged rings stay near kStageBudget.
-static int parents_per_block(size_t ring_bytes, int nparent) {
-  const int npb = (int)std::max<size_t>(1, kStageBudget / std::max<size_t>(1, ring_bytes));
-  return std::min(npb, std::max(1, nparent));
-}
-
-// Splits each block's outputs over several blocks when the level has too few
-// parents to fill the GPU (the top levels, and any level at small batches).
-static int output_chunks(int blocks, int nrhs, int npb, int ns_out) {
-  const int want = 2 * 148;
-  if (npb != 1 || blocks * nrhs >= want) return 1;
-  return std::max(1, std::min((ns_out + 127) / 128, (want + blocks * nrhs - 1) / (blocks * nrhs)));
+static TileArgs tile_args(const float2 *src, float2 *dst, size_t mp, size_t off_in, size_t off_out, int n_p,
+                          int ns_in, int ns_out, int nrhs, const TileBand &tb, const float2 *shT, int cap,
+                          const int *active) {
+  TileArgs A;
+  A.src = src;
+  A.dst = dst;
+  A.mp = mp;
+  A.off_in = off_in;
+  A.off_out = off_out;
+  A.n_p = n_p;
+  A.ns_in = ns_in;
+  A.ns_out = ns_out;
+  A.nparent = n_p * n_p;
+  A.ncols = A.nparent * nrhs;
+  A.cols = std::min(cap, std::max(32, (A.ncols + 31) / 32 * 32));
+  A.tb = tb;
+  A.shT = shT;
+  A.active = active;
+  return A;
 }
 
 void launch_m2m(const DevPlan &P, int lvl, float2 *mul, int nrhs, const int *active, cudaStream_t st) {
   const DevLevel &p = P.lv[lvl], &c = P.lv[lvl + 1];
-  const size_t ring = (size_t)4 * c.ns * sizeof(float2);
-  const int nparent = p.n * p.n;
+  const TileArgs A = tile_args(mul, mul, P.mp, c.off, p.off, p.n, c.ns, p.ns, nrhs, p.mt, p.shmT, 32, active);
+  const TileSmem L(p.mt.wmax, 4 * A.cols + 1, p.mt.out, 4 * A.cols, A.cols, (size_t)p.mt.out * (A.cols + 1));
+  const size_t smem = L.total * sizeof(float2);
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_m2m_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   count_launch();
-  if (ring <= (size_t)kSmemStage) {
-    const int npb = parents_per_block(ring, nparent), blocks = (nparent + npb - 1) / npb;
-    const int chunks = output_chunks(blocks, nrhs, npb, p.ns);
-    const size_t smem = ring * npb;
-    if (smem > 48 * 1024) cudaFuncSetAttribute(k_m2m<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    dim3 grid(blocks * chunks, nrhs);
-    k_m2m<true><<<grid, 256, smem, st>>>(mul, P.mp, p.off, c.off, p.n, p.ns, c.ns, npb, chunks, p.ifirst, p.iw,
-                                         p.shm, P.ninter, active);
-  } else {
-    const int chunks = output_chunks(nparent, nrhs, 1, p.ns);
-    dim3 grid(nparent * chunks, nrhs);
-    k_m2m<false><<<grid, 256, 0, st>>>(mul, P.mp, p.off, c.off, p.n, p.ns, c.ns, 1, chunks, p.ifirst, p.iw, p.shm,
-                                       P.ninter, active);
-  }
+  k_m2m_tile<<<dim3((A.ncols + A.cols - 1) / A.cols, p.mt.tiles), A.cols * (p.mt.out / kTileOut), smem, st>>>(A);
 }
 
-void launch_m2l(const DevPlan &P, int lvl, const float2 *mul, float2 *loc, int nrhs, const int *active,
+void launch_m2l(const DevPlan &P, int lvl, const float2 *mul, float2 *loc, int nrhs, const int *active, bool accumulate,
                 cudaStream_t st) {
   const DevLevel &c = P.lv[lvl];
   M2lArgs A;
@@ -520,40 +591,26 @@ void launch_m2l(const DevPlan &P, int lvl, const float2 *mul, float2 *loc, int n
   A.off = c.off;
   A.n = c.n;
   A.ns = c.ns;
-  A.tiles_x = (c.n + kM2lCols - 1) / kM2lCols;
-  A.tiles = A.tiles_x * ((c.n + kM2lRows - 1) / kM2lRows);
-  A.nitems = A.tiles * nrhs;
   A.T = c.T;
   A.active = active;
-  const int nkc = (c.ns + kM2lKC - 1) / kM2lKC;
-  // one resident block per SM: spread the items so every SM has a sample chunk
-  const int groups = std::max(1, std::min(A.nitems, (2 * 148 + nkc - 1) / nkc));
-  const size_t smem = 2 * (size_t)kM2lHalo * sizeof(float2);
-  cudaFuncSetAttribute(k_m2l, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  A.accumulate = accumulate ? 1 : 0;
+  const int half = c.n / 2, bx = (half * c.ns + 127) / 128;
+  // eight groups per thread when the grid stays large, fewer for small batches
+  int ty = std::min(8, half);
+  while (ty > 1 && (size_t)bx * ((half + ty - 1) / ty) * nrhs < 4 * 148) ty /= 2;
+  A.ty = ty;
   count_launch();
-  k_m2l<<<dim3(nkc, groups), 256, smem, st>>>(A);
+  k_m2l<<<dim3(bx, (half + ty - 1) / ty, nrhs), 128, 0, st>>>(A);
 }
 
-void launch_l2l(const DevPlan &P, int lvl, float2 *loc, int nrhs, const int *active, bool accumulate,
-                cudaStream_t st) {
+void launch_l2l(const DevPlan &P, int lvl, float2 *loc, int nrhs, const int *active, cudaStream_t st) {
   const DevLevel &c = P.lv[lvl], &p = P.lv[lvl - 1];
-  const size_t ring = (size_t)4 * p.ns * sizeof(float2);
-  const int nparent = p.n * p.n;
+  const TileArgs A = tile_args(loc, loc, P.mp, p.off, c.off, p.n, p.ns, c.ns, nrhs, c.at, p.shlT, 64, active);
+  const TileSmem L(c.at.wmax, A.cols + 1, c.at.out, A.cols, 4 * A.cols, (size_t)4 * c.at.out * (A.cols + 1));
+  const size_t smem = L.total * sizeof(float2);
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_l2l_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   count_launch();
-  if (ring <= (size_t)kSmemStage) {
-    const int npb = parents_per_block(ring, nparent), blocks = (nparent + npb - 1) / npb;
-    const int chunks = output_chunks(blocks, nrhs, npb, c.ns);
-    const size_t smem = ring * npb;
-    if (smem > 48 * 1024) cudaFuncSetAttribute(k_l2l<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    dim3 grid(blocks * chunks, nrhs);
-    k_l2l<true><<<grid, 256, smem, st>>>(loc, P.mp, p.off, c.off, p.n, p.ns, c.ns, npb, chunks, c.afirst, c.aw,
-                                         c.awidth, p.shl, accumulate ? 1 : 0, active);
-  } else {
-    const int chunks = output_chunks(nparent, nrhs, 1, c.ns);
-    dim3 grid(nparent * chunks, nrhs);
-    k_l2l<false><<<grid, 256, 0, st>>>(loc, P.mp, p.off, c.off, p.n, p.ns, c.ns, 1, chunks, c.afirst, c.aw,
-                                       c.awidth, p.shl, accumulate ? 1 : 0, active);
-  }
+  k_l2l_tile<<<dim3((A.ncols + A.cols - 1) / A.cols, c.at.tiles), A.cols * (c.at.out / kTileOut), smem, st>>>(A);
 }
 
 int near_blocks_per_rhs(const DevPlan &P) {

@@ -346,10 +346,12 @@ isg_status run_matvec(isg_ctx *c, const float2 *x, const float2 *g, int64_t gs, 
   for (int i = P.L - 2; i >= 2; i--)
     if (!(tc && band_m2m(c, i, c->mul, nrhs, active, st, &be))) launch_m2m(P, i, c->mul, nrhs, active, st);
   if (be != ISG_OK) return be;
-  for (int i = 2; i < P.L; i++) launch_m2l(P, i, c->mul, c->loc, nrhs, active, st);
-  for (int i = 3; i < P.L; i++)
-    if (!(tc && band_l2l(c, i, c->loc, nrhs, active, true, st, &be))) launch_l2l(P, i, c->loc, nrhs, active, true, st);
-  if (be != ISG_OK) return be;
+  // level by level: the parent's locals anterpolated over the level (L2L),
+  // then the level's own far-field translations added (M2L)
+  for (int i = 2; i < P.L; i++) {
+    if (i >= 3) launch_l2l(P, i, c->loc, nrhs, active, st);
+    launch_m2l(P, i, c->mul, c->loc, nrhs, active, i >= 3, st);
+  }
   NearArgs A;
   A.in = B;
   A.loc = c->loc;

@@ -1,8 +1,8 @@
-// M2M and L2L on the tensor cores as banded GEMMs over every ring of a level.
+// M2M on the tensor cores as a banded GEMM over every ring of a level.
 //
-// Interpolation (M2M, kernels.cu:83-136, solve.cpp:93-112) and anterpolation
-// (L2L, kernels.cu:137-238, solve.cpp:149-169) apply one real banded matrix
-// per level to complex rings: D[sample][ring] = sum_j W[sample][j] ring[j].
+// Interpolation (M2M, kernels.cu:83-136, solve.cpp:93-112) applies one real
+// banded matrix per level to complex rings: D[sample][ring] = sum_j W[sample][j]
+// ring[j].
 // Output samples are tiled by 128 (the MMA M); for each tile the weights are
 // restricted to the circular window of input samples its rows touch (a few
 // dozen more than 128 x the rate ratio), precomputed on the host as FP16 hi/lo
@@ -10,8 +10,9 @@
 // CTA's 256 MMA columns are 32 parents x 4 children x (re, im) of one level of
 // one or more RHS; ring values are split into FP16 hi/lo after a power-of-two
 // scale per CTA (3 products, FP32 accumulation in TMEM).  The child shift
-// phases are folded into the epilogue (M2M: sum over the four children) or into
-// the operand (L2L: shifted parent ring), exactly as in the reference.
+// phases are folded into the epilogue (sum over the four children), exactly as
+// in the reference.  (Anterpolation, whose windows are about twice as wide,
+// runs on the SIMT tiled kernel: measured faster there.)
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -33,15 +34,12 @@ constexpr int kBHalf = kCols * kKC * 2;  // 32 KB
 constexpr int kSmem = 2 * kAHalf + 2 * kBHalf + 128;
 constexpr int kErrBand = 121;
 
-enum BandMode { BAND_M2M = 0, BAND_L2L_ADD = 1, BAND_L2L_SET = 2 };
-
 struct BandArgs {
-  int mode;
-  const float2 *src;  // M2M: child-level multipoles; L2L: parent-level locals (level base)
-  float2 *dst;        // M2M: parent-level multipoles; L2L: child-level locals (level base)
+  const float2 *src;  // child-level multipoles (level base)
+  float2 *dst;        // parent-level multipoles (level base)
   size_t mp;
   int n_p, ns_in, ns_out;
-  const float2 *shift;  // M2M: shiftmul of the parent level; L2L: shiftloc of the parent level, [4][ns_p]
+  const float2 *shift;  // shiftmul of the parent level, [4][ns_p]
   const uint8_t *A;     // K-chunks of this transition (hi then lo, 32 KB each)
   const int *kw0, *nchunk, *chunk0;  // per M-tile: window start (-1: whole ring), chunks, first chunk
   float inv_a;
@@ -50,26 +48,20 @@ struct BandArgs {
   int *err;
 };
 
-// One ring of the CTA: its base pointer (and shift row for L2L), or none.
+// One ring of the CTA: its base pointer, or none.
 struct RingRef {
   const float2 *p;
-  const float2 *sh;
 };
 
 __device__ __forceinline__ RingRef ring_ref(const BandArgs &A, int ring) {
   const int pl = ring >> 2, q = ring & 3, gp = blockIdx.x * kParents + pl;
-  RingRef r{nullptr, nullptr};
+  RingRef r{nullptr};
   if (gp >= A.ncols) return r;
   const int rhs = gp / A.nparents, P = gp % A.nparents;
   if (A.active && !A.active[rhs]) return r;
   const float2 *base = A.src + (size_t)rhs * A.mp;
-  if (A.mode == BAND_M2M) {
-    const int py = P / A.n_p, px = P % A.n_p, nc = 2 * A.n_p;
-    r.p = base + (size_t)((2 * py + (q >> 1)) * nc + 2 * px + (q & 1)) * A.ns_in;
-  } else {
-    r.p = base + (size_t)P * A.ns_in;
-    r.sh = A.shift + q * A.ns_in;
-  }
+  const int py = P / A.n_p, px = P % A.n_p, nc = 2 * A.n_p;
+  r.p = base + (size_t)((2 * py + (q >> 1)) * nc + 2 * px + (q & 1)) * A.ns_in;
   return r;
 }
 
@@ -91,7 +83,7 @@ __device__ __forceinline__ void ring_load8(const BandArgs &A, const RingRef &r, 
       j -= A.ns_in;
     }
     float2 x = make_float2(0.f, 0.f);
-    if (ok) x = r.sh ? cmul(__ldg(&r.sh[j]), r.p[j]) : r.p[j];
+    if (ok) x = r.p[j];
     v[k] = x;
   }
 }
@@ -205,21 +197,11 @@ __global__ void __launch_bounds__(256, 2) k_tc_band(BandArgs A) {
       if (A.active && !A.active[rhs]) continue;
       float2 *base = A.dst + (size_t)rhs * A.mp;
       const float *dv = d + 8 * u;
-      if (A.mode == BAND_M2M) {
-        float2 acc = make_float2(0.f, 0.f);
+      float2 acc = make_float2(0.f, 0.f);
 #pragma unroll
-        for (int q = 0; q < 4; q++)
-          cfma(acc, __ldg(&A.shift[q * A.ns_out + km]), make_float2(dv[2 * q] * inv, dv[2 * q + 1] * inv));
-        base[(size_t)P * A.ns_out + km] = acc;
-      } else {
-        const int py = P / A.n_p, px = P % A.n_p, nc = 2 * A.n_p;
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-          float2 *o = base + (size_t)((2 * py + (q >> 1)) * nc + 2 * px + (q & 1)) * A.ns_out + km;
-          const float2 v = make_float2(dv[2 * q] * inv, dv[2 * q + 1] * inv);
-          *o = A.mode == BAND_L2L_ADD ? cadd(*o, v) : v;
-        }
-      }
+      for (int q = 0; q < 4; q++)
+        cfma(acc, __ldg(&A.shift[q * A.ns_out + km]), make_float2(dv[2 * q] * inv, dv[2 * q + 1] * inv));
+      base[(size_t)P * A.ns_out + km] = acc;
     }
   }
   tc_fence_before();
@@ -256,7 +238,6 @@ void pack_chunk(std::vector<uint8_t> &buf, size_t at, int k0, double scale, F re
 
 struct BandPlan {
   Transition m2m[kMaxLevels];  // indexed by parent level
-  Transition l2l[kMaxLevels];  // indexed by child level
   std::vector<void *> allocs;
 };
 
@@ -334,11 +315,10 @@ static isg_status build_transition(isg_ctx *c, Transition &T, int ns_out, int ns
 }
 
 isg_status band_setup(isg_ctx *c) {
-  const bool build_l2l = false;
   c->band = new BandPlan();
   if (!tc_available(c)) return ISG_OK;
   const HostTables &H = c->T;
-  const int L = H.L, ni = H.ninter, W = 2 * ni;
+  const int L = H.L, ni = H.ninter;
   isg_status e;
   for (int i = 2; i <= L - 2; i++) {  // M2M into parent level i
     const int nsp = H.nsamp[i], nsc = H.nsamp[i + 1];
@@ -348,19 +328,6 @@ isg_status band_setup(isg_ctx *c) {
         rows[k].push_back({H.intind[i][(size_t)k * ni + t], H.interp[i][(size_t)k * ni + t]});
     if ((e = build_transition(c, c->band->m2m[i], nsp, nsc, rows)) != ISG_OK) return e;
   }
-  // L2L stays on the SIMT kernel: its windows are ~2x wider than M2M's (the
-  // parent rate is higher) and the per-CTA operand conversion outweighs the
-  // MMAs (measured slower than k_l2l on the 1024^2 workload).
-  for (int i = 3; i <= L - 1 && build_l2l; i++) {  // L2L into child level i
-    const int nsc = H.nsamp[i], nsp = H.nsamp[i - 1];
-    std::vector<std::vector<std::pair<int, double>>> rows(nsc);
-    for (int k = 0; k < nsc; k++)
-      for (int t = 0; t < W; t++) {
-        const double w = H.anterp[i][(size_t)k * W + t];
-        if (w != 0.0) rows[k].push_back({H.antind[i][(size_t)k * W + t], w});
-      }
-    if ((e = build_transition(c, c->band->l2l[i], nsc, nsp, rows)) != ISG_OK) return e;
-  }
   return cuda_check(c, cudaFuncSetAttribute(k_tc_band, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem),
                     "band attr");
 }
@@ -368,21 +335,21 @@ isg_status band_setup(isg_ctx *c) {
 void band_destroy(isg_ctx *c) {
   if (!c->band) return;
   for (int i = 0; i < kMaxLevels; i++)
-    for (Transition *T : {&c->band->m2m[i], &c->band->l2l[i]}) {
-      cudaFree(T->A);
-      cudaFree(T->kw0);
-      cudaFree(T->nchunk);
-      cudaFree(T->chunk0);
-    }
+  {
+    Transition *T = &c->band->m2m[i];
+    cudaFree(T->A);
+    cudaFree(T->kw0);
+    cudaFree(T->nchunk);
+    cudaFree(T->chunk0);
+  }
   delete c->band;
   c->band = nullptr;
 }
 
-static isg_status band_launch(isg_ctx *c, const Transition &T, int mode, const float2 *src, float2 *dst, int n_p,
+static isg_status band_launch(isg_ctx *c, const Transition &T, const float2 *src, float2 *dst, int n_p,
                               int ns_in, int ns_out, const float2 *shift, int nrhs, const int *active,
                               cudaStream_t st) {
   BandArgs A;
-  A.mode = mode;
   A.src = src;
   A.dst = dst;
   A.mp = c->P.mp;
@@ -407,18 +374,10 @@ static isg_status band_launch(isg_ctx *c, const Transition &T, int mode, const f
 bool band_m2m(isg_ctx *c, int lvl, float2 *mul, int nrhs, const int *active, cudaStream_t st, isg_status *e) {
   if (!c->band || lvl >= kMaxLevels || !c->band->m2m[lvl].ok) return false;
   const DevLevel &p = c->P.lv[lvl], &ch = c->P.lv[lvl + 1];
-  *e = band_launch(c, c->band->m2m[lvl], BAND_M2M, mul + ch.off, mul + p.off, p.n, ch.ns, p.ns, p.shm, nrhs, active,
+  *e = band_launch(c, c->band->m2m[lvl], mul + ch.off, mul + p.off, p.n, ch.ns, p.ns, p.shm, nrhs, active,
                    st);
   return true;
 }
 
-bool band_l2l(isg_ctx *c, int lvl, float2 *loc, int nrhs, const int *active, bool accumulate, cudaStream_t st,
-              isg_status *e) {
-  if (!c->band || lvl >= kMaxLevels || !c->band->l2l[lvl].ok) return false;
-  const DevLevel &ch = c->P.lv[lvl], &p = c->P.lv[lvl - 1];
-  *e = band_launch(c, c->band->l2l[lvl], accumulate ? BAND_L2L_ADD : BAND_L2L_SET, loc + p.off, loc + ch.off, p.n,
-                   p.ns, ch.ns, p.shl, nrhs, active, st);
-  return true;
-}
 
 }  // namespace isg
