@@ -67,13 +67,14 @@ typedef struct isg_opts {
 /* Engines for the dense leaf stages (near field, P2M, L2P). */
 typedef enum isg_engine {
   ISG_ENGINE_SIMT = 0,  /* complex FP32 CUDA cores: the plain solver */
-  ISG_ENGINE_TENSOR = 1 /* 3xTF32 split products on the tcgen05 tensor cores, FP32 accumulate */
+  ISG_ENGINE_TENSOR = 1 /* 3xFP16 split products (hi*hi + hi*lo + lo*hi) on the tcgen05 tensor cores, FP32 accumulate */
 } isg_engine;
 
 typedef enum isg_guess {
   ISG_GUESS_ZERO = 0,   /* x0 = 0, as every reference call site (mom.cpp:254,286,324) */
   ISG_GUESS_CALLER = 1, /* x0 = the caller's x on entry (bicgs.cpp:115) */
-  ISG_GUESS_LEARNED = 2 /* x0 from the loaded neural-operator warm start */
+  ISG_GUESS_LEARNED = 2 /* x0 from the context's neural-operator warm start (isg_fno_create); forward
+                           solves only, adjoint solves start from zero */
 } isg_guess;
 
 typedef struct isg_solve_opts {
@@ -233,6 +234,43 @@ isg_status isg_make_plane_waves(const isg_ctx *ctx, int ntx, int first, int coun
  * radius (the reference's near-field form, setup_born.cpp:66-72); rows as above. */
 isg_status isg_make_line_sources(const isg_ctx *ctx, int ntx, int first, int count, double radius, int order,
                                  double *inc);
+
+/* ---- learned warm start (no counterpart in the reference) ----
+ * A Fourier neural operator on the pixel grid maps the contrast g and the
+ * incident field b of a forward solve to an estimate of its total field; with
+ * ISG_GUESS_LEARNED, isg_bicgs starts from it and still iterates to tol.
+ * Architecture: per-pixel lift of (chi, b, chi b) (chi = g / k0^2) to `width`
+ * channels, `layers` spectral layers (GELU(W v + b + Re iDFT(R(k) DFT v)) over
+ * the lowest `modes` x 2 `modes` frequencies; no GELU after the last), and a
+ * per-pixel projection to a correction added to b.  FP32 parameters, trained
+ * by the library's own forward/backward kernels and Adam. */
+typedef struct isg_fno_opts {
+  int width;     /* channels (default 32) */
+  int modes;     /* retained kx modes; ky keeps 2 x modes (default 12) */
+  int layers;    /* spectral layers (default 4) */
+  int batch;     /* samples per device pass; sizes the activation buffers (default 4) */
+  uint64_t seed; /* parameter initialisation */
+} isg_fno_opts;
+void isg_default_fno_opts(isg_fno_opts *o);
+/* Attach a freshly initialised network to the context (replaces any). */
+isg_status isg_fno_create(isg_ctx *ctx, const isg_fno_opts *o);
+int64_t isg_fno_param_count(const isg_ctx *ctx);
+/* Copy the flat FP32 parameter vector (which 0) or the last gradient (which 1)
+ * to host[n]; with set = 1, load parameters from host (which must be 0). */
+isg_status isg_fno_params(isg_ctx *ctx, float *host, int64_t n, int which, int set);
+/* x = b + N(g, b) for nrhs RHS (device complex64, caller order); g_stride 0 or numunk. */
+isg_status isg_fno_apply(isg_ctx *ctx, const void *g, int64_t g_stride, const void *b, void *x, int nrhs, int order,
+                         isg_stream stream);
+/* Gradient of a loss over nrhs samples; *loss receives the loss.  With u (the
+ * solver's total fields): mean_s ||x0_s - u_s||^2 / ||u_s||^2, x0 = b + N(g, b).
+ * With u NULL: the initial residual of the forward solves it would seed,
+ * mean_s ||b_s - A_s x0_s||^2 / ||b_s||^2 with A = I - G diag(g) (one forward
+ * and one adjoint matvec per sample; needs no solved fields). */
+isg_status isg_fno_grad(isg_ctx *ctx, const void *g, int64_t g_stride, const void *b, const void *u, int nrhs,
+                        int order, double *loss, isg_stream stream);
+/* isg_fno_grad followed by one Adam step (beta 0.9, 0.999) with learning rate lr. */
+isg_status isg_fno_train_step(isg_ctx *ctx, const void *g, int64_t g_stride, const void *b, const void *u, int nrhs,
+                              int order, float lr, double *loss, isg_stream stream);
 
 #ifdef __cplusplus
 }

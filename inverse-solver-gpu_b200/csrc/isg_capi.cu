@@ -362,6 +362,7 @@ void isg_destroy(isg_ctx *c) {
   if (c->gpu_ready || !c->dev_allocs.empty()) {
     cudaSetDevice(c->opts.device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    fno_destroy(c);
     band_destroy(c);
     tc_destroy(c);
     for (void *p : c->dev_allocs) cudaFree(p);
@@ -471,11 +472,20 @@ isg_status isg_bicgs(isg_ctx *c, void *x, const void *g, int64_t g_stride, const
     c->err = "bad solve options";
     return ISG_BAD_ARG;
   }
-  if (o.guess == ISG_GUESS_LEARNED) {
-    c->err = "no warm-start model is loaded";
-    return ISG_UNSUPPORTED;
-  }
   cudaStream_t st = pick(c, stream);
+  if (o.guess == ISG_GUESS_LEARNED) {
+    if (hermitian) {
+      o.guess = ISG_GUESS_ZERO;  // the network is trained on forward solves
+    } else {
+      if (!c->fno || (g_stride != 0 && g_stride != c->P.U)) {
+        c->err = "ISG_GUESS_LEARNED needs a warm-start network (isg_fno_create) and g_stride 0 or numunk";
+        return ISG_UNSUPPORTED;
+      }
+      if ((e = fno_apply(c, (const float2 *)g, g_stride, (const float2 *)b, (float2 *)x, nrhs, order, st)) != ISG_OK)
+        return e;
+      o.guess = ISG_GUESS_CALLER;
+    }
+  }
   const float2 *gb = nullptr;
   if ((e = contrast(c, g, g_stride, nrhs, order, st, &gb)) != ISG_OK) return e;
   const int64_t gs = (g_stride && order != ISG_ORDER_BLOCKED) ? c->P.U : g_stride;

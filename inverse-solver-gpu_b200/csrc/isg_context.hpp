@@ -23,6 +23,7 @@ struct RhsState {
 };
 
 struct TcPlan;    // tensor-core leaf stage tables (isg_tc.cu)
+struct FnoModel;  // learned warm start (isg_fno.cu)
 struct BandPlan;  // tensor-core M2M tables (isg_tc_band.cu)
 
 }  // namespace isg
@@ -50,6 +51,7 @@ struct isg_ctx {
   int vec_blocks = 0;
   isg::TcPlan *tc = nullptr;
   isg::BandPlan *band = nullptr;
+  isg::FnoModel *fno = nullptr;
   int *tc_err_flag() const;
 };
 
@@ -80,4 +82,14 @@ int tc_error(isg_ctx *c);
 isg_status band_setup(isg_ctx *c);
 void band_destroy(isg_ctx *c);
 bool band_m2m(isg_ctx *c, int lvl, float2 *mul, int nrhs, const int *active, cudaStream_t st, isg_status *e);
+// Learned warm start (isg_fno.cu).
+isg_status fno_create(isg_ctx *c, const isg_fno_opts *o);
+void fno_destroy(isg_ctx *c);
+isg_status fno_apply(isg_ctx *c, const float2 *g, int64_t gs, const float2 *b, float2 *x, int nrhs, int order,
+                     cudaStream_t st);
+isg_status fno_gradient(isg_ctx *c, const float2 *g, int64_t gs, const float2 *b, const float2 *u, int nrhs, int order,
+                        double *loss, cudaStream_t st);
+isg_status fno_adam(isg_ctx *c, float lr, cudaStream_t st);
+size_t fno_param_count(const isg_ctx *c);
+float *fno_param_ptr(isg_ctx *c, int which);
 }  // namespace isg

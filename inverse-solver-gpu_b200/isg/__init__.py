@@ -75,6 +75,11 @@ class Phantom(ctypes.Structure):
                 ("tand_max", ctypes.c_double), ("corr_len", ctypes.c_double), ("seed", ctypes.c_uint64)]
 
 
+class FnoOpts(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_int), ("modes", ctypes.c_int), ("layers", ctypes.c_int), ("batch", ctypes.c_int),
+                ("seed", ctypes.c_uint64)]
+
+
 _lib = None
 
 # Every entry point declared in include/isg.h, with its ctypes signature.
@@ -107,6 +112,13 @@ SIGNATURES = {
     "isg_make_phantom": (_I, [_P, ctypes.POINTER(Phantom), _P]),
     "isg_make_plane_waves": (_I, [_P, _I, _I, _I, _I, _P]),
     "isg_make_line_sources": (_I, [_P, _I, _I, _I, _D, _I, _P]),
+    "isg_default_fno_opts": (None, [ctypes.POINTER(FnoOpts)]),
+    "isg_fno_create": (_I, [_P, ctypes.POINTER(FnoOpts)]),
+    "isg_fno_param_count": (_L, [_P]),
+    "isg_fno_params": (_I, [_P, _P, _L, _I, _I]),
+    "isg_fno_apply": (_I, [_P, _P, _L, _P, _P, _I, _I, _P]),
+    "isg_fno_grad": (_I, [_P, _P, _L, _P, _P, _I, _I, ctypes.POINTER(_D), _P]),
+    "isg_fno_train_step": (_I, [_P, _P, _L, _P, _P, _I, _I, ctypes.c_float, ctypes.POINTER(_D), _P]),
 }
 
 
@@ -279,6 +291,49 @@ class Solver:
                             device=rx.device)
         self._check(lib().isg_aggregateh(self._h, _ptr(x), _ptr(rx), R, order, _stream(stream)), "aggregateh")
         return x
+
+    # ---- learned warm start ----
+    def fno_create(self, width: int = 32, modes: int = 12, layers: int = 4, batch: int = 4, seed: int = 1):
+        """Attach a freshly initialised neural-operator warm start (ISG_GUESS_LEARNED)."""
+        o = FnoOpts()
+        lib().isg_default_fno_opts(ctypes.byref(o))
+        o.width, o.modes, o.layers, o.batch, o.seed = width, modes, layers, batch, seed
+        self._check(lib().isg_fno_create(self._h, ctypes.byref(o)), "fno_create")
+
+    def fno_params(self, which: int = 0) -> np.ndarray:
+        """Flat FP32 parameters (which 0) or the last gradient (which 1)."""
+        n = lib().isg_fno_param_count(self._h)
+        out = np.empty(n, dtype=np.float32)
+        self._check(lib().isg_fno_params(self._h, out.ctypes.data, n, which, 0), "fno_params")
+        return out
+
+    def fno_set_params(self, p: np.ndarray):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        self._check(lib().isg_fno_params(self._h, p.ctypes.data, p.size, 0, 1), "fno_set_params")
+
+    def fno_apply(self, g, b, order: int = ORDER_TREE, stream=None):
+        """x = b + N(g, b): the warm start for the forward solves of b."""
+        import torch
+        x = torch.empty_like(b)
+        gs = 0 if g.dim() == 1 else self.numunk
+        self._check(lib().isg_fno_apply(self._h, _ptr(g), gs, _ptr(b), _ptr(x), self._nrhs(b), order,
+                                        _stream(stream)), "fno_apply")
+        return x
+
+    def fno_grad(self, g, b, u=None, order: int = ORDER_TREE, stream=None) -> float:
+        """Loss and gradient (fno_params(1)): field error against u, or the initial residual when u is None."""
+        loss = ctypes.c_double()
+        gs = 0 if g.dim() == 1 else self.numunk
+        self._check(lib().isg_fno_grad(self._h, _ptr(g), gs, _ptr(b), _ptr(u), self._nrhs(b), order,
+                                       ctypes.byref(loss), _stream(stream)), "fno_grad")
+        return loss.value
+
+    def fno_train_step(self, g, b, u=None, lr: float = 1e-3, order: int = ORDER_TREE, stream=None) -> float:
+        loss = ctypes.c_double()
+        gs = 0 if g.dim() == 1 else self.numunk
+        self._check(lib().isg_fno_train_step(self._h, _ptr(g), gs, _ptr(b), _ptr(u), self._nrhs(b), order, lr,
+                                             ctypes.byref(loss), _stream(stream)), "fno_train_step")
+        return loss.value
 
     def time_stages(self, nrhs: int = 1, engine: int = ENGINE_SIMT, reps: int = 5) -> dict:
         """Mean device ms per matvec stage (P2M, M2M, M2L+L2L, L2P+near, total)."""
