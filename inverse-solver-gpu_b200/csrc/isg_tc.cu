@@ -36,7 +36,7 @@ constexpr int kSboA = 16 * kLboA;                // 2560 (one halo row: 16 K-chu
 constexpr int kRegion = kHR * kSboA;             // 46080 bytes per FP16 split
 constexpr int kStageBytes = 16384;               // hi [128 x 32] + lo [128 x 32]
 constexpr int kStageHalf = 8192;
-constexpr int kNB = 4;                           // ring depth
+constexpr int kNB = 6;                           // ring depth
 constexpr int kNearStages = 36;                  // 9 slots x 4 K-chunks of 32 reals
 constexpr int kLocChunksMax = 20;                // K chunks (8 reals each) of the L2P operand
 constexpr int kSboL = kLocChunksMax * 128;       // 2560
@@ -140,6 +140,51 @@ __global__ void __launch_bounds__(256, 1) k_tc_near(TcNearArgs A) {
   tc_fence_after();
   const uint32_t tmem = *tslot;
 
+  // ---- halo of the input: every thread stages raw FP32 copies with cp.async,
+  // x where its FP16 hi/lo halves will go (first two pixels of a 4-pixel chunk
+  // in the hi slot, last two in the lo slot) and, for g x, the contrast in the
+  // weight ring (not streaming yet); the loaders then form g x and its max in
+  // place, and convert to hi/lo once the tile's scale is known ----
+  constexpr int kItems = kHR * kHC * 16;  // (halo leaf, 4-pixel chunk)
+  const bool with_g = A.mode == IN_G;
+  for (int it = threadIdx.x; it < kItems; it += blockDim.x) {
+    const int h = it >> 4, c = it & 15;
+    const int ly = ty0 - 1 + h / kHC, lx = tx0 - 1 + h % kHC;
+    const bool in = ly >= 0 && ly < A.nleaf && lx >= 0 && lx < A.nleaf;
+    const size_t i = in ? (size_t)(ly * A.nleaf + lx) * kBB + 4 * c : 0;
+    const int off = (h / kHC) * kSboA + c * kLboA + (h % kHC) * 16;
+    cp_async16z(sm + NearSmem::hi + off, A.x + rbase + i, in);
+    cp_async16z(sm + NearSmem::lo + off, A.x + rbase + i + 2, in);
+    if (with_g) {
+      cp_async16z(sm + NearSmem::stages + it * 32, gr + i, in);
+      cp_async16z(sm + NearSmem::stages + it * 32 + 16, gr + i + 2, in);
+    }
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  float mx = 0.f;
+  if (warp != 1) {
+    for (int it = loader_id(); it < kItems; it += kLoaders) {
+      const int h = it >> 4, c = it & 15;
+      const int off = (h / kHC) * kSboA + c * kLboA + (h % kHC) * 16;
+      float4 *ph = (float4 *)(sm + NearSmem::hi + off), *pl = (float4 *)(sm + NearSmem::lo + off);
+      const float4 a0 = *ph, a1 = *pl;
+      float4 g0 = make_float4(0.f, 0.f, 0.f, 0.f), g1 = g0;
+      if (with_g) {
+        g0 = *(const float4 *)(sm + NearSmem::stages + it * 32);
+        g1 = *(const float4 *)(sm + NearSmem::stages + it * 32 + 16);
+      }
+      const float2 v0 = transform(make_float2(a0.x, a0.y), make_float2(g0.x, g0.y), A.mode);
+      const float2 v1 = transform(make_float2(a0.z, a0.w), make_float2(g0.z, g0.w), A.mode);
+      const float2 v2 = transform(make_float2(a1.x, a1.y), make_float2(g1.x, g1.y), A.mode);
+      const float2 v3 = transform(make_float2(a1.z, a1.w), make_float2(g1.z, g1.w), A.mode);
+      mx = fmaxf(mx, fmaxf(fmaxf(cabs1(v0), cabs1(v1)), fmaxf(cabs1(v2), cabs1(v3))));
+      *ph = make_float4(v0.x, v0.y, v1.x, v1.y);
+      *pl = make_float4(v2.x, v2.y, v3.x, v3.y);
+    }
+  }
+  __syncthreads();  // the ring is free for the weights
+
   if (warp == 1) {
     // ---- producer: weight stages through the ring ----
     if (lane == 0) {
@@ -151,45 +196,15 @@ __global__ void __launch_bounds__(256, 1) k_tc_near(TcNearArgs A) {
       }
     }
   } else {
-    // ---- loaders: halo of the transformed input, FP16 hi/lo ----
     const int li = loader_id();
-    constexpr int kItems = kHR * kHC * 16;  // (halo leaf, 4-pixel chunk)
-    constexpr int kPer = (kItems + kLoaders - 1) / kLoaders;
-    float2 v[kPer][4];
-    float mx = 0.f;
-#pragma unroll
-    for (int r = 0; r < kPer; r++) {
-      const int it = li + r * kLoaders;
-#pragma unroll
-      for (int p = 0; p < 4; p++) v[r][p] = make_float2(0.f, 0.f);
-      if (it < kItems) {
-        const int h = it >> 4, c = it & 15;
-        const int ly = ty0 - 1 + h / kHC, lx = tx0 - 1 + h % kHC;
-        if (ly >= 0 && ly < A.nleaf && lx >= 0 && lx < A.nleaf) {
-          const size_t i = (size_t)(ly * A.nleaf + lx) * kBB + 4 * c;
-          const float4 a0 = *(const float4 *)(A.x + rbase + i), a1 = *(const float4 *)(A.x + rbase + i + 2);
-          float4 g0 = make_float4(0.f, 0.f, 0.f, 0.f), g1 = g0;
-          if (A.mode == IN_G) {
-            g0 = *(const float4 *)(gr + i);
-            g1 = *(const float4 *)(gr + i + 2);
-          }
-          v[r][0] = transform(make_float2(a0.x, a0.y), make_float2(g0.x, g0.y), A.mode);
-          v[r][1] = transform(make_float2(a0.z, a0.w), make_float2(g0.z, g0.w), A.mode);
-          v[r][2] = transform(make_float2(a1.x, a1.y), make_float2(g1.x, g1.y), A.mode);
-          v[r][3] = transform(make_float2(a1.z, a1.w), make_float2(g1.z, g1.w), A.mode);
-#pragma unroll
-          for (int p = 0; p < 4; p++) mx = fmaxf(mx, cabs1(v[r][p]));
-        }
-      }
-    }
     const float s1 = pow2_scale(loaders_max(mx, fscr));
-#pragma unroll
-    for (int r = 0; r < kPer; r++) {
-      const int it = li + r * kLoaders;
-      if (it < kItems) {
-        const int h = it >> 4, c = it & 15;
-        store_chunk(sm, (h / kHC) * kSboA + c * kLboA + (h % kHC) * 16, v[r], s1);
-      }
+    for (int it = li; it < kItems; it += kLoaders) {
+      const int h = it >> 4, c = it & 15;
+      const int off = (h / kHC) * kSboA + c * kLboA + (h % kHC) * 16;
+      const float4 q0 = *(const float4 *)(sm + NearSmem::hi + off), q1 = *(const float4 *)(sm + NearSmem::lo + off);
+      const float2 v[4] = {make_float2(q0.x, q0.y), make_float2(q0.z, q0.w), make_float2(q1.x, q1.y),
+                           make_float2(q1.z, q1.w)};
+      store_chunk(sm, off, v, s1);
     }
     if (li == 0) scales[0] = s1;
     fence_proxy_async();
@@ -288,16 +303,27 @@ __global__ void __launch_bounds__(256, 1) k_tc_near(TcNearArgs A) {
   }
 
   // ---- epilogue (all warps) ----
+  const int q = warp & 3, hh = warp >> 2;
+  const int m = 32 * q + lane;
+  const int ly = ty0 + m / kTX, lx = tx0 + m % kTX;
+  const bool in_grid = ly < A.nleaf && lx < A.nleaf;
+  const size_t leafbase = rbase + (size_t)(ly * A.nleaf + lx) * kBB;
+  // this thread's 32 input pixels, fetched while the last MMAs run
+  const bool need_x = in_grid && (A.epi == EPI_FWD || A.epi == EPI_ADJ || A.red == RED_TS);
+  float4 xpre[4][4];
+#pragma unroll
+  for (int ch = 0; ch < 4; ch++)
+#pragma unroll
+    for (int pp = 0; pp < 4; pp++)
+      xpre[ch][pp] = need_x ? *(const float4 *)(A.x + leafbase + 32 * hh + 8 * ch + 2 * pp)
+                            : make_float4(0.f, 0.f, 0.f, 0.f);
   const bool ok = mbar_wait(done, 1, A.err, kErrNearDone);
   __syncthreads();
   tc_fence_after();
   const float inv1 = A.inv_w / scales[0], inv2 = A.inv_b / scales[1];
-  const int q = warp & 3, hh = warp >> 2;
-  const int m = 32 * q + lane;
-  const int ly = ty0 + m / kTX, lx = tx0 + m % kTX;
-  const bool valid = ok && ly < A.nleaf && lx < A.nleaf;
-  const size_t leafbase = rbase + (size_t)(ly * A.nleaf + lx) * kBB;
+  const bool valid = ok && in_grid;
   double r0 = 0, r1 = 0, r2 = 0;
+#pragma unroll
   for (int ch = 0; ch < 4; ch++) {
     const int col = 64 * hh + 16 * ch;
     float d1[16], d2[16];
@@ -313,12 +339,8 @@ __global__ void __launch_bounds__(256, 1) k_tc_near(TcNearArgs A) {
         o[e] = make_float2(d1[2 * (p + e)] * inv1 + d2[2 * (p + e)] * inv2,
                            d1[2 * (p + e) + 1] * inv1 + d2[2 * (p + e) + 1] * inv2);
       const size_t i = leafbase + t0;
-      float2 xin[2] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
-      if (A.epi == EPI_FWD || A.epi == EPI_ADJ || A.red == RED_TS) {
-        const float4 xv = *(const float4 *)(A.x + i);
-        xin[0] = make_float2(xv.x, xv.y);
-        xin[1] = make_float2(xv.z, xv.w);
-      }
+      const float4 xv = xpre[ch][p / 2];
+      const float2 xin[2] = {make_float2(xv.x, xv.y), make_float2(xv.z, xv.w)};
       if (A.epi == EPI_FWD) {
         o[0] = csub(xin[0], o[0]);
         o[1] = csub(xin[1], o[1]);
