@@ -112,14 +112,35 @@ def peaks() -> dict:
     if os.path.exists(p):
         with open(p) as f:
             d = json.load(f)
-        return {"hbm_gbs": d["hbm_gbs"], "src": "measured"}
-    return {"hbm_gbs": 6650.0, "src": "fallback"}
+        return {"hbm_gbs": d["hbm_gbs"], "bf16_tflops": d["bf16_tflops"], "src": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "src": "fallback"}
 
 
 def algorithmic_bytes_per_matvec(s) -> float:
     """8 (3U + 4S), S = sum over levels >= 2 of clusters x samples."""
     S = sum((4 ** i) * s.numsamp(i) for i in range(2, s.level))
     return 8.0 * (3 * s.numunk + 4 * S)
+
+
+def near_field_flops_per_rhs(s) -> tuple[float, float]:
+    """(tensor FLOPs executed, useful complex FLOPs) of the near-field + L2P
+    kernel for one RHS.  Executed: per 16 x 8-leaf tile, 9 neighbour slots x 4
+    K-chunks x 2 K-steps x 3 split products (hi hi, hi lo, lo hi) of
+    128 x 128 x 16 MMAs, plus the L2P chunks (2 ns reals padded to 32) the same
+    way.  Useful: (9 x 64 + ns) complex MACs x 8 flops per pixel."""
+    tiles = -(-s.side // 8 // 16) * -(-s.side // 8 // 8)
+    ns = s.numsamp(s.level - 1)
+    mma = 2 * 128 * 128 * 16
+    stages = 36 + -(-2 * ns // 32)
+    executed = tiles * stages * 6 * mma
+    useful = s.numunk * (9 * 64 + ns) * 8
+    return float(executed), float(useful)
+
+
+# DRAM bytes (read + write) of one near-field launch over 16 RHS of the 1024^2
+# workload, from `ncu --set full -k regex:k_tc_near` on that launch
+# (profiles/k_tc_near_1024_16rhs.md).
+NEAR_TRAFFIC_16RHS = 293.4e6 + 109.0e6
 
 
 def cpu_reference_sample(g, b, budget_s: float, max_solves: int):
@@ -283,11 +304,16 @@ def main():
             p_iters.append(inf["iterations"])
     plain_value = 1000.0 / (sum(p_ms) / len(p_ms))
 
-    # Roofline of the matvec (whole stage sequence) on a 16-RHS batch.
+    # Roofline: the dominant kernel (near field + L2P on the tensor cores) and,
+    # beside it, the whole matvec against HBM; both on a 16-RHS batch, each
+    # stage timed alone with CUDA events on the launching stream.
     st = s.time_stages(nrhs=16, engine=engine, reps=5)
     pk = peaks()
     bytes_mv = algorithmic_bytes_per_matvec(s) * 16
     achieved = bytes_mv / (st["total"] * 1e-3) / 1e9
+    exe, useful = near_field_flops_per_rhs(s)
+    near_tflops = 16 * exe / (st["near"] * 1e-3) / 1e12
+    tc = engine == isg.ENGINE_TENSOR
 
     out = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
@@ -297,10 +323,19 @@ def main():
                    "parallelism": f"tx-sharded x{world}" if world > 1 else "single GPU"},
         "mean_iterations": float(np.mean(iters)), "all_converged": not bad,
         "max_true_residual": max(i["true_residual"] for i in infos),
-        "roofline": {"bound": "hbm", "kernel": "MLFMA matvec (P2M, M2M, M2L+L2L, L2P+near), 16 RHS",
-                     "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved / pk["hbm_gbs"],
-                     "peak_src": pk["src"], "traffic": None, "stage_ms": st,
-                     "algorithmic_bytes_per_rhs": algorithmic_bytes_per_matvec(s)},
+        "roofline": ({"bound": "tensor", "kernel": "k_tc_near (near field + L2P, 3xFP16 split tcgen05), 16 RHS",
+                      "achieved": near_tflops, "peak": pk["bf16_tflops"], "unit": "TFLOP/s",
+                      "frac": near_tflops / pk["bf16_tflops"], "peak_src": pk["src"] + " (bf16 burst)",
+                      "traffic": NEAR_TRAFFIC_16RHS, "launch_ms": st["near"],
+                      "useful_complex_tflops": 16 * useful / (st["near"] * 1e-3) / 1e12,
+                      "executed_flops_per_rhs": exe} if tc else
+                     {"bound": "hbm", "kernel": "MLFMA matvec (SIMT engine), 16 RHS", "achieved": achieved,
+                      "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved / pk["hbm_gbs"], "peak_src": pk["src"],
+                      "traffic": None}),
+        "roofline_matvec": {"bound": "hbm", "kernel": "MLFMA matvec (P2M, M2M, M2L+L2L, L2P+near), 16 RHS",
+                            "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                            "frac": achieved / pk["hbm_gbs"], "peak_src": pk["src"], "stage_ms": st,
+                            "algorithmic_bytes_per_rhs": algorithmic_bytes_per_matvec(s)},
         "plain": {"value": plain_value, "unit": "solves/s", "solves": len(p_ms),
                   "mean_iterations": float(np.mean(p_iters)), "ms_per_solve": float(np.mean(p_ms))},
         "e2e": {"value": world * NTX * 1000.0 / e2e_ms, "unit": "solves/s",

@@ -173,7 +173,11 @@ typedef struct isg_dbim_opts {
   double regular;        /* Tikhonov weight; adds regular^2 chi per transmitter (mom.cpp:32,268-269) */
   int start_from_chi;    /* 0: chi = 0 and total field = incident (mom.cpp:225-229);
                             1: start from the caller's chi (the reference's commented restart, mom.cpp:230-245) */
-  isg_solve_opts solve;  /* inner BiCGSTAB options (tol: mom.cpp:21) */
+  isg_solve_opts solve;  /* inner BiCGSTAB options (tol: mom.cpp:21); ISG_GUESS_LEARNED seeds the
+                            forward solves of the total fields from the context's network */
+  int warm_start;        /* 0: every solve starts from zero, as the reference; 1: each transmitter's
+                            total-field and adjoint solves start from its fields of the previous
+                            iteration (same tolerance; not in the reference) */
 } isg_dbim_opts;
 
 typedef struct isg_dbim_record {

@@ -157,6 +157,8 @@ struct Dbim {
   std::vector<void *> allocs;
   float2 *incb = nullptr, *tot = nullptr, *X = nullptr, *Y = nullptr, *C = nullptr, *g = nullptr;
   float2 *rxd = nullptr;  // ntx x nrx receiver-side scratch
+  float2 *adj = nullptr;  // ntx x U previous adjoint fields (warm start only)
+  bool warm = false;
   double2 *o = nullptr, *od = nullptr, *ot = nullptr, *save = nullptr, *otrue = nullptr;
   double *part = nullptr;
   std::vector<zd> mes, mesd, rhs;
@@ -180,9 +182,17 @@ struct Dbim {
   int chunk(int k) const { return std::min(R, ntx - k * R); }
   int nchunks() const { return (ntx + R - 1) / R; }
 
-  isg_status solve(float2 *x, const float2 *b, int n, int hermitian) {
+  // guess: ISG_GUESS_ZERO, or ISG_GUESS_CALLER with x holding the start
+  isg_status solve(float2 *x, const float2 *b, int n, int hermitian, int guess = ISG_GUESS_ZERO) {
     std::vector<isg_solve_info> info(n);
-    isg_status e = run_bicgs(c, x, g, 0, b, n, hermitian, &so, info.data(), st);
+    isg_solve_opts o = so;
+    o.guess = guess;
+    if (so.guess == ISG_GUESS_LEARNED && !hermitian && guess == ISG_GUESS_ZERO && c->fno) {
+      isg_status e = fno_apply(c, g, 0, b, x, n, ISG_ORDER_BLOCKED, st);
+      if (e != ISG_OK) return e;
+      o.guess = ISG_GUESS_CALLER;
+    }
+    isg_status e = run_bicgs(c, x, g, 0, b, n, hermitian, &o, info.data(), st);
     if (e == ISG_CUDA_ERROR || e == ISG_BAD_ARG || e == ISG_UNSUPPORTED || e == ISG_TIMEOUT) return e;
     solves += n;
     for (auto &i : info) iters += i.iterations;
@@ -205,6 +215,7 @@ struct Dbim {
   }
   // mom.cpp:247-271: od = sum over transmitters of conj(tot) (y + mlfmah(x))
   // with y = aggregateh(mesd) and x the adjoint solve with rhs conj(g) y.
+  bool warm_ready = false;  // adj holds a previous iteration's adjoint fields
   isg_status gradient(double regular) {
     isg_status e;
     cudaMemsetAsync(od, 0, (size_t)U * sizeof(double2), st);
@@ -219,7 +230,9 @@ struct Dbim {
       if ((e = run_aggregateh(c, Y, rxd, n, st)) != ISG_OK) return e;
       k_conj_g_mul<<<vgrid(n), 256, 0, st>>>(g, Y, C, U);
       count_launch();
-      if ((e = solve(X, C, n, 1)) != ISG_OK) return e;
+      float2 *xa = warm ? adj + (size_t)k * R * U : X;  // the previous adjoint fields, when kept
+      if ((e = solve(xa, C, n, 1, warm && warm_ready ? ISG_GUESS_CALLER : ISG_GUESS_ZERO)) != ISG_OK) return e;
+      if (warm) cudaMemcpyAsync(X, xa, (size_t)n * U * sizeof(float2), cudaMemcpyDeviceToDevice, st);
       if ((e = run_matvec(c, X, nullptr, 0, C, n, OP_GCONJ, so.engine, RED_NONE, nullptr, nullptr, st)) != ISG_OK)
         return e;
       k_add<<<vgrid(n), 256, 0, st>>>(Y, C, U);
@@ -227,6 +240,7 @@ struct Dbim {
       count_launch(2);
       if ((e = cuda_check(c, cudaStreamSynchronize(st), "dbim gradient")) != ISG_OK) return e;
     }
+    warm_ready = warm;
     return ISG_OK;
   }
   isg_status sums(const double2 *a, const double2 *b, const double2 *cc, int mode, double *out) {
@@ -258,6 +272,7 @@ void isg_default_dbim_opts(isg_dbim_opts *o) {
   o->start_from_chi = 0;
   isg_default_solve_opts(&o->solve);
   o->solve.tol = 1e-4;
+  o->warm_start = 0;
 }
 
 isg_status isg_measure(isg_ctx *c, int ntx, const void *inc, const double *chi, int order, double noise,
@@ -334,6 +349,11 @@ isg_status isg_dbim(isg_ctx *c, int ntx, const void *inc, const void *mes, const
   D.k2 = c->T.k0 * c->T.k0;
   D.so = O.solve;
   if (D.so.guess == ISG_GUESS_CALLER) D.so.guess = ISG_GUESS_ZERO;  // every reference solve starts at 0
+  if (D.so.guess == ISG_GUESS_LEARNED && !c->fno) {
+    c->err = "ISG_GUESS_LEARNED needs a warm-start network (isg_fno_create)";
+    return ISG_UNSUPPORTED;
+  }
+  D.warm = O.warm_start != 0;
   const size_t U = D.U, nm = (size_t)ntx * D.nrx;
   if ((e = D.alloc(&D.incb, (size_t)ntx * U)) || (e = D.alloc(&D.tot, (size_t)ntx * U)) ||
       (e = D.alloc(&D.X, (size_t)D.R * U)) || (e = D.alloc(&D.Y, (size_t)D.R * U)) ||
@@ -342,6 +362,7 @@ isg_status isg_dbim(isg_ctx *c, int ntx, const void *inc, const void *mes, const
       (e = D.alloc(&D.rxd, (size_t)D.R * D.nrx)) || (e = D.alloc(&D.part, 256 * 3)))
     return e;
   if (chi_true && (e = D.alloc(&D.otrue, U))) return e;
+  if (D.warm && (e = D.alloc(&D.adj, (size_t)ntx * U))) return e;
   const int *perm = order_perm(c, order);
   cudaStream_t st = D.st;
   // inputs into the blocked layout
@@ -440,7 +461,10 @@ isg_status isg_dbim(isg_ctx *c, int ntx, const void *inc, const void *mes, const
     for (int k = 0; k < D.nchunks(); k++) {
       const int n = D.chunk(k);
       float2 *tk = D.tot + (size_t)k * D.R * U;
-      if ((e = D.solve(tk, D.incb + (size_t)k * D.R * U, n, 0)) != ISG_OK) return e;
+      // warm: tk still holds this transmitter's total field of the previous contrast
+      if ((e = D.solve(tk, D.incb + (size_t)k * D.R * U, n, 0, D.warm ? ISG_GUESS_CALLER : ISG_GUESS_ZERO)) !=
+          ISG_OK)
+        return e;
       k_gx<<<D.vgrid(n), 256, 0, st>>>(D.X, D.g, tk, D.U, 1);
       count_launch();
       if ((e = D.far_field(D.X, k, n, D.rhs)) != ISG_OK) return e;

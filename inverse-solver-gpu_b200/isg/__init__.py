@@ -56,7 +56,7 @@ class SolveInfo(ctypes.Structure):
 
 class DbimOpts(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int), ("regular", ctypes.c_double), ("start_from_chi", ctypes.c_int),
-                ("solve", SolveOpts)]
+                ("solve", SolveOpts), ("warm_start", ctypes.c_int)]
 
 
 class DbimRecord(ctypes.Structure):
@@ -353,7 +353,8 @@ class Solver:
         return mes
 
     def dbim(self, inc, mes, chi=None, chi_true=None, iterations: int = 3, regular: float = 0.0,
-             order: int = ORDER_TREE, start_from_chi: bool = False, stream=None, **solve):
+             order: int = ORDER_TREE, start_from_chi: bool = False, warm_start: bool = False, stream=None,
+             **solve):
         """The reference's inversion loop (mom.cpp:222-399); returns (chi, history records)."""
         import torch
         ntx = 1 if inc.dim() == 1 else inc.shape[0]
@@ -362,6 +363,7 @@ class Solver:
         o = DbimOpts()
         lib().isg_default_dbim_opts(ctypes.byref(o))
         o.iterations, o.regular, o.start_from_chi = iterations, regular, int(start_from_chi)
+        o.warm_start = int(warm_start)
         for k, v in solve.items():
             setattr(o.solve, k, v)
         hist = (DbimRecord * (iterations + 1))()
