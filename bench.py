@@ -161,6 +161,16 @@ def cpu_reference_sample(g, b, budget_s: float, max_solves: int):
                       f"{threads} OpenMP threads, {t_total:.1f} s"}
 
 
+def max_over_ranks(v: float, dist, device) -> float:
+    """The largest of every rank's v (the job's time is its slowest rank's)."""
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_reference_arm(args, rank: int, world: int):
     """--impl reference: the reference's own CPU implementation, rank 0 only."""
     if rank != 0:
@@ -263,12 +273,10 @@ def main():
             iters.append([i["iterations"] for i in infos])
         ev1.record(stream)
         torch.cuda.synchronize()
-    launches = isg.kernel_launches() - launches0
-    ms = ev0.elapsed_time(ev1) / args.steps
     if dist:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        dist.barrier()
+    launches = isg.kernel_launches() - launches0
+    ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, dist, dev)
     bad = [i for i in infos if i["status"] != 0 or not (0 <= i["true_residual"] <= TOL)]
     value = world * NTX * 1000.0 / ms
 
@@ -287,7 +295,7 @@ def main():
             x_host.copy_(xd, non_blocking=True)
         e1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1) / max(1, args.steps)
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / max(1, args.steps), dist, dev)
 
     # Plain single-RHS FP32 solver: one transmitter per launch sequence.
     plain_opts = isg.default_solve_opts(tol=TOL, maxit=300, engine=isg.ENGINE_SIMT, check_every=1)
