@@ -85,6 +85,8 @@ typedef struct isg_solve_opts {
   int true_residual;   /* 1: after convergence recompute b - A x and restart any RHS above tol */
   int max_restarts;    /* restarts allowed by the true-residual check */
   int engine;          /* isg_engine */
+  int graph;           /* 1: replay the check_every-iteration block as a CUDA graph captured on the
+                          first poll (streams other than the legacy default stream); 0: launch directly */
 } isg_solve_opts;
 
 typedef struct isg_solve_info {

@@ -205,6 +205,7 @@ void isg_default_solve_opts(isg_solve_opts *o) {
   o->check_every = 1;
   o->true_residual = 1;
   o->max_restarts = 2;
+  o->graph = 1;
   o->engine = ISG_ENGINE_SIMT;
 }
 
@@ -351,6 +352,7 @@ isg_status isg_setup_gpu(isg_ctx *c) {
   if ((e = cuda_check(c, cudaMallocHost(&c->h_count, sizeof(int)), "cudaMallocHost"))) return e;
   if ((e = cuda_check(c, cudaMemset(c->mul, 0, R * P.mp * sizeof(float2)), "memset"))) return e;
   if ((e = cuda_check(c, cudaMemset(c->loc, 0, R * P.mp * sizeof(float2)), "memset"))) return e;
+  if ((e = cuda_check(c, kernels_setup(), "kernel attributes")) != ISG_OK) return e;
   if ((e = tc_setup(c)) != ISG_OK) return e;
   if ((e = band_setup(c)) != ISG_OK) return e;
   c->gpu_ready = true;
@@ -362,6 +364,7 @@ void isg_destroy(isg_ctx *c) {
   if (c->gpu_ready || !c->dev_allocs.empty()) {
     cudaSetDevice(c->opts.device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->graph_exec) cudaGraphExecDestroy((cudaGraphExec_t)c->graph_exec);
     fno_destroy(c);
     band_destroy(c);
     tc_destroy(c);

@@ -52,6 +52,19 @@ struct isg_ctx {
   isg::TcPlan *tc = nullptr;
   isg::BandPlan *band = nullptr;
   isg::FnoModel *fno = nullptr;
+  // BiCGSTAB iteration block captured as a CUDA graph, and what it was captured for
+  void *graph_exec = nullptr;
+  int64_t graph_launches = 0;
+  struct GraphKey {
+    const void *x = nullptr, *g = nullptr;
+    int64_t gs = 0;
+    int R = 0, kind = 0, engine = 0, check = 0, maxit = 0;
+    double tol = 0;
+    bool operator==(const GraphKey &o) const {
+      return x == o.x && g == o.g && gs == o.gs && R == o.R && kind == o.kind && engine == o.engine &&
+             check == o.check && maxit == o.maxit && tol == o.tol;
+    }
+  } graph_key;
   int *tc_err_flag() const;
 };
 

@@ -110,6 +110,10 @@ struct BatchArgs {
 // Process-wide count of kernel launches issued by this library.
 void count_launch(int n = 1);
 int64_t launch_count();
+// Non-null: this thread's launches go to *sink (graph capture); null: back to the count.
+void capture_launches(int64_t *sink);
+// Per-device kernel attributes (isg_kernels.cu), called by isg_setup_gpu.
+cudaError_t kernels_setup();
 
 // ---- launchers (isg_kernels.cu) ----
 void launch_p2m(const DevPlan &P, const BatchArgs &B, float2 *mul, cudaStream_t st);

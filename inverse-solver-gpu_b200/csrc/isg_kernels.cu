@@ -10,8 +10,17 @@
 namespace isg {
 
 static std::atomic<int64_t> g_launches{0};
-void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+// While this thread captures a CUDA graph its launches are tallied here
+// instead; each replay of the graph then counts them again.
+static thread_local int64_t *t_capture_sink = nullptr;
+void count_launch(int n) {
+  if (t_capture_sink)
+    *t_capture_sink += n;
+  else
+    g_launches.fetch_add(n, std::memory_order_relaxed);
+}
 int64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
+void capture_launches(int64_t *sink) { t_capture_sink = sink; }
 
 namespace {
 
@@ -576,7 +585,6 @@ void launch_m2m(const DevPlan &P, int lvl, float2 *mul, int nrhs, const int *act
   const TileArgs A = tile_args(mul, mul, P.mp, c.off, p.off, p.n, c.ns, p.ns, nrhs, p.mt, p.shmT, 32, active);
   const TileSmem L(p.mt.wmax, 4 * A.cols + 1, p.mt.out, 4 * A.cols, A.cols, (size_t)p.mt.out * (A.cols + 1));
   const size_t smem = L.total * sizeof(float2);
-  if (smem > 48 * 1024) cudaFuncSetAttribute(k_m2m_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   count_launch();
   k_m2m_tile<<<dim3((A.ncols + A.cols - 1) / A.cols, p.mt.tiles), A.cols * (p.mt.out / kTileOut), smem, st>>>(A);
 }
@@ -608,7 +616,6 @@ void launch_l2l(const DevPlan &P, int lvl, float2 *loc, int nrhs, const int *act
   const TileArgs A = tile_args(loc, loc, P.mp, p.off, c.off, p.n, p.ns, c.ns, nrhs, c.at, p.shlT, 64, active);
   const TileSmem L(c.at.wmax, A.cols + 1, c.at.out, A.cols, 4 * A.cols, (size_t)4 * c.at.out * (A.cols + 1));
   const size_t smem = L.total * sizeof(float2);
-  if (smem > 48 * 1024) cudaFuncSetAttribute(k_l2l_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   count_launch();
   k_l2l_tile<<<dim3((A.ncols + A.cols - 1) / A.cols, c.at.tiles), A.cols * (c.at.out / kTileOut), smem, st>>>(A);
 }
@@ -622,7 +629,6 @@ void launch_near(const DevPlan &P, const NearArgs &A, cudaStream_t st) {
   const int tiles_x = (P.nleaf + kNearTX - 1) / kNearTX;
   const int tiles = near_blocks_per_rhs(P);
   const size_t smem = (size_t)(kHaloLeaves * kBB + kNearTY * kNearTX * P.ns_leaf) * sizeof(float2);
-  if (smem > 48 * 1024) cudaFuncSetAttribute(k_near, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   dim3 grid(tiles, A.in.nrhs);
   count_launch();
   k_near<<<grid, 256, smem, st>>>(A.in.x, A.in.g, A.in.gstride, A.in.mode, A.in.active, A.loc + P.lv[P.L - 1].off,
@@ -648,4 +654,26 @@ void launch_permute(const int *perm, const float2 *in, float2 *out, int U, int n
   k_permute<<<grid, 256, 0, st>>>(perm, in, out, U, gather ? 1 : 0);
 }
 
+}  // namespace isg
+
+namespace isg {
+// Opt-in shared memory for the kernels whose size depends on the level, set
+// once per device so that no launch (and no graph capture) needs it.
+template <class K>
+static cudaError_t allow_max_smem(K kernel, int optin) {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, kernel);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+}
+
+cudaError_t kernels_setup() {
+  int dev = 0, optin = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e == cudaSuccess) e = allow_max_smem(k_m2m_tile, optin);
+  if (e == cudaSuccess) e = allow_max_smem(k_l2l_tile, optin);
+  if (e == cudaSuccess) e = allow_max_smem(k_near, optin);
+  return e;
+}
 }  // namespace isg

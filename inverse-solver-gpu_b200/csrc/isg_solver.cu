@@ -391,30 +391,76 @@ isg_status run_bicgs(isg_ctx *c, float2 *x, const float2 *g, int64_t gs, const f
   const int check = std::max(1, o->check_every);
   const long host_cap = (long)(o->maxit + 2) * (o->max_restarts + 1) + 8;
   long host_iters = 0;
+  // `check` iterations of every active RHS (bicgs.cpp:120-177); inactive ones return at once
+  auto block = [&]() -> isg_status {
+    for (int k = 0; k < check; k++) {
+      count_launch();
+      k_update_p<<<vgrid, 256, 0, st>>>(c->state, c->active, c->vr, c->vp, c->vv, U);
+      isg_status be = run_matvec(c, c->vp, g, gs, c->vv, R, kind, engine, RED_DOT, c->vrt, c->active, st);
+      if (be != ISG_OK) return be;
+      count_launch();
+      k_fin_alpha<<<R, 256, 0, st>>>(c->state, c->active, c->part, nbn);
+      count_launch();
+      k_update_s<<<vgrid, 256, 0, st>>>(c->state, c->active, c->vr, c->vv, c->vs, U);
+      be = run_matvec(c, c->vs, g, gs, c->vt, R, kind, engine, RED_TS, nullptr, c->active, st);
+      if (be != ISG_OK) return be;
+      count_launch();
+      k_fin_omega<<<R, 256, 0, st>>>(c->state, c->active, c->part, nbn);
+      count_launch();
+      k_update_xr<<<vgrid, 256, 0, st>>>(c->state, c->active, x, c->vr, c->vrt, c->vp, c->vs, c->vt, U, c->part);
+      cudaMemsetAsync(c->count, 0, sizeof(int), st);
+      count_launch();
+      k_fin_iter<<<R, 256, 0, st>>>(c->state, c->active, c->count, c->part, nbv, tol, o->maxit);
+    }
+    return cuda_check(c, cudaGetLastError(), "bicgs iteration");
+  };
+  // The block's launches depend only on the pointers and sizes below, so it is
+  // captured once and replayed (not on the legacy default stream, which cannot
+  // be captured).
+  isg_ctx::GraphKey key;
+  key.x = x;
+  key.g = g;
+  key.gs = gs;
+  key.R = R;
+  key.kind = kind;
+  key.engine = engine;
+  key.check = check;
+  key.maxit = o->maxit;
+  key.tol = tol;
+  const bool want_graph = o->graph && st != nullptr && st != cudaStreamLegacy && st != cudaStreamPerThread;
+  auto replay = [&]() -> isg_status {
+    if (!(c->graph_exec && c->graph_key == key)) {
+      if (c->graph_exec) cudaGraphExecDestroy((cudaGraphExec_t)c->graph_exec);
+      c->graph_exec = nullptr;
+      int64_t captured = 0;
+      isg_status ce = cuda_check(c, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "graph capture");
+      if (ce != ISG_OK) return ce;
+      capture_launches(&captured);
+      isg_status be = block();
+      capture_launches(nullptr);
+      cudaGraph_t gr = nullptr;
+      ce = cuda_check(c, cudaStreamEndCapture(st, &gr), "graph capture end");
+      if (be != ISG_OK || ce != ISG_OK) {
+        if (gr) cudaGraphDestroy(gr);
+        return be != ISG_OK ? be : ce;
+      }
+      cudaGraphExec_t ex = nullptr;
+      ce = cuda_check(c, cudaGraphInstantiate(&ex, gr, 0), "graph instantiate");
+      cudaGraphDestroy(gr);
+      if (ce != ISG_OK) return ce;
+      c->graph_exec = ex;
+      c->graph_key = key;
+      c->graph_launches = captured;
+    }
+    count_launch((int)c->graph_launches);
+    return cuda_check(c, cudaGraphLaunch((cudaGraphExec_t)c->graph_exec, st), "graph launch");
+  };
   for (;;) {
     cudaMemcpyAsync(c->h_count, c->count, sizeof(int), cudaMemcpyDeviceToHost, st);
     if ((e = cuda_check(c, cudaStreamSynchronize(st), "bicgs poll")) != ISG_OK) return e;
     if (*c->h_count > 0 && host_iters < host_cap) {
-      for (int k = 0; k < check; k++, host_iters++) {
-        count_launch();
-        k_update_p<<<vgrid, 256, 0, st>>>(c->state, c->active, c->vr, c->vp, c->vv, U);
-        e = run_matvec(c, c->vp, g, gs, c->vv, R, kind, engine, RED_DOT, c->vrt, c->active, st);
-        if (e != ISG_OK) return e;
-        count_launch();
-        k_fin_alpha<<<R, 256, 0, st>>>(c->state, c->active, c->part, nbn);
-        count_launch();
-        k_update_s<<<vgrid, 256, 0, st>>>(c->state, c->active, c->vr, c->vv, c->vs, U);
-        e = run_matvec(c, c->vs, g, gs, c->vt, R, kind, engine, RED_TS, nullptr, c->active, st);
-        if (e != ISG_OK) return e;
-        count_launch();
-        k_fin_omega<<<R, 256, 0, st>>>(c->state, c->active, c->part, nbn);
-        count_launch();
-        k_update_xr<<<vgrid, 256, 0, st>>>(c->state, c->active, x, c->vr, c->vrt, c->vp, c->vs, c->vt, U, c->part);
-        cudaMemsetAsync(c->count, 0, sizeof(int), st);
-        count_launch();
-        k_fin_iter<<<R, 256, 0, st>>>(c->state, c->active, c->count, c->part, nbv, tol, o->maxit);
-      }
-      if ((e = cuda_check(c, cudaGetLastError(), "bicgs iteration")) != ISG_OK) return e;
+      if ((e = want_graph ? replay() : block()) != ISG_OK) return e;
+      host_iters += check;
       continue;
     }
     if (!o->true_residual) break;

@@ -43,7 +43,7 @@ class Opts(ctypes.Structure):
 class SolveOpts(ctypes.Structure):
     _fields_ = [("tol", ctypes.c_double), ("maxit", ctypes.c_int), ("guess", ctypes.c_int),
                 ("check_every", ctypes.c_int), ("true_residual", ctypes.c_int), ("max_restarts", ctypes.c_int),
-                ("engine", ctypes.c_int)]
+                ("engine", ctypes.c_int), ("graph", ctypes.c_int)]
 
 
 class SolveInfo(ctypes.Structure):

@@ -96,3 +96,28 @@ def test_nonfinite_input_is_reported():
     infos = s.bicgs(X, torch_dev(g), torch_dev(B))
     assert infos[0]["status"] == 0
     assert infos[1]["status"] == 3
+
+
+def test_graph_replay_matches_direct_launches():
+    """The iteration block replayed as a CUDA graph (captured on the first poll,
+    reused by the next call with the same buffers) gives the same iterations
+    and fields as launching every kernel, and counts the same launches."""
+    import torch
+    s = isg.Solver(5, numrx=16, max_rhs=3, device=0)
+    o = Oracle(5)
+    pos = o.pos()
+    g = torch.from_numpy(disk_contrast(pos, radius=2.0, chi=0.4).astype(np.complex64)).cuda()
+    b = torch.from_numpy(np.stack([plane_wave(pos, a) for a in (0.0, 1.0, 2.0)]).astype(np.complex64)).cuda()
+    stream = torch.cuda.Stream()
+    runs = []
+    for graph in (0, 1, 1):
+        x = torch.zeros_like(b)
+        n0 = isg.kernel_launches()
+        info = s.bicgs(x, g, b, tol=1e-6, engine=isg.ENGINE_TENSOR, check_every=3, graph=graph, stream=stream)
+        stream.synchronize()
+        runs.append((x.cpu().numpy(), [i["iterations"] for i in info], isg.kernel_launches() - n0))
+        assert all(i["status"] == 0 for i in info)
+    (x0, it0, l0), (x1, it1, l1), (x2, it2, l2) = runs
+    assert it0 == it1 == it2
+    assert l0 == l1 == l2
+    assert np.array_equal(x0, x1) and np.array_equal(x1, x2)
