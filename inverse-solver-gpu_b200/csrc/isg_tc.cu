@@ -29,17 +29,19 @@ namespace {
 
 using namespace tc;
 
-constexpr int kTY = 16, kTX = 8;                 // leaves per tile
-constexpr int kHR = kTY + 2, kHC = kTX + 2;      // halo
+constexpr int kTY = 16, kTX = 8;                 // leaves per tile (one 128-row MMA)
+constexpr int kPair = 2;                         // tiles per CTA, stacked in y, sharing every weight stage
+constexpr int kHR = kPair * kTY + 2, kHC = kTX + 2;  // 34 x 10 halo of the pair
 constexpr int kLboA = kHC * 16;                  // 160
 constexpr int kSboA = 16 * kLboA;                // 2560 (one halo row: 16 K-chunks)
-constexpr int kRegion = kHR * kSboA;             // 46080 bytes per FP16 split
+constexpr int kRegion = kHR * kSboA;             // 87040 bytes per FP16 split
 constexpr int kStageBytes = 16384;               // hi [128 x 32] + lo [128 x 32]
 constexpr int kStageHalf = 8192;
-constexpr int kNB = 6;                           // ring depth
+constexpr int kNB = 3;                           // ring depth
 constexpr int kNearStages = 36;                  // 9 slots x 4 K-chunks of 32 reals
 constexpr int kLocChunksMax = 20;                // K chunks (8 reals each) of the L2P operand
 constexpr int kSboL = kLocChunksMax * 128;       // 2560
+constexpr int kL2pTile = 16 * kSboL;             // 40960: one tile's L2P operand per split
 constexpr int kLoaders = 224;                    // warps 0, 2..7
 constexpr int kErrNearFull = 101, kErrNearEmpty = 102, kErrNearDone = 103, kErrP2m = 111;
 
@@ -48,6 +50,7 @@ struct NearSmem {
   static constexpr int misc = bars + 16 * 8;
   static constexpr int total = misc + 256;
 };
+static_assert(kPair * kL2pTile <= kRegion, "the L2P operands reuse the halo region");
 
 __device__ __forceinline__ int loader_id() {
   const int w = threadIdx.x >> 5;
@@ -105,6 +108,7 @@ struct TcNearArgs {
   const float2 *dot_a;
   double *part;
   int nleaf, U, tiles_x, tiles;
+  int loc_vec;  // leaf locals can be copied in 16-byte chunks (ns % 4 == 0, aligned)
   int *err;
 };
 
@@ -120,8 +124,11 @@ __global__ void __launch_bounds__(256, 1) k_tc_near(TcNearArgs A) {
   float *scales = (float *)(sm + NearSmem::misc + 48);    // [2]
   double *dscr = (double *)(sm + NearSmem::misc + 64);    // [8][3]
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int tile = blockIdx.x;
-  const int ty0 = (tile / A.tiles_x) * kTY, tx0 = (tile % A.tiles_x) * kTX;
+  const int pair = blockIdx.x;
+  const int pty = pair / A.tiles_x, ptx = pair % A.tiles_x;
+  const int ty0 = pty * kPair * kTY, tx0 = ptx * kTX;
+  const int tiles_y = (A.nleaf + kTY - 1) / kTY;
+  const int ntile = min(kPair, tiles_y - pty * kPair);
   const size_t rbase = (size_t)rhs * A.U;
   const float2 *gr = A.g ? A.g + rhs * A.gstride : nullptr;
   const int nstages = kNearStages + A.nl2p;
@@ -134,56 +141,29 @@ __global__ void __launch_bounds__(256, 1) k_tc_near(TcNearArgs A) {
     mbar_init(done, 1);
     fence_mbar_init();
   }
-  if (warp == 0) tmem_alloc(tslot, 256);
+  if (warp == 0) tmem_alloc(tslot, 512);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  const uint32_t tmem = *tslot;
+  const uint32_t tmem = *tslot;  // near field of tile u in columns [128 u, +128), L2P in [256 + 128 u, +128)
 
-  // ---- halo of the input: every thread stages raw FP32 copies with cp.async,
-  // x where its FP16 hi/lo halves will go (first two pixels of a 4-pixel chunk
-  // in the hi slot, last two in the lo slot) and, for g x, the contrast in the
-  // weight ring (not streaming yet); the loaders then form g x and its max in
-  // place, and convert to hi/lo once the tile's scale is known ----
-  constexpr int kItems = kHR * kHC * 16;  // (halo leaf, 4-pixel chunk)
-  const bool with_g = A.mode == IN_G;
+  // ---- halo of the input: every thread stages x as FP32 with cp.async where its
+  // FP16 halves will go (first two pixels of a 4-pixel chunk in the hi slot,
+  // last two in the lo slot); the loaders then form g x and its max in place,
+  // and convert to hi/lo once the pair's scale is known ----
+  constexpr int kItems = kHR * kHC * 16;  // (halo row, 4-pixel chunk, halo column): consecutive
+                                          // items are consecutive 16-byte slots, free of bank conflicts
   for (int it = threadIdx.x; it < kItems; it += blockDim.x) {
-    const int h = it >> 4, c = it & 15;
-    const int ly = ty0 - 1 + h / kHC, lx = tx0 - 1 + h % kHC;
+    const int hc = it % kHC, c = (it / kHC) & 15, hr = it / (kHC * 16);
+    const int ly = ty0 - 1 + hr, lx = tx0 - 1 + hc;
     const bool in = ly >= 0 && ly < A.nleaf && lx >= 0 && lx < A.nleaf;
     const size_t i = in ? (size_t)(ly * A.nleaf + lx) * kBB + 4 * c : 0;
-    const int off = (h / kHC) * kSboA + c * kLboA + (h % kHC) * 16;
+    const int off = hr * kSboA + c * kLboA + hc * 16;
     cp_async16z(sm + NearSmem::hi + off, A.x + rbase + i, in);
     cp_async16z(sm + NearSmem::lo + off, A.x + rbase + i + 2, in);
-    if (with_g) {
-      cp_async16z(sm + NearSmem::stages + it * 32, gr + i, in);
-      cp_async16z(sm + NearSmem::stages + it * 32 + 16, gr + i + 2, in);
-    }
   }
   cp_async_wait_all();
   __syncthreads();
-  float mx = 0.f;
-  if (warp != 1) {
-    for (int it = loader_id(); it < kItems; it += kLoaders) {
-      const int h = it >> 4, c = it & 15;
-      const int off = (h / kHC) * kSboA + c * kLboA + (h % kHC) * 16;
-      float4 *ph = (float4 *)(sm + NearSmem::hi + off), *pl = (float4 *)(sm + NearSmem::lo + off);
-      const float4 a0 = *ph, a1 = *pl;
-      float4 g0 = make_float4(0.f, 0.f, 0.f, 0.f), g1 = g0;
-      if (with_g) {
-        g0 = *(const float4 *)(sm + NearSmem::stages + it * 32);
-        g1 = *(const float4 *)(sm + NearSmem::stages + it * 32 + 16);
-      }
-      const float2 v0 = transform(make_float2(a0.x, a0.y), make_float2(g0.x, g0.y), A.mode);
-      const float2 v1 = transform(make_float2(a0.z, a0.w), make_float2(g0.z, g0.w), A.mode);
-      const float2 v2 = transform(make_float2(a1.x, a1.y), make_float2(g1.x, g1.y), A.mode);
-      const float2 v3 = transform(make_float2(a1.z, a1.w), make_float2(g1.z, g1.w), A.mode);
-      mx = fmaxf(mx, fmaxf(fmaxf(cabs1(v0), cabs1(v1)), fmaxf(cabs1(v2), cabs1(v3))));
-      *ph = make_float4(v0.x, v0.y, v1.x, v1.y);
-      *pl = make_float4(v2.x, v2.y, v3.x, v3.y);
-    }
-  }
-  __syncthreads();  // the ring is free for the weights
 
   if (warp == 1) {
     // ---- producer: weight stages through the ring ----
@@ -197,10 +177,34 @@ __global__ void __launch_bounds__(256, 1) k_tc_near(TcNearArgs A) {
     }
   } else {
     const int li = loader_id();
+    float mx = 0.f;
+#pragma unroll 8
+    for (int it = li; it < kItems; it += kLoaders) {
+      const int hc = it % kHC, c = (it / kHC) & 15, hr = it / (kHC * 16);
+      const int off = hr * kSboA + c * kLboA + hc * 16;
+      float4 *ph = (float4 *)(sm + NearSmem::hi + off), *pl = (float4 *)(sm + NearSmem::lo + off);
+      float4 g0 = make_float4(0.f, 0.f, 0.f, 0.f), g1 = g0;
+      if (A.mode == IN_G) {
+        const int ly = ty0 - 1 + hr, lx = tx0 - 1 + hc;
+        if (ly >= 0 && ly < A.nleaf && lx >= 0 && lx < A.nleaf) {
+          const size_t i = (size_t)(ly * A.nleaf + lx) * kBB + 4 * c;
+          g0 = *(const float4 *)(gr + i);
+          g1 = *(const float4 *)(gr + i + 2);
+        }
+      }
+      const float4 a0 = *ph, a1 = *pl;
+      const float2 v0 = transform(make_float2(a0.x, a0.y), make_float2(g0.x, g0.y), A.mode);
+      const float2 v1 = transform(make_float2(a0.z, a0.w), make_float2(g0.z, g0.w), A.mode);
+      const float2 v2 = transform(make_float2(a1.x, a1.y), make_float2(g1.x, g1.y), A.mode);
+      const float2 v3 = transform(make_float2(a1.z, a1.w), make_float2(g1.z, g1.w), A.mode);
+      mx = fmaxf(mx, fmaxf(fmaxf(cabs1(v0), cabs1(v1)), fmaxf(cabs1(v2), cabs1(v3))));
+      *ph = make_float4(v0.x, v0.y, v1.x, v1.y);
+      *pl = make_float4(v2.x, v2.y, v3.x, v3.y);
+    }
     const float s1 = pow2_scale(loaders_max(mx, fscr));
     for (int it = li; it < kItems; it += kLoaders) {
-      const int h = it >> 4, c = it & 15;
-      const int off = (h / kHC) * kSboA + c * kLboA + (h % kHC) * 16;
+      const int hc = it % kHC, c = (it / kHC) & 15, hr = it / (kHC * 16);
+      const int off = hr * kSboA + c * kLboA + hc * 16;
       const float4 q0 = *(const float4 *)(sm + NearSmem::hi + off), q1 = *(const float4 *)(sm + NearSmem::lo + off);
       const float2 v[4] = {make_float2(q0.x, q0.y), make_float2(q0.z, q0.w), make_float2(q1.x, q1.y),
                            make_float2(q1.z, q1.w)};
@@ -210,7 +214,7 @@ __global__ void __launch_bounds__(256, 1) k_tc_near(TcNearArgs A) {
     fence_proxy_async();
     loaders_bar();
 
-    // ---- MMA issue: near field into D1 = columns [0, 128) ----
+    // ---- MMA issue: every weight stage serves both tiles of the pair ----
     const uint32_t idesc = idesc_f16_f32(128, 128);
     const uint32_t sbase = smem_u32(sm);
     if (threadIdx.x == 0) {
@@ -219,61 +223,80 @@ __global__ void __launch_bounds__(256, 1) k_tc_near(TcNearArgs A) {
         const int b = t % kNB;
         if (!mbar_wait(&full[b], (t / kNB) & 1, A.err, kErrNearFull)) break;
         const int s = t >> 2, c = t & 3, dr = s / 3 - 1, dc = s % 3 - 1;
-        const uint32_t abase = (1 + dr) * kSboA + (1 + dc) * 16;
         const uint32_t bst = sbase + NearSmem::stages + b * kStageBytes;
 #pragma unroll
         for (int ks = 0; ks < 2; ks++) {
-          const uint32_t aoff = abase + (uint32_t)(c * 4 + ks * 2) * kLboA;
-          const uint64_t ahi = smem_desc(sbase + NearSmem::hi + aoff, kLboA, kSboA);
-          const uint64_t alo = smem_desc(sbase + NearSmem::lo + aoff, kLboA, kSboA);
           const uint64_t bhi = smem_desc(bst + ks * 256, 128, 512);
           const uint64_t blo = smem_desc(bst + kStageHalf + ks * 256, 128, 512);
-          mma_f16(tmem, ahi, bhi, idesc, (t | ks) ? 1 : 0);
-          mma_f16(tmem, ahi, blo, idesc, 1);
-          mma_f16(tmem, alo, bhi, idesc, 1);
+          for (int u = 0; u < ntile; u++) {
+            const uint32_t aoff = (u * kTY + 1 + dr) * kSboA + (1 + dc) * 16 + (uint32_t)(c * 4 + ks * 2) * kLboA;
+            const uint64_t ahi = smem_desc(sbase + NearSmem::hi + aoff, kLboA, kSboA);
+            const uint64_t alo = smem_desc(sbase + NearSmem::lo + aoff, kLboA, kSboA);
+            const uint32_t d = tmem + 128 * u;
+            mma_f16(d, ahi, bhi, idesc, (t | ks) ? 1 : 0);
+            mma_f16(d, ahi, blo, idesc, 1);
+            mma_f16(d, alo, bhi, idesc, 1);
+          }
         }
         mma_commit(&empty[b]);
       }
       mma_commit(done);
     }
 
-    // ---- L2P operand: leaf locals of the tile, once the near MMAs are done ----
-    constexpr int kLItems = 128 * kLocChunksMax;
-    constexpr int kLPer = (kLItems + kLoaders - 1) / kLoaders;
+    // ---- L2P operands: the tiles' leaf locals, staged with cp.async into the
+    // halo region once the near-field MMAs are done, then scaled and converted ----
     const int nchunk = (A.ns + 3) / 4;
-    float2 w[kLPer][4];
-    float mx2 = 0.f;
+    const bool vec_ok = A.loc_vec != 0;
+    const int kL = ntile * 128 * kLocChunksMax;
     const float2 *lr = A.loc_leaf + (size_t)rhs * A.mp;
+    const bool near_ok = mbar_wait(done, 0, A.err, kErrNearDone);
+    float s2 = 1.f;
+    if (near_ok) {
+      for (int it = li; it < kL; it += kLoaders) {
+        // (tile, row group, chunk, row in group): consecutive 16-byte slots
+        const int m7 = it & 7, c = (it >> 3) % kLocChunksMax, mg = (it >> 3) / kLocChunksMax;
+        const int u = mg >> 4, m = ((mg & 15) << 3) | m7;
+        const int ly = ty0 + u * kTY + m / kTX, lx = tx0 + m % kTX;
+        const bool valid = c < nchunk && ly < A.nleaf && lx < A.nleaf;
+        const int off = u * kL2pTile + (m >> 3) * kSboL + c * 128 + (m & 7) * 16;
+        const float2 *src = lr + (valid ? (size_t)(ly * A.nleaf + lx) * A.ns + 4 * c : 0);
+        if (vec_ok) {
+          cp_async16z(sm + NearSmem::hi + off, src, valid);
+          cp_async16z(sm + NearSmem::lo + off, src + 2, valid);
+        } else {
+          float2 v[4];
 #pragma unroll
-    for (int r = 0; r < kLPer; r++) {
-      const int it = li + r * kLoaders;
-#pragma unroll
-      for (int p = 0; p < 4; p++) w[r][p] = make_float2(0.f, 0.f);
-      if (it < kLItems) {
-        const int m = it / kLocChunksMax, c = it % kLocChunksMax;
-        const int ly = ty0 + m / kTX, lx = tx0 + m % kTX;
-        if (c < nchunk && ly < A.nleaf && lx < A.nleaf) {
-          const float2 *src = lr + (size_t)(ly * A.nleaf + lx) * A.ns + 4 * c;
-#pragma unroll
-          for (int p = 0; p < 4; p++)
-            if (4 * c + p < A.ns) w[r][p] = src[p];
-#pragma unroll
-          for (int p = 0; p < 4; p++) mx2 = fmaxf(mx2, cabs1(w[r][p]));
+          for (int p = 0; p < 4; p++) v[p] = (valid && 4 * c + p < A.ns) ? src[p] : make_float2(0.f, 0.f);
+          *(float4 *)(sm + NearSmem::hi + off) = make_float4(v[0].x, v[0].y, v[1].x, v[1].y);
+          *(float4 *)(sm + NearSmem::lo + off) = make_float4(v[2].x, v[2].y, v[3].x, v[3].y);
         }
       }
-    }
-    const float s2 = pow2_scale(loaders_max(mx2, fscr));
-    if (!mbar_wait(done, 0, A.err, kErrNearDone)) {
-      // leave the operand region untouched; the result is flagged
+      cp_async_wait_all();
+      loaders_bar();
+      float mx2 = 0.f;
+      for (int it = li; it < kL; it += kLoaders) {
+        // (tile, row group, chunk, row in group): consecutive 16-byte slots
+        const int m7 = it & 7, c = (it >> 3) % kLocChunksMax, mg = (it >> 3) / kLocChunksMax;
+        const int u = mg >> 4, m = ((mg & 15) << 3) | m7;
+        const int off = u * kL2pTile + (m >> 3) * kSboL + c * 128 + (m & 7) * 16;
+        const float4 q0 = *(const float4 *)(sm + NearSmem::hi + off), q1 = *(const float4 *)(sm + NearSmem::lo + off);
+        mx2 = fmaxf(mx2, fmaxf(fmaxf(fabsf(q0.x), fabsf(q0.y)), fmaxf(fabsf(q0.z), fabsf(q0.w))));
+        mx2 = fmaxf(mx2, fmaxf(fmaxf(fabsf(q1.x), fabsf(q1.y)), fmaxf(fabsf(q1.z), fabsf(q1.w))));
+      }
+      s2 = pow2_scale(loaders_max(mx2, fscr));
+      for (int it = li; it < kL; it += kLoaders) {
+        // (tile, row group, chunk, row in group): consecutive 16-byte slots
+        const int m7 = it & 7, c = (it >> 3) % kLocChunksMax, mg = (it >> 3) / kLocChunksMax;
+        const int u = mg >> 4, m = ((mg & 15) << 3) | m7;
+        const int off = u * kL2pTile + (m >> 3) * kSboL + c * 128 + (m & 7) * 16;
+        const float4 q0 = *(const float4 *)(sm + NearSmem::hi + off), q1 = *(const float4 *)(sm + NearSmem::lo + off);
+        const float2 v[4] = {make_float2(q0.x, q0.y), make_float2(q0.z, q0.w), make_float2(q1.x, q1.y),
+                             make_float2(q1.z, q1.w)};
+        store_chunk(sm, off, v, s2);
+      }
     } else {
-#pragma unroll
-      for (int r = 0; r < kLPer; r++) {
-        const int it = li + r * kLoaders;
-        if (it < kLItems) {
-          const int m = it / kLocChunksMax, c = it % kLocChunksMax;
-          store_chunk(sm, (m >> 3) * kSboL + c * 128 + (m & 7) * 16, w[r], s2);
-        }
-      }
+      loaders_bar();  // keeps the named-barrier count of the loaders the same on this path
+      (void)loaders_max(0.f, fscr);
     }
     if (li == 0) scales[1] = s2;
     fence_proxy_async();
@@ -287,14 +310,17 @@ __global__ void __launch_bounds__(256, 1) k_tc_near(TcNearArgs A) {
         const uint32_t bst = sbase + NearSmem::stages + b * kStageBytes;
 #pragma unroll
         for (int ks = 0; ks < 2; ks++) {
-          const uint32_t aoff = (uint32_t)(c * 4 + ks * 2) * 128;
-          const uint64_t ahi = smem_desc(sbase + NearSmem::hi + aoff, 128, kSboL);
-          const uint64_t alo = smem_desc(sbase + NearSmem::lo + aoff, 128, kSboL);
           const uint64_t bhi = smem_desc(bst + ks * 256, 128, 512);
           const uint64_t blo = smem_desc(bst + kStageHalf + ks * 256, 128, 512);
-          mma_f16(tmem + 128, ahi, bhi, idesc, (c | ks) ? 1 : 0);
-          mma_f16(tmem + 128, ahi, blo, idesc, 1);
-          mma_f16(tmem + 128, alo, bhi, idesc, 1);
+          for (int u = 0; u < ntile; u++) {
+            const uint32_t aoff = u * kL2pTile + (uint32_t)(c * 4 + ks * 2) * 128;
+            const uint64_t ahi = smem_desc(sbase + NearSmem::hi + aoff, 128, kSboL);
+            const uint64_t alo = smem_desc(sbase + NearSmem::lo + aoff, 128, kSboL);
+            const uint32_t d = tmem + 256 + 128 * u;
+            mma_f16(d, ahi, bhi, idesc, (c | ks) ? 1 : 0);
+            mma_f16(d, ahi, blo, idesc, 1);
+            mma_f16(d, alo, bhi, idesc, 1);
+          }
         }
         mma_commit(&empty[b]);
       }
@@ -302,101 +328,109 @@ __global__ void __launch_bounds__(256, 1) k_tc_near(TcNearArgs A) {
     }
   }
 
-  // ---- epilogue (all warps) ----
+  // ---- epilogue (all warps), one tile of the pair at a time ----
   const int q = warp & 3, hh = warp >> 2;
   const int m = 32 * q + lane;
-  const int ly = ty0 + m / kTX, lx = tx0 + m % kTX;
-  const bool in_grid = ly < A.nleaf && lx < A.nleaf;
-  const size_t leafbase = rbase + (size_t)(ly * A.nleaf + lx) * kBB;
-  // this thread's 32 input pixels, fetched while the last MMAs run
-  const bool need_x = in_grid && (A.epi == EPI_FWD || A.epi == EPI_ADJ || A.red == RED_TS);
-  float4 xpre[4][4];
+  const bool need_x = A.epi == EPI_FWD || A.epi == EPI_ADJ || A.red == RED_TS;
+  bool ok = true;
+  for (int u = 0; u < ntile; u++) {
+    const int ly = ty0 + u * kTY + m / kTX, lx = tx0 + m % kTX;
+    const bool in_grid = ly < A.nleaf && lx < A.nleaf;
+    const size_t leafbase = rbase + (size_t)(ly * A.nleaf + lx) * kBB;
+    // this thread's 32 input pixels (for the first tile, fetched while the last MMAs run)
+    float4 xpre[4][4];
 #pragma unroll
-  for (int ch = 0; ch < 4; ch++)
+    for (int ch = 0; ch < 4; ch++)
 #pragma unroll
-    for (int pp = 0; pp < 4; pp++)
-      xpre[ch][pp] = need_x ? *(const float4 *)(A.x + leafbase + 32 * hh + 8 * ch + 2 * pp)
-                            : make_float4(0.f, 0.f, 0.f, 0.f);
-  const bool ok = mbar_wait(done, 1, A.err, kErrNearDone);
-  __syncthreads();
-  tc_fence_after();
-  const float inv1 = A.inv_w / scales[0], inv2 = A.inv_b / scales[1];
-  const bool valid = ok && in_grid;
-  double r0 = 0, r1 = 0, r2 = 0;
+      for (int pp = 0; pp < 4; pp++)
+        xpre[ch][pp] = (need_x && in_grid) ? *(const float4 *)(A.x + leafbase + 32 * hh + 8 * ch + 2 * pp)
+                                           : make_float4(0.f, 0.f, 0.f, 0.f);
+    if (u == 0) {
+      ok = mbar_wait(done, 1, A.err, kErrNearDone);
+      __syncthreads();
+      tc_fence_after();
+    }
+    const float inv1 = A.inv_w / scales[0], inv2 = A.inv_b / scales[1];
+    const bool valid = ok && in_grid;
+    double r0 = 0, r1 = 0, r2 = 0;
 #pragma unroll
-  for (int ch = 0; ch < 4; ch++) {
-    const int col = 64 * hh + 16 * ch;
-    float d1[16], d2[16];
-    tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + col, d1);
-    tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + 128 + col, d2);
-    if (!valid) continue;
+    for (int ch = 0; ch < 4; ch++) {
+      const int col = 64 * hh + 16 * ch;
+      float d1[16], d2[16];
+      tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + 128 * u + col, d1);
+      tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + 256 + 128 * u + col, d2);
+      if (!valid) continue;
 #pragma unroll
-    for (int p = 0; p < 8; p += 2) {
-      const int t0 = col / 2 + p;  // complex pixel
-      float2 o[2];
+      for (int p = 0; p < 8; p += 2) {
+        const int t0 = col / 2 + p;  // complex pixel
+        float2 o[2];
 #pragma unroll
-      for (int e = 0; e < 2; e++)
-        o[e] = make_float2(d1[2 * (p + e)] * inv1 + d2[2 * (p + e)] * inv2,
-                           d1[2 * (p + e) + 1] * inv1 + d2[2 * (p + e) + 1] * inv2);
-      const size_t i = leafbase + t0;
-      const float4 xv = xpre[ch][p / 2];
-      const float2 xin[2] = {make_float2(xv.x, xv.y), make_float2(xv.z, xv.w)};
-      if (A.epi == EPI_FWD) {
-        o[0] = csub(xin[0], o[0]);
-        o[1] = csub(xin[1], o[1]);
-      } else if (A.epi == EPI_ADJ) {
-        const float4 gv = *(const float4 *)(gr + (i - rbase));
-        o[0] = csub(xin[0], cconj(cmul(make_float2(gv.x, gv.y), o[0])));
-        o[1] = csub(xin[1], cconj(cmul(make_float2(gv.z, gv.w), o[1])));
-      } else if (A.epi == EPI_CONJ) {
-        o[0] = cconj(o[0]);
-        o[1] = cconj(o[1]);
-      }
-      *(float4 *)(A.y + i) = make_float4(o[0].x, o[0].y, o[1].x, o[1].y);
-      if (A.red == RED_DOT) {
-        const float4 av = *(const float4 *)(A.dot_a + i);
-        const float2 a0 = make_float2(av.x, av.y), a1 = make_float2(av.z, av.w);
-        r0 += (double)a0.x * o[0].x + (double)a0.y * o[0].y + (double)a1.x * o[1].x + (double)a1.y * o[1].y;
-        r1 += (double)a0.x * o[0].y - (double)a0.y * o[0].x + (double)a1.x * o[1].y - (double)a1.y * o[1].x;
-      } else if (A.red == RED_TS) {
+        for (int e = 0; e < 2; e++)
+          o[e] = make_float2(d1[2 * (p + e)] * inv1 + d2[2 * (p + e)] * inv2,
+                             d1[2 * (p + e) + 1] * inv1 + d2[2 * (p + e) + 1] * inv2);
+        const size_t i = leafbase + t0;
+        const float4 xv = xpre[ch][p / 2];
+        const float2 xin[2] = {make_float2(xv.x, xv.y), make_float2(xv.z, xv.w)};
+        if (A.epi == EPI_FWD) {
+          o[0] = csub(xin[0], o[0]);
+          o[1] = csub(xin[1], o[1]);
+        } else if (A.epi == EPI_ADJ) {
+          const float4 gv = *(const float4 *)(gr + (i - rbase));
+          o[0] = csub(xin[0], cconj(cmul(make_float2(gv.x, gv.y), o[0])));
+          o[1] = csub(xin[1], cconj(cmul(make_float2(gv.z, gv.w), o[1])));
+        } else if (A.epi == EPI_CONJ) {
+          o[0] = cconj(o[0]);
+          o[1] = cconj(o[1]);
+        }
+        *(float4 *)(A.y + i) = make_float4(o[0].x, o[0].y, o[1].x, o[1].y);
+        if (A.red == RED_DOT) {
+          const float4 av = *(const float4 *)(A.dot_a + i);
+          const float2 a0 = make_float2(av.x, av.y), a1 = make_float2(av.z, av.w);
+          r0 += (double)a0.x * o[0].x + (double)a0.y * o[0].y + (double)a1.x * o[1].x + (double)a1.y * o[1].y;
+          r1 += (double)a0.x * o[0].y - (double)a0.y * o[0].x + (double)a1.x * o[1].y - (double)a1.y * o[1].x;
+        } else if (A.red == RED_TS) {
 #pragma unroll
-        for (int e = 0; e < 2; e++) {
-          r0 += (double)o[e].x * xin[e].x + (double)o[e].y * xin[e].y;
-          r1 += (double)o[e].x * xin[e].y - (double)o[e].y * xin[e].x;
-          r2 += (double)o[e].x * o[e].x + (double)o[e].y * o[e].y;
+          for (int e = 0; e < 2; e++) {
+            r0 += (double)o[e].x * xin[e].x + (double)o[e].y * xin[e].y;
+            r1 += (double)o[e].x * xin[e].y - (double)o[e].y * xin[e].x;
+            r2 += (double)o[e].x * o[e].x + (double)o[e].y * o[e].y;
+          }
         }
       }
     }
-  }
-  if (A.red != RED_NONE) {
+    if (A.red != RED_NONE) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      r0 += __shfl_xor_sync(0xffffffffu, r0, o);
-      r1 += __shfl_xor_sync(0xffffffffu, r1, o);
-      r2 += __shfl_xor_sync(0xffffffffu, r2, o);
+      for (int o = 16; o > 0; o >>= 1) {
+        r0 += __shfl_xor_sync(0xffffffffu, r0, o);
+        r1 += __shfl_xor_sync(0xffffffffu, r1, o);
+        r2 += __shfl_xor_sync(0xffffffffu, r2, o);
+      }
+      if (lane == 0) {
+        dscr[warp * 3 + 0] = r0;
+        dscr[warp * 3 + 1] = r1;
+        dscr[warp * 3 + 2] = r2;
+      }
     }
-    if (lane == 0) {
-      dscr[warp * 3 + 0] = r0;
-      dscr[warp * 3 + 1] = r1;
-      dscr[warp * 3 + 2] = r2;
+    __syncthreads();
+    if (A.red != RED_NONE && threadIdx.x == 0) {
+      double s0 = 0, s1v = 0, s2v = 0;
+      for (int w2 = 0; w2 < 8; w2++) {
+        s0 += dscr[w2 * 3 + 0];
+        s1v += dscr[w2 * 3 + 1];
+        s2v += dscr[w2 * 3 + 2];
+      }
+      const int tile = (pty * kPair + u) * A.tiles_x + ptx;
+      double *p = A.part + ((size_t)rhs * A.tiles + tile) * 4;
+      p[0] = s0;
+      p[1] = s1v;
+      p[2] = s2v;
+      p[3] = 0;
     }
+    __syncthreads();  // dscr is reused by the next tile
   }
   tc_fence_before();
   __syncthreads();
-  if (A.red != RED_NONE && threadIdx.x == 0) {
-    double s0 = 0, s1 = 0, s2 = 0;
-    for (int w2 = 0; w2 < 8; w2++) {
-      s0 += dscr[w2 * 3 + 0];
-      s1 += dscr[w2 * 3 + 1];
-      s2 += dscr[w2 * 3 + 2];
-    }
-    double *p = A.part + ((size_t)rhs * A.tiles + tile) * 4;
-    p[0] = s0;
-    p[1] = s1;
-    p[2] = s2;
-    p[3] = 0;
-  }
-  if (warp == 0) tmem_dealloc(tmem, 256);
+  if (warp == 0) tmem_dealloc(tmem, 512);
 }
 
 // ---- P2M: 128 consecutive leaves of one RHS per CTA, N = 2 ns padded to 16 ----
@@ -700,10 +734,13 @@ isg_status tc_near(isg_ctx *c, const NearArgs &N, cudaStream_t st) {
   A.nleaf = P.nleaf;
   A.U = P.U;
   A.tiles_x = (P.nleaf + kTX - 1) / kTX;
-  A.tiles = A.tiles_x * ((P.nleaf + kTY - 1) / kTY);
+  const int tiles_y = (P.nleaf + kTY - 1) / kTY;
+  A.tiles = A.tiles_x * tiles_y;
+  A.loc_vec = (P.ns_leaf % 4 == 0) && aligned16(A.loc_leaf) && (P.mp % 2 == 0);
   A.err = T.err;
   count_launch();
-  k_tc_near<<<dim3(A.tiles, N.in.nrhs), 256, NearSmem::total, st>>>(A);
+  const int pairs = A.tiles_x * ((tiles_y + kPair - 1) / kPair);
+  k_tc_near<<<dim3(pairs, N.in.nrhs), 256, NearSmem::total, st>>>(A);
   return cuda_check(c, cudaGetLastError(), "tc near launch");
 }
 
