@@ -345,7 +345,7 @@ isg_status isg_setup_gpu(isg_ctx *c) {
   if ((e = dalloc(c, &c->mul, R * P.mp)) || (e = dalloc(c, &c->loc, R * P.mp)) || (e = dalloc(c, &c->wx, R * U)) ||
       (e = dalloc(c, &c->wy, R * U)) || (e = dalloc(c, &c->wg, R * U)) || (e = dalloc(c, &c->vr, R * U)) ||
       (e = dalloc(c, &c->vrt, R * U)) || (e = dalloc(c, &c->vp, R * U)) || (e = dalloc(c, &c->vv, R * U)) ||
-      (e = dalloc(c, &c->vs, R * U)) || (e = dalloc(c, &c->vt, R * U)) ||
+      (e = dalloc(c, &c->vs, R * U)) || (e = dalloc(c, &c->vt, R * U)) || (e = dalloc(c, &c->vgx, R * U)) ||
       (e = dalloc(c, &c->part, R * (size_t)c->part_blocks * 4 + 64)) || (e = dalloc(c, &c->state, R)) ||
       (e = dalloc(c, &c->active, R)) || (e = dalloc(c, &c->count, 1)))
     return e;

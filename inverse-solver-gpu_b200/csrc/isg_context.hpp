@@ -42,6 +42,7 @@ struct isg_ctx {
   float2 *wx = nullptr, *wy = nullptr;    // [R][U] reorder scratch
   float2 *wg = nullptr;                   // [R][U] contrast in blocked order
   float2 *vr = nullptr, *vrt = nullptr, *vp = nullptr, *vv = nullptr, *vs = nullptr, *vt = nullptr;
+  float2 *vgx = nullptr;  // [R][U] g times the next matvec's input, written by the update kernels
   double *part = nullptr;  // [R][part_blocks][4]
   int part_blocks = 0;
   isg::RhsState *state = nullptr;  // [R]
@@ -72,7 +73,8 @@ namespace isg {
 // Internal operator entry points shared by the C ABI and the solver.
 enum OpKind { OP_G = 0, OP_GCONJ = 1, OP_FWD = 2, OP_ADJ = 3 };
 isg_status run_matvec(isg_ctx *c, const float2 *x, const float2 *g, int64_t gs, float2 *y, int nrhs, int kind,
-                      int engine, int red, const float2 *dot_a, const int *active, cudaStream_t st);
+                      int engine, int red, const float2 *dot_a, const int *active, cudaStream_t st,
+                      const float2 *gx = nullptr);
 isg_status run_bicgs(isg_ctx *c, float2 *x, const float2 *g, int64_t gs, const float2 *b, int nrhs, int hermitian,
                      const isg_solve_opts *o, isg_solve_info *info, cudaStream_t st);
 isg_status cuda_check(isg_ctx *c, cudaError_t e, const char *what);

@@ -150,21 +150,24 @@ __global__ void __launch_bounds__(256) k_fin_init(RhsState *st, int *active, int
 
 // p = r (first iteration) or p = r + beta (p - omega v), beta = (rho/rho1)(alpha/omega)
 // (bicgs.cpp:132-139).
+// With gp: also gp = g p, the input of the forward matvec that follows.
 __global__ void __launch_bounds__(256) k_update_p(const RhsState *st, const int *active, const float2 *__restrict__ r,
-                                                  float2 *__restrict__ p, const float2 *__restrict__ v, int U) {
+                                                  float2 *__restrict__ p, const float2 *__restrict__ v, int U,
+                                                  const float2 *__restrict__ g, int64_t gstride,
+                                                  float2 *__restrict__ gp) {
   const int rhs = blockIdx.y;
   if (inactive(active, rhs)) return;
   const RhsState &s = st[rhs];
   const size_t base = (size_t)rhs * U;
-  if (s.fresh) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < U; i += gridDim.x * blockDim.x) p[base + i] = r[base + i];
-    return;
-  }
-  const double2 beta = dmul(cdiv(ld2(s.rho), ld2(s.rho1)), cdiv(ld2(s.alpha), ld2(s.omega)));
-  const float2 bf = f2(beta), of = f2(ld2(s.omega));
+  const float2 *gr = g + rhs * gstride;
+  const bool fresh = s.fresh;
+  const double2 beta = fresh ? make_double2(0.0, 0.0) : dmul(cdiv(ld2(s.rho), ld2(s.rho1)), cdiv(ld2(s.alpha), ld2(s.omega)));
+  const float2 bf = f2(beta), of = fresh ? make_float2(0.f, 0.f) : f2(ld2(s.omega));
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < U; i += gridDim.x * blockDim.x) {
-    const float2 pv = p[base + i], vv = v[base + i];
-    p[base + i] = cadd(r[base + i], cmul(bf, csub(pv, cmul(of, vv))));
+    float2 pn = r[base + i];
+    if (!fresh) pn = cadd(pn, cmul(bf, csub(p[base + i], cmul(of, v[base + i]))));
+    p[base + i] = pn;
+    if (gp) gp[base + i] = cmul(gr[i], pn);
   }
 }
 
@@ -188,14 +191,21 @@ __global__ void __launch_bounds__(256) k_fin_alpha(RhsState *st, int *active, co
 }
 
 // s = r - alpha v (bicgs.cpp:146).
+// With gsv: also gsv = g s, the input of the forward matvec that follows.
 __global__ void __launch_bounds__(256) k_update_s(const RhsState *st, const int *active, const float2 *__restrict__ r,
-                                                  const float2 *__restrict__ v, float2 *__restrict__ s, int U) {
+                                                  const float2 *__restrict__ v, float2 *__restrict__ s, int U,
+                                                  const float2 *__restrict__ g, int64_t gstride,
+                                                  float2 *__restrict__ gsv) {
   const int rhs = blockIdx.y;
   if (inactive(active, rhs)) return;
   const float2 a = f2(ld2(st[rhs].alpha));
   const size_t base = (size_t)rhs * U;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < U; i += gridDim.x * blockDim.x)
-    s[base + i] = csub(r[base + i], cmul(a, v[base + i]));
+  const float2 *gr = g + rhs * gstride;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < U; i += gridDim.x * blockDim.x) {
+    const float2 sv = csub(r[base + i], cmul(a, v[base + i]));
+    s[base + i] = sv;
+    if (gsv) gsv[base + i] = cmul(gr[i], sv);
+  }
 }
 
 // omega = <t, s> / ||t||^2 (bicgs.cpp:153); zero when t vanishes, which only
@@ -325,7 +335,8 @@ __global__ void __launch_bounds__(256) k_fin_true(RhsState *st, int *active, int
 }  // namespace
 
 isg_status run_matvec(isg_ctx *c, const float2 *x, const float2 *g, int64_t gs, float2 *y, int nrhs, int kind,
-                      int engine, int red, const float2 *dot_a, const int *active, cudaStream_t st) {
+                      int engine, int red, const float2 *dot_a, const int *active, cudaStream_t st,
+                      const float2 *gx) {
   const DevPlan &P = c->P;
   BatchArgs B;
   B.x = x;
@@ -336,8 +347,17 @@ isg_status run_matvec(isg_ctx *c, const float2 *x, const float2 *g, int64_t gs, 
   B.mode = (kind == OP_FWD) ? IN_G : (kind == OP_G ? IN_PLAIN : IN_CONJ);
   const bool tc = (engine == ISG_ENGINE_TENSOR) && tc_available(c);
   if (engine == ISG_ENGINE_TENSOR && !tc) return ISG_UNSUPPORTED;
+  // the tensor leaf kernels read g x directly when the caller already formed it
+  BatchArgs Bg = B;
+  const bool pre = tc && gx && kind == OP_FWD;
+  if (pre) {
+    Bg.x = gx;
+    Bg.g = nullptr;
+    Bg.gstride = 0;
+    Bg.mode = IN_PLAIN;
+  }
   if (tc) {
-    isg_status e = tc_p2m(c, B, c->mul, st);
+    isg_status e = tc_p2m(c, Bg, c->mul, st);
     if (e != ISG_OK) return e;
   } else {
     launch_p2m(P, B, c->mul, st);
@@ -353,7 +373,8 @@ isg_status run_matvec(isg_ctx *c, const float2 *x, const float2 *g, int64_t gs, 
     launch_m2l(P, i, c->mul, c->loc, nrhs, active, i >= 3, st);
   }
   NearArgs A;
-  A.in = B;
+  A.in = pre ? Bg : B;
+  A.x_epi = pre ? x : nullptr;
   A.loc = c->loc;
   A.y = y;
   A.epi = (kind == OP_FWD) ? EPI_FWD : (kind == OP_ADJ ? EPI_ADJ : (kind == OP_GCONJ ? EPI_CONJ : EPI_G));
@@ -392,17 +413,20 @@ isg_status run_bicgs(isg_ctx *c, float2 *x, const float2 *g, int64_t gs, const f
   const long host_cap = (long)(o->maxit + 2) * (o->max_restarts + 1) + 8;
   long host_iters = 0;
   // `check` iterations of every active RHS (bicgs.cpp:120-177); inactive ones return at once
+  // forward solves on the tensor engine: the updates also write g p and g s,
+  // which the leaf kernels then read instead of forming them
+  float2 *gx = (kind == OP_FWD && engine == ISG_ENGINE_TENSOR && tc_available(c)) ? c->vgx : nullptr;
   auto block = [&]() -> isg_status {
     for (int k = 0; k < check; k++) {
       count_launch();
-      k_update_p<<<vgrid, 256, 0, st>>>(c->state, c->active, c->vr, c->vp, c->vv, U);
-      isg_status be = run_matvec(c, c->vp, g, gs, c->vv, R, kind, engine, RED_DOT, c->vrt, c->active, st);
+      k_update_p<<<vgrid, 256, 0, st>>>(c->state, c->active, c->vr, c->vp, c->vv, U, g, gs, gx);
+      isg_status be = run_matvec(c, c->vp, g, gs, c->vv, R, kind, engine, RED_DOT, c->vrt, c->active, st, gx);
       if (be != ISG_OK) return be;
       count_launch();
       k_fin_alpha<<<R, 256, 0, st>>>(c->state, c->active, c->part, nbn);
       count_launch();
-      k_update_s<<<vgrid, 256, 0, st>>>(c->state, c->active, c->vr, c->vv, c->vs, U);
-      be = run_matvec(c, c->vs, g, gs, c->vt, R, kind, engine, RED_TS, nullptr, c->active, st);
+      k_update_s<<<vgrid, 256, 0, st>>>(c->state, c->active, c->vr, c->vv, c->vs, U, g, gs, gx);
+      be = run_matvec(c, c->vs, g, gs, c->vt, R, kind, engine, RED_TS, nullptr, c->active, st, gx);
       if (be != ISG_OK) return be;
       count_launch();
       k_fin_omega<<<R, 256, 0, st>>>(c->state, c->active, c->part, nbn);

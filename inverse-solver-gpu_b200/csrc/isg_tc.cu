@@ -93,7 +93,8 @@ __device__ __forceinline__ void store_chunk(char *smem, int off, const float2 *v
 }
 
 struct TcNearArgs {
-  const float2 *x, *g;
+  const float2 *x, *g;  // operator input (transformed by mode)
+  const float2 *xe;     // x of the `x - ...` epilogue
   int64_t gstride;
   int mode;
   const int *active;
@@ -343,7 +344,7 @@ __global__ void __launch_bounds__(256, 1) k_tc_near(TcNearArgs A) {
     for (int ch = 0; ch < 4; ch++)
 #pragma unroll
       for (int pp = 0; pp < 4; pp++)
-        xpre[ch][pp] = (need_x && in_grid) ? *(const float4 *)(A.x + leafbase + 32 * hh + 8 * ch + 2 * pp)
+        xpre[ch][pp] = (need_x && in_grid) ? *(const float4 *)(A.xe + leafbase + 32 * hh + 8 * ch + 2 * pp)
                                            : make_float4(0.f, 0.f, 0.f, 0.f);
     if (u == 0) {
       ok = mbar_wait(done, 1, A.err, kErrNearDone);
@@ -710,11 +711,13 @@ static bool aligned16(const void *p) { return ((uintptr_t)p & 15) == 0; }
 isg_status tc_near(isg_ctx *c, const NearArgs &N, cudaStream_t st) {
   const DevPlan &P = c->P;
   const TcPlan &T = *c->tc;
-  if (!aligned16(N.in.x) || (N.in.g && !aligned16(N.in.g)) || !aligned16(N.y) || (N.dot_a && !aligned16(N.dot_a)) ||
+  if (!aligned16(N.in.x) || (N.x_epi && !aligned16(N.x_epi)) || (N.in.g && !aligned16(N.in.g)) || !aligned16(N.y) ||
+      (N.dot_a && !aligned16(N.dot_a)) ||
       (N.in.gstride % 2) || N.epi == EPI_L2P_ONLY)
     return ISG_UNSUPPORTED;
   TcNearArgs A;
   A.x = N.in.x;
+  A.xe = N.x_epi ? N.x_epi : N.in.x;
   A.g = N.in.g;
   A.gstride = N.in.gstride;
   A.mode = N.in.mode;
