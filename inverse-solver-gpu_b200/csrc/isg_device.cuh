@@ -83,6 +83,28 @@ __device__ __forceinline__ void cfma(float2 &acc, float2 a, float2 b) {
   acc.y = fmaf(a.x, b.y, acc.y);
   acc.y = fmaf(a.y, b.x, acc.y);
 }
+// Packed FP32 pairs (fma/mul .f32x2, sm_100): one instruction does both halves.
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 pk2(float a, float b) {
+  f32x2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ float2 upk2(f32x2 r) {
+  float2 a;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(r));
+  return a;
+}
+__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
+  f32x2 d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b) {
+  f32x2 d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
 // acc += w * b (real weight)
 __device__ __forceinline__ void rfma(float2 &acc, float w, float2 b) {
   acc.x = fmaf(w, b.x, acc.x);

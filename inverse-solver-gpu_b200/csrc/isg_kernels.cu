@@ -212,14 +212,16 @@ struct TileArgs {
 };
 
 // Shared-memory carve-up of one tiled block (float2 units, 16-byte aligned parts).
+// With dup, the weights are stored as (w, w) pairs and each shift phase s as
+// (s.x, s.x, -s.y, s.y), the operands of packed FP32 pair arithmetic.
 struct TileSmem {
   size_t win, w, sh, src, dst, total;
-  __host__ __device__ TileSmem(int wmax, int ld, int out, int nsrc, int ndst, size_t out_tile) {
+  __host__ __device__ TileSmem(int wmax, int ld, int out, int nsrc, int ndst, size_t out_tile, bool dup = false) {
     auto up2 = [](size_t x) { return (x + 1) & ~(size_t)1; };
     win = 0;
     w = up2(((size_t)wmax * ld > out_tile ? (size_t)wmax * ld : out_tile));
-    sh = w + up2((size_t)wmax * out / 2);
-    src = sh + (size_t)wmax * 4;
+    sh = w + up2((size_t)wmax * out / (dup ? 1 : 2));
+    src = sh + (size_t)wmax * (dup ? 8 : 4);
     dst = src + nsrc;
     total = dst + ndst;
   }
@@ -245,23 +247,27 @@ __global__ void __launch_bounds__(128) k_l2l_tile(TileArgs A) {
   extern __shared__ float2 sm[];
   const int cols = A.cols, TO = A.tb.out, tile = blockIdx.y, c0 = blockIdx.x * cols;
   const int a0 = A.tb.a0[tile], wl = A.tb.wl[tile], ld = cols + 1;
-  const TileSmem L(A.tb.wmax, ld, TO, cols, 4 * cols, (size_t)4 * TO * ld);
+  const TileSmem L(A.tb.wmax, ld, TO, cols, 4 * cols, (size_t)4 * TO * ld, true);
   const float2 **sp = (const float2 **)(sm + L.src);
   float2 **dp = (float2 **)(sm + L.dst);
-  float4 *sw = (float4 *)(sm + L.w);
-  float4 *ss = (float4 *)(sm + L.sh);
+  float4 *sw = (float4 *)(sm + L.w);   // [wl][TO / 2]: (w, w, w', w') pairs
+  float4 *ss = (float4 *)(sm + L.sh);  // [wl][4]: (s.x, s.x, -s.y, s.y) per child
   for (int t = threadIdx.x; t < 4 * cols; t += blockDim.x) {
     if (t < cols) sp[t] = ring_ptr(A, A.src, A.off_in, c0 + t, -1, A.n_p, A.ns_in);
     dp[t] = (float2 *)ring_ptr(A, A.dst, A.off_out, c0 + (t >> 2), t & 3, 2 * A.n_p, A.ns_out);
   }
   {
     const float4 *wt = (const float4 *)(A.tb.w + (size_t)tile * A.tb.wmax * TO);
-    for (int e = threadIdx.x; e < wl * TO / 4; e += blockDim.x) cp_async16(sw + e, wt + e);
-    const float4 *sh = (const float4 *)A.shT;
-    for (int e = threadIdx.x; e < 2 * wl; e += blockDim.x) {
-      int j = a0 + (e >> 1);
+    for (int e = threadIdx.x; e < wl * TO / 4; e += blockDim.x) {
+      const float4 w = __ldg(wt + e);
+      sw[2 * e] = make_float4(w.x, w.x, w.y, w.y);
+      sw[2 * e + 1] = make_float4(w.z, w.z, w.w, w.w);
+    }
+    for (int e = threadIdx.x; e < 4 * wl; e += blockDim.x) {
+      int j = a0 + (e >> 2);
       if (j >= A.ns_in) j -= A.ns_in;
-      cp_async16(ss + e, sh + 2 * j + (e & 1));
+      const float2 v = __ldg(A.shT + 4 * j + (e & 3));
+      ss[e] = make_float4(v.x, v.x, -v.y, v.y);
     }
   }
   __syncthreads();
@@ -277,26 +283,38 @@ __global__ void __launch_bounds__(128) k_l2l_tile(TileArgs A) {
   cp_async_wait_all();
   __syncthreads();
   const int col = threadIdx.x % cols, sub = threadIdx.x / cols;
-  float2 acc[kTileOut][4] = {};
-  const int wstep = TO / 4;
+  f32x2 acc[kTileOut][4];
+#pragma unroll
+  for (int i = 0; i < kTileOut; i++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) acc[i][q] = 0ull;
+  const int wstep = TO / 2;
 #pragma unroll 2
   for (int jj = 0; jj < wl; jj++) {
     const float2 z = sm[jj * ld + col];
-    const float4 s01 = ss[2 * jj], s23 = ss[2 * jj + 1];
-    const float2 v[4] = {cmul(make_float2(s01.x, s01.y), z), cmul(make_float2(s01.z, s01.w), z),
-                         cmul(make_float2(s23.x, s23.y), z), cmul(make_float2(s23.z, s23.w), z)};
-    const float4 w0 = sw[jj * wstep + 2 * sub], w1 = sw[jj * wstep + 2 * sub + 1];
-    const float wv[kTileOut] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+    const f32x2 zz = pk2(z.x, z.y), zs = pk2(z.y, z.x);
+    f32x2 v[4];
 #pragma unroll
-    for (int i = 0; i < kTileOut; i++)
+    for (int q = 0; q < 4; q++) {  // shl[q] z as packed pairs
+      const float4 sq = ss[4 * jj + q];
+      v[q] = fma2(pk2(sq.z, sq.w), zs, mul2(pk2(sq.x, sq.y), zz));
+    }
 #pragma unroll
-      for (int q = 0; q < 4; q++) rfma(acc[i][q], wv[i], v[q]);
+    for (int i2 = 0; i2 < kTileOut / 2; i2++) {
+      const float4 w = sw[jj * wstep + sub * (kTileOut / 2) + i2];
+      const f32x2 wa = pk2(w.x, w.y), wb = pk2(w.z, w.w);
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        acc[2 * i2][q] = fma2(wa, v[q], acc[2 * i2][q]);
+        acc[2 * i2 + 1][q] = fma2(wb, v[q], acc[2 * i2 + 1][q]);
+      }
+    }
   }
   __syncthreads();
 #pragma unroll
   for (int q = 0; q < 4; q++)
 #pragma unroll
-    for (int i = 0; i < kTileOut; i++) sm[(q * TO + sub * kTileOut + i) * ld + col] = acc[i][q];
+    for (int i = 0; i < kTileOut; i++) sm[(q * TO + sub * kTileOut + i) * ld + col] = upk2(acc[i][q]);
   __syncthreads();
   for (int e = threadIdx.x; e < cols * 4 * TO; e += blockDim.x) {
     const int i = e % TO, cq = e / TO, km = tile * TO + i;
@@ -614,7 +632,7 @@ void launch_m2l(const DevPlan &P, int lvl, const float2 *mul, float2 *loc, int n
 void launch_l2l(const DevPlan &P, int lvl, float2 *loc, int nrhs, const int *active, cudaStream_t st) {
   const DevLevel &c = P.lv[lvl], &p = P.lv[lvl - 1];
   const TileArgs A = tile_args(loc, loc, P.mp, p.off, c.off, p.n, p.ns, c.ns, nrhs, c.at, p.shlT, 64, active);
-  const TileSmem L(c.at.wmax, A.cols + 1, c.at.out, A.cols, 4 * A.cols, (size_t)4 * c.at.out * (A.cols + 1));
+  const TileSmem L(c.at.wmax, A.cols + 1, c.at.out, A.cols, 4 * A.cols, (size_t)4 * c.at.out * (A.cols + 1), true);
   const size_t smem = L.total * sizeof(float2);
   count_launch();
   k_l2l_tile<<<dim3((A.ncols + A.cols - 1) / A.cols, c.at.tiles), A.cols * (c.at.out / kTileOut), smem, st>>>(A);
