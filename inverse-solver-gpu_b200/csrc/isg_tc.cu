@@ -110,6 +110,7 @@ struct TcNearArgs {
   double *part;
   int nleaf, U, tiles_x, tiles;
   int loc_vec;  // leaf locals can be copied in 16-byte chunks (ns % 4 == 0, aligned)
+  int pair;     // tiles per CTA: kPair, or 1 when the launch is too small to fill the GPU
   int *err;
 };
 
@@ -127,9 +128,9 @@ __global__ void __launch_bounds__(256, 1) k_tc_near(TcNearArgs A) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int pair = blockIdx.x;
   const int pty = pair / A.tiles_x, ptx = pair % A.tiles_x;
-  const int ty0 = pty * kPair * kTY, tx0 = ptx * kTX;
+  const int ty0 = pty * A.pair * kTY, tx0 = ptx * kTX;
   const int tiles_y = (A.nleaf + kTY - 1) / kTY;
-  const int ntile = min(kPair, tiles_y - pty * kPair);
+  const int ntile = min(A.pair, tiles_y - pty * A.pair);
   const size_t rbase = (size_t)rhs * A.U;
   const float2 *gr = A.g ? A.g + rhs * A.gstride : nullptr;
   const int nstages = kNearStages + A.nl2p;
@@ -152,8 +153,9 @@ __global__ void __launch_bounds__(256, 1) k_tc_near(TcNearArgs A) {
   // FP16 halves will go (first two pixels of a 4-pixel chunk in the hi slot,
   // last two in the lo slot); the loaders then form g x and its max in place,
   // and convert to hi/lo once the pair's scale is known ----
-  constexpr int kItems = kHR * kHC * 16;  // (halo row, 4-pixel chunk, halo column): consecutive
-                                          // items are consecutive 16-byte slots, free of bank conflicts
+  // (halo row, 4-pixel chunk, halo column): consecutive items are consecutive
+  // 16-byte slots, free of bank conflicts
+  const int kItems = (A.pair * kTY + 2) * kHC * 16;
   for (int it = threadIdx.x; it < kItems; it += blockDim.x) {
     const int hc = it % kHC, c = (it / kHC) & 15, hr = it / (kHC * 16);
     const int ly = ty0 - 1 + hr, lx = tx0 - 1 + hc;
@@ -420,7 +422,7 @@ __global__ void __launch_bounds__(256, 1) k_tc_near(TcNearArgs A) {
         s1v += dscr[w2 * 3 + 1];
         s2v += dscr[w2 * 3 + 2];
       }
-      const int tile = (pty * kPair + u) * A.tiles_x + ptx;
+      const int tile = (pty * A.pair + u) * A.tiles_x + ptx;
       double *p = A.part + ((size_t)rhs * A.tiles + tile) * 4;
       p[0] = s0;
       p[1] = s1v;
@@ -434,10 +436,18 @@ __global__ void __launch_bounds__(256, 1) k_tc_near(TcNearArgs A) {
   if (warp == 0) tmem_dealloc(tmem, 512);
 }
 
-// ---- P2M: 128 consecutive leaves of one RHS per CTA, N = 2 ns padded to 16 ----
+// ---- P2M: persistent CTAs over (RHS, 128-leaf tile) items, N = 2 ns padded to 16 ----
+// The coefficient matrix is loaded once per CTA; each item's input is loaded
+// into registers while the previous item's outputs are written, converted to
+// FP16 hi/lo, multiplied, and its multipoles go back through shared memory so
+// that the 128 consecutive leaf rings are written as one contiguous block.
 constexpr int kP2mA = 16 * 2048;  // one FP16 split of the [128 x 128] operand
 struct P2mSmem {
   static constexpr int hi = 0, lo = kP2mA, b = 2 * kP2mA;
+  // then: B (4 stages), output tile [128][ns + 1] float2, barriers
+  __host__ __device__ static size_t out(int stage_bytes) { return (size_t)b + 4 * (size_t)stage_bytes; }
+  __host__ __device__ static size_t bars(int stage_bytes, int ns) { return (out(stage_bytes) + (size_t)128 * (ns + 1) * 8 + 15) & ~(size_t)15; }
+  __host__ __device__ static size_t total(int stage_bytes, int ns) { return bars(stage_bytes, ns) + 64; }
 };
 
 struct TcP2mArgs {
@@ -450,23 +460,18 @@ struct TcP2mArgs {
   float inv_c;
   float2 *mul_leaf;
   size_t mp;
-  int ns, nleaves, U;
+  int ns, nleaves, U, tiles, nitems;
   int *err;
 };
 
 __global__ void __launch_bounds__(256, 1) k_tc_p2m(TcP2mArgs A) {
   extern __shared__ __align__(1024) char sm[];
-  const int rhs = blockIdx.y;
-  if (A.active && !A.active[rhs]) return;
-  const int bbytes = 4 * A.stage_bytes;
-  uint64_t *bar = (uint64_t *)(sm + P2mSmem::b + bbytes);
+  float2 *osm = (float2 *)(sm + P2mSmem::out(A.stage_bytes));
+  uint64_t *bar = (uint64_t *)(sm + P2mSmem::bars(A.stage_bytes, A.ns));
   uint64_t *done = bar + 1;
   uint32_t *tslot = (uint32_t *)(bar + 2);
-  float *fscr = (float *)(bar + 3);
+  float *fscr = (float *)(bar + 3);  // [8]
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int leaf0 = blockIdx.x * 128;
-  const size_t rbase = (size_t)rhs * A.U;
-  const float2 *gr = A.g ? A.g + rhs * A.gstride : nullptr;
   if (threadIdx.x == 0) {
     mbar_init(bar, 1);
     mbar_init(done, 1);
@@ -477,98 +482,132 @@ __global__ void __launch_bounds__(256, 1) k_tc_p2m(TcP2mArgs A) {
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tslot;
+  const int bbytes = 4 * A.stage_bytes;
   if (threadIdx.x == 0) {
     mbar_expect_tx(bar, bbytes);
     for (int c = 0; c < 4; c++)
       bulk_g2s(sm + P2mSmem::b + c * A.stage_bytes, A.B + (size_t)c * A.stage_bytes, A.stage_bytes, bar);
   }
-  // operand: 128 leaves x 16 chunks of 4 pixels
+  auto active_item = [&](int w) {
+    while (w < A.nitems && A.active && !A.active[w / A.tiles]) w += gridDim.x;
+    return w;
+  };
+  // one item's input: 128 leaves x 16 chunks of 4 pixels, 8 chunks per thread;
+  // chunk r of thread t is (row group, chunk, row in group) = it >> 7, (it >> 3) & 15, it & 7
   constexpr int kPer = 128 * 16 / 256;
   float2 v[kPer][4];
-  float mx = 0.f;
+  auto load = [&](int w, float &mx) {
+    const int rhs = w / A.tiles, leaf0 = (w % A.tiles) * 128;
+    const size_t rbase = (size_t)rhs * A.U;
+    const float2 *gr = A.g ? A.g + rhs * A.gstride : nullptr;
+    mx = 0.f;
 #pragma unroll
-  for (int r = 0; r < kPer; r++) {
-    const int it = threadIdx.x + r * 256;
-    const int m = it >> 4, c = it & 15, leaf = leaf0 + m;
+    for (int r = 0; r < kPer; r++) {
+      const int it = threadIdx.x + r * 256;
+      const int m = ((it >> 7) << 3) | (it & 7), c = (it >> 3) & 15, leaf = leaf0 + m;
 #pragma unroll
-    for (int p = 0; p < 4; p++) v[r][p] = make_float2(0.f, 0.f);
-    if (leaf < A.nleaves) {
-      const size_t i = (size_t)leaf * kBB + 4 * c;
-      const float4 a0 = *(const float4 *)(A.x + rbase + i), a1 = *(const float4 *)(A.x + rbase + i + 2);
-      float4 g0 = make_float4(0.f, 0.f, 0.f, 0.f), g1 = g0;
-      if (A.mode == IN_G) {
-        g0 = *(const float4 *)(gr + i);
-        g1 = *(const float4 *)(gr + i + 2);
-      }
-      v[r][0] = transform(make_float2(a0.x, a0.y), make_float2(g0.x, g0.y), A.mode);
-      v[r][1] = transform(make_float2(a0.z, a0.w), make_float2(g0.z, g0.w), A.mode);
-      v[r][2] = transform(make_float2(a1.x, a1.y), make_float2(g1.x, g1.y), A.mode);
-      v[r][3] = transform(make_float2(a1.z, a1.w), make_float2(g1.z, g1.w), A.mode);
-#pragma unroll
-      for (int p = 0; p < 4; p++) mx = fmaxf(mx, cabs1(v[r][p]));
-    }
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-  if (lane == 0) fscr[warp] = mx;
-  __syncthreads();
-  float m2 = 0.f;
-  for (int q = 0; q < 8; q++) m2 = fmaxf(m2, fscr[q]);
-  const float s = pow2_scale(m2);
-#pragma unroll
-  for (int r = 0; r < kPer; r++) {
-    const int it = threadIdx.x + r * 256;
-    const int m = it >> 4, c = it & 15;
-    __align__(16) __half h[8], l[8];
-#pragma unroll
-    for (int p = 0; p < 4; p++) {
-      split_f16(v[r][p].x * s, h[2 * p], l[2 * p]);
-      split_f16(v[r][p].y * s, h[2 * p + 1], l[2 * p + 1]);
-    }
-    const int off = (m >> 3) * 2048 + c * 128 + (m & 7) * 16;
-    *(uint4 *)(sm + P2mSmem::hi + off) = *(uint4 *)h;
-    *(uint4 *)(sm + P2mSmem::lo + off) = *(uint4 *)l;
-  }
-  fence_proxy_async();
-  __syncthreads();
-  const uint32_t sbase = smem_u32(sm);
-  if (threadIdx.x == 0) {
-    tc_fence_after();
-    if (mbar_wait(bar, 0, A.err, kErrP2m)) {
-      const uint32_t idesc = idesc_f16_f32(128, A.npad);
-      for (int c = 0; c < 4; c++)
-#pragma unroll
-        for (int ks = 0; ks < 2; ks++) {
-          const uint32_t aoff = (uint32_t)(c * 4 + ks * 2) * 128;
-          const uint64_t ahi = smem_desc(sbase + P2mSmem::hi + aoff, 128, 2048);
-          const uint64_t alo = smem_desc(sbase + P2mSmem::lo + aoff, 128, 2048);
-          const uint32_t bst = sbase + P2mSmem::b + c * A.stage_bytes + ks * 256;
-          const uint64_t bhi = smem_desc(bst, 128, 512);
-          const uint64_t blo = smem_desc(bst + A.stage_bytes / 2, 128, 512);
-          mma_f16(tmem, ahi, bhi, idesc, (c | ks) ? 1 : 0);
-          mma_f16(tmem, ahi, blo, idesc, 1);
-          mma_f16(tmem, alo, bhi, idesc, 1);
+      for (int p = 0; p < 4; p++) v[r][p] = make_float2(0.f, 0.f);
+      if (leaf < A.nleaves) {
+        const size_t i = (size_t)leaf * kBB + 4 * c;
+        const float4 a0 = *(const float4 *)(A.x + rbase + i), a1 = *(const float4 *)(A.x + rbase + i + 2);
+        float4 g0 = make_float4(0.f, 0.f, 0.f, 0.f), g1 = g0;
+        if (A.mode == IN_G) {
+          g0 = *(const float4 *)(gr + i);
+          g1 = *(const float4 *)(gr + i + 2);
         }
-    }
-    mma_commit(done);
-  }
-  const bool ok = mbar_wait(done, 0, A.err, kErrP2m);
-  __syncthreads();
-  tc_fence_after();
-  const float inv = A.inv_c / s;
-  const int q = warp & 3, hh = warp >> 2;
-  const int leaf = leaf0 + 32 * q + lane;
-  const int nchunks = A.npad / 16, c0 = hh ? (nchunks + 1) / 2 : 0, c1 = hh ? nchunks : (nchunks + 1) / 2;
-  float2 *out = A.mul_leaf + (size_t)rhs * A.mp + (size_t)leaf * A.ns;
-  for (int ch = c0; ch < c1; ch++) {
-    float d[16];
-    tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + 16 * ch, d);
-    if (!ok || leaf >= A.nleaves) continue;
+        v[r][0] = transform(make_float2(a0.x, a0.y), make_float2(g0.x, g0.y), A.mode);
+        v[r][1] = transform(make_float2(a0.z, a0.w), make_float2(g0.z, g0.w), A.mode);
+        v[r][2] = transform(make_float2(a1.x, a1.y), make_float2(g1.x, g1.y), A.mode);
+        v[r][3] = transform(make_float2(a1.z, a1.w), make_float2(g1.z, g1.w), A.mode);
 #pragma unroll
-    for (int p = 0; p < 8; p++) {
-      const int k = 8 * ch + p;
-      if (k < A.ns) out[k] = make_float2(d[2 * p] * inv, d[2 * p + 1] * inv);
+        for (int p = 0; p < 4; p++) mx = fmaxf(mx, cabs1(v[r][p]));
+      }
     }
+  };
+  const uint32_t sbase = smem_u32(sm);
+  const uint32_t idesc = idesc_f16_f32(128, A.npad);
+  const int nchunks = A.npad / 16;
+  const int q = warp & 3, hh = warp >> 2;
+  const int c0 = hh ? (nchunks + 1) / 2 : 0, c1 = hh ? nchunks : (nchunks + 1) / 2;
+  bool ok = mbar_wait(bar, 0, A.err, kErrP2m);  // the coefficients
+  int parity = 0;
+  int w = active_item(blockIdx.x);
+  float mx = 0.f;
+  if (w < A.nitems) load(w, mx);
+  while (w < A.nitems) {
+    // scale, convert and store this item's operand; the previous item's MMAs are done
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) fscr[warp] = mx;
+    __syncthreads();
+    float m2 = 0.f;
+    for (int k = 0; k < 8; k++) m2 = fmaxf(m2, fscr[k]);
+    const float s = pow2_scale(m2);
+#pragma unroll
+    for (int r = 0; r < kPer; r++) {
+      const int it = threadIdx.x + r * 256;
+      __align__(16) __half h[8], l[8];
+#pragma unroll
+      for (int p = 0; p < 4; p++) {
+        split_f16(v[r][p].x * s, h[2 * p], l[2 * p]);
+        split_f16(v[r][p].y * s, h[2 * p + 1], l[2 * p + 1]);
+      }
+      const int off = it * 16;  // (it >> 7) * 2048 + ((it >> 3) & 15) * 128 + (it & 7) * 16
+      *(uint4 *)(sm + P2mSmem::hi + off) = *(uint4 *)h;
+      *(uint4 *)(sm + P2mSmem::lo + off) = *(uint4 *)l;
+    }
+    fence_proxy_async();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      tc_fence_after();
+      if (ok)
+        for (int c = 0; c < 4; c++)
+#pragma unroll
+          for (int ks = 0; ks < 2; ks++) {
+            const uint32_t aoff = (uint32_t)(c * 4 + ks * 2) * 128;
+            const uint64_t ahi = smem_desc(sbase + P2mSmem::hi + aoff, 128, 2048);
+            const uint64_t alo = smem_desc(sbase + P2mSmem::lo + aoff, 128, 2048);
+            const uint32_t bst = sbase + P2mSmem::b + c * A.stage_bytes + ks * 256;
+            const uint64_t bhi = smem_desc(bst, 128, 512);
+            const uint64_t blo = smem_desc(bst + A.stage_bytes / 2, 128, 512);
+            mma_f16(tmem, ahi, bhi, idesc, (c | ks) ? 1 : 0);
+            mma_f16(tmem, ahi, blo, idesc, 1);
+            mma_f16(tmem, alo, bhi, idesc, 1);
+          }
+      mma_commit(done);
+    }
+    // the next item's input, in flight while this one is multiplied and written
+    const int rhs = w / A.tiles, leaf0 = (w % A.tiles) * 128;
+    const int nxt = active_item(w + gridDim.x);
+    float mxn = 0.f;
+    if (nxt < A.nitems) load(nxt, mxn);
+    ok = mbar_wait(done, parity, A.err, kErrP2m) && ok;
+    parity ^= 1;
+    tc_fence_after();
+    const float inv = A.inv_c / s;
+    const int m = 32 * q + lane;
+    for (int ch = c0; ch < c1; ch++) {
+      float d[16];
+      tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + 16 * ch, d);
+#pragma unroll
+      for (int p = 0; p < 8; p++) {
+        const int k = 8 * ch + p;
+        if (k < A.ns) osm[m * (A.ns + 1) + k] = make_float2(d[2 * p] * inv, d[2 * p + 1] * inv);
+      }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (ok) {
+      const int nl = min(128, A.nleaves - leaf0);
+      float2 *out = A.mul_leaf + (size_t)rhs * A.mp + (size_t)leaf0 * A.ns;
+      for (int e = threadIdx.x; e < nl * A.ns; e += blockDim.x) {
+        const int mm = e / A.ns, k = e - mm * A.ns;
+        out[e] = osm[mm * (A.ns + 1) + k];
+      }
+    }
+    __syncthreads();  // the output tile and fscr are reused by the next item
+    w = nxt;
+    mx = mxn;
   }
   tc_fence_before();
   __syncthreads();
@@ -679,7 +718,7 @@ isg_status tc_setup(isg_ctx *c) {
   cudaMemset(P.err, 0, sizeof(int));
   cudaFuncSetAttribute(k_tc_near, cudaFuncAttributeMaxDynamicSharedMemorySize, NearSmem::total);
   cudaFuncSetAttribute(k_tc_p2m, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       P2mSmem::b + 4 * P.p2m_stage + 64);
+                       (int)P2mSmem::total(P.p2m_stage, ns));
   if ((e = cuda_check(c, cudaGetLastError(), "tc setup")) != ISG_OK) return e;
   P.ok = true;
   return ISG_OK;
@@ -742,7 +781,10 @@ isg_status tc_near(isg_ctx *c, const NearArgs &N, cudaStream_t st) {
   A.loc_vec = (P.ns_leaf % 4 == 0) && aligned16(A.loc_leaf) && (P.mp % 2 == 0);
   A.err = T.err;
   count_launch();
-  const int pairs = A.tiles_x * ((tiles_y + kPair - 1) / kPair);
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->opts.device);
+  A.pair = (A.tiles * N.in.nrhs >= 2 * kPair * sms) ? kPair : 1;
+  const int pairs = A.tiles_x * ((tiles_y + A.pair - 1) / A.pair);
   k_tc_near<<<dim3(pairs, N.in.nrhs), 256, NearSmem::total, st>>>(A);
   return cuda_check(c, cudaGetLastError(), "tc near launch");
 }
@@ -766,9 +808,13 @@ isg_status tc_p2m(isg_ctx *c, const BatchArgs &B, float2 *mul, cudaStream_t st) 
   A.ns = P.ns_leaf;
   A.nleaves = P.nleaf * P.nleaf;
   A.U = P.U;
+  A.tiles = (A.nleaves + 127) / 128;
+  A.nitems = A.tiles * B.nrhs;
   A.err = T.err;
   count_launch();
-  k_tc_p2m<<<dim3((A.nleaves + 127) / 128, B.nrhs), 256, P2mSmem::b + 4 * T.p2m_stage + 64, st>>>(A);
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->opts.device);
+  k_tc_p2m<<<std::min(A.nitems, sms), 256, P2mSmem::total(T.p2m_stage, A.ns), st>>>(A);
   return cuda_check(c, cudaGetLastError(), "tc p2m launch");
 }
 
