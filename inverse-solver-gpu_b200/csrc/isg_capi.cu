@@ -345,7 +345,7 @@ isg_status isg_setup_gpu(isg_ctx *c) {
   if ((e = dalloc(c, &c->mul, R * P.mp)) || (e = dalloc(c, &c->loc, R * P.mp)) || (e = dalloc(c, &c->wx, R * U)) ||
       (e = dalloc(c, &c->wy, R * U)) || (e = dalloc(c, &c->wg, R * U)) || (e = dalloc(c, &c->vr, R * U)) ||
       (e = dalloc(c, &c->vrt, R * U)) || (e = dalloc(c, &c->vp, R * U)) || (e = dalloc(c, &c->vv, R * U)) ||
-      (e = dalloc(c, &c->vs, R * U)) || (e = dalloc(c, &c->vt, R * U)) || (e = dalloc(c, &c->vgx, R * U)) ||
+      (e = dalloc(c, &c->vs, R * U)) || (e = dalloc(c, &c->vt, R * U)) || (e = dalloc(c, &c->vgx, R * U)) || (e = dalloc(c, &c->levmax, R * kMaxLevels)) ||
       (e = dalloc(c, &c->part, R * (size_t)c->part_blocks * 4 + 64)) || (e = dalloc(c, &c->state, R)) ||
       (e = dalloc(c, &c->active, R)) || (e = dalloc(c, &c->count, 1)))
     return e;
@@ -555,7 +555,12 @@ isg_status isg_time_stages(isg_ctx *c, int nrhs, int engine, int reps, double *m
   const bool tc = engine == ISG_ENGINE_TENSOR;
   for (int r = -1; r < reps; r++) {
     cudaEventRecord(ev[0], st);
-    if (tc) tc_p2m(c, B, c->mul, st); else launch_p2m(P, B, c->mul, st);
+    if (tc) {
+      cudaMemsetAsync(c->levmax, 0, (size_t)nrhs * kMaxLevels * sizeof(unsigned), st);
+      tc_p2m(c, B, c->mul, st);
+    } else {
+      launch_p2m(P, B, c->mul, st);
+    }
     cudaEventRecord(ev[1], st);
     isg_status be = ISG_OK;
     for (int i = P.L - 2; i >= 2; i--)

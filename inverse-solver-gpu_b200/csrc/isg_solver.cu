@@ -357,6 +357,7 @@ isg_status run_matvec(isg_ctx *c, const float2 *x, const float2 *g, int64_t gs, 
     Bg.mode = IN_PLAIN;
   }
   if (tc) {
+    cudaMemsetAsync(c->levmax, 0, (size_t)nrhs * kMaxLevels * sizeof(unsigned), st);
     isg_status e = tc_p2m(c, Bg, c->mul, st);
     if (e != ISG_OK) return e;
   } else {

@@ -462,6 +462,8 @@ struct TcP2mArgs {
   size_t mp;
   int ns, nleaves, U, tiles, nitems;
   int *err;
+  unsigned *levmax;  // [R][kMaxLevels]: this level's max |re|, |im| per RHS (FP32 bits)
+  int lvl;
 };
 
 __global__ void __launch_bounds__(256, 1) k_tc_p2m(TcP2mArgs A) {
@@ -586,15 +588,23 @@ __global__ void __launch_bounds__(256, 1) k_tc_p2m(TcP2mArgs A) {
     tc_fence_after();
     const float inv = A.inv_c / s;
     const int m = 32 * q + lane;
+    float omx = 0.f;
     for (int ch = c0; ch < c1; ch++) {
       float d[16];
       tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + 16 * ch, d);
 #pragma unroll
       for (int p = 0; p < 8; p++) {
         const int k = 8 * ch + p;
-        if (k < A.ns) osm[m * (A.ns + 1) + k] = make_float2(d[2 * p] * inv, d[2 * p + 1] * inv);
+        if (k < A.ns) {
+          const float2 o = make_float2(d[2 * p] * inv, d[2 * p + 1] * inv);
+          osm[m * (A.ns + 1) + k] = o;
+          if (leaf0 + m < A.nleaves) omx = fmaxf(omx, fmaxf(fabsf(o.x), fabsf(o.y)));
+        }
       }
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) omx = fmaxf(omx, __shfl_xor_sync(0xffffffffu, omx, o));
+    if (lane == 0 && ok) atomicMax(&A.levmax[rhs * kMaxLevels + A.lvl], __float_as_uint(omx));
     tc_fence_before();
     __syncthreads();
     if (ok) {
@@ -811,6 +821,8 @@ isg_status tc_p2m(isg_ctx *c, const BatchArgs &B, float2 *mul, cudaStream_t st) 
   A.tiles = (A.nleaves + 127) / 128;
   A.nitems = A.tiles * B.nrhs;
   A.err = T.err;
+  A.levmax = c->levmax;
+  A.lvl = P.L - 1;
   count_launch();
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->opts.device);

@@ -31,7 +31,7 @@ constexpr int kParents = 32;
 constexpr int kKC = 64;           // K chunk
 constexpr int kAHalf = 128 * kKC * 2;    // 16 KB: one FP16 split of an A chunk
 constexpr int kBHalf = kCols * kKC * 2;  // 32 KB
-constexpr int kSmem = 2 * kAHalf + 2 * kBHalf + 128;
+constexpr int kSmem = 2 * kAHalf + 2 * kBHalf + 256;  // + barriers, TMEM slot, scratch, per-parent maxima
 constexpr int kErrBand = 121;
 
 struct BandArgs {
@@ -46,6 +46,8 @@ struct BandArgs {
   int nparents, ncols;  // ncols = parents x RHS
   const int *active;
   int *err;
+  unsigned *levmax;        // [R][kMaxLevels] max |re|, |im| per RHS and level (FP32 bits)
+  int lvl_in, lvl_out;
 };
 
 // One ring of the CTA: its base pointer, or none.
@@ -95,25 +97,22 @@ __global__ void __launch_bounds__(256, 2) k_tc_band(BandArgs A) {
   uint64_t *mbar = abar + 1;
   uint32_t *tslot = (uint32_t *)(abar + 2);
   float *fscr = (float *)(abar + 3);  // [8]
+  unsigned *pmax = (unsigned *)(abar + 16);  // [kParents] output maxima (FP32 bits)
+  if (threadIdx.x < kParents) pmax[threadIdx.x] = 0u;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int mt = blockIdx.y, m0 = mt * 128;
   const int kw0 = A.kw0[mt], nch = A.nchunk[mt];
   const uint8_t *Achunks = A.A + (size_t)A.chunk0[mt] * 2 * kAHalf;
   const int kwtot = nch * kKC;
 
-  // per-CTA power-of-two scale of the ring values in the window
+  // power-of-two scale from the input level's maximum over the CTA's RHS
+  // (written by the kernel that produced that level)
   float mx = 0.f;
-  const int g8n = kwtot / 8;
-#pragma unroll 2
-  for (int it = threadIdx.x; it < 128 * g8n; it += blockDim.x) {
-    const RingRef rr = ring_ref(A, it / g8n);
-    float2 v[8];
-    ring_load8(A, rr, (it % g8n) * 8, kw0, v);
-#pragma unroll
-    for (int k = 0; k < 8; k++) mx = fmaxf(mx, fmaxf(fabsf(v[k].x), fabsf(v[k].y)));
+  if (threadIdx.x == 0) {
+    const int g0 = blockIdx.x * kParents, g1 = min(A.ncols, g0 + kParents) - 1;
+    for (int r = g0 / A.nparents; r <= g1 / A.nparents; r++)
+      mx = fmaxf(mx, __uint_as_float(A.levmax[r * kMaxLevels + A.lvl_in]));
   }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
   if (lane == 0) fscr[warp] = mx;
   if (threadIdx.x == 0) {
     mbar_init(abar, 1);
@@ -188,24 +187,36 @@ __global__ void __launch_bounds__(256, 2) k_tc_band(BandArgs A) {
   for (int pp = 0; pp < 8; pp++) {
     float d[16];
     tmem_ld16(tmem + ((uint32_t)(32 * qd) << 16) + 128 * h + 16 * pp, d);
-    if (!row_ok) continue;
 #pragma unroll
     for (int u = 0; u < 2; u++) {
+      // the parent is the same for every lane of the warp
       const int pl = 16 * h + 2 * pp + u, gp = blockIdx.x * kParents + pl;
       if (gp >= A.ncols) continue;
       const int rhs = gp / A.nparents, P = gp % A.nparents;
       if (A.active && !A.active[rhs]) continue;
-      float2 *base = A.dst + (size_t)rhs * A.mp;
-      const float *dv = d + 8 * u;
-      float2 acc = make_float2(0.f, 0.f);
+      unsigned mbits = 0u;
+      if (row_ok) {
+        float2 *base = A.dst + (size_t)rhs * A.mp;
+        const float *dv = d + 8 * u;
+        float2 acc = make_float2(0.f, 0.f);
 #pragma unroll
-      for (int q = 0; q < 4; q++)
-        cfma(acc, __ldg(&A.shift[q * A.ns_out + km]), make_float2(dv[2 * q] * inv, dv[2 * q + 1] * inv));
-      base[(size_t)P * A.ns_out + km] = acc;
+        for (int q = 0; q < 4; q++)
+          cfma(acc, __ldg(&A.shift[q * A.ns_out + km]), make_float2(dv[2 * q] * inv, dv[2 * q + 1] * inv));
+        base[(size_t)P * A.ns_out + km] = acc;
+        mbits = __float_as_uint(fmaxf(fabsf(acc.x), fabsf(acc.y)));
+      }
+      mbits = __reduce_max_sync(0xffffffffu, mbits);
+      if (lane == 0 && mbits) atomicMax(&pmax[pl], mbits);
     }
   }
   tc_fence_before();
   __syncthreads();
+  // the parent level's maximum per RHS, read by the next coarser M2M
+  if (threadIdx.x < kParents) {
+    const int gp = blockIdx.x * kParents + threadIdx.x;
+    if (gp < A.ncols && pmax[threadIdx.x])
+      atomicMax(&A.levmax[(gp / A.nparents) * kMaxLevels + A.lvl_out], pmax[threadIdx.x]);
+  }
   if (warp == 0) tmem_dealloc(tmem, 256);
 }
 
@@ -346,7 +357,7 @@ void band_destroy(isg_ctx *c) {
   c->band = nullptr;
 }
 
-static isg_status band_launch(isg_ctx *c, const Transition &T, const float2 *src, float2 *dst, int n_p,
+static isg_status band_launch(isg_ctx *c, int lvl, const Transition &T, const float2 *src, float2 *dst, int n_p,
                               int ns_in, int ns_out, const float2 *shift, int nrhs, const int *active,
                               cudaStream_t st) {
   BandArgs A;
@@ -366,6 +377,9 @@ static isg_status band_launch(isg_ctx *c, const Transition &T, const float2 *src
   A.ncols = A.nparents * nrhs;
   A.active = active;
   A.err = c->tc_err_flag();
+  A.levmax = c->levmax;
+  A.lvl_in = lvl + 1;
+  A.lvl_out = lvl;
   count_launch();
   k_tc_band<<<dim3((A.ncols + kParents - 1) / kParents, T.mtiles), 256, kSmem, st>>>(A);
   return cuda_check(c, cudaGetLastError(), "band launch");
@@ -374,7 +388,7 @@ static isg_status band_launch(isg_ctx *c, const Transition &T, const float2 *src
 bool band_m2m(isg_ctx *c, int lvl, float2 *mul, int nrhs, const int *active, cudaStream_t st, isg_status *e) {
   if (!c->band || lvl >= kMaxLevels || !c->band->m2m[lvl].ok) return false;
   const DevLevel &p = c->P.lv[lvl], &ch = c->P.lv[lvl + 1];
-  *e = band_launch(c, c->band->m2m[lvl], mul + ch.off, mul + p.off, p.n, ch.ns, p.ns, p.shm, nrhs, active,
+  *e = band_launch(c, lvl, c->band->m2m[lvl], mul + ch.off, mul + p.off, p.n, ch.ns, p.ns, p.shm, nrhs, active,
                    st);
   return true;
 }
