@@ -87,11 +87,27 @@ isg_status upload_tile_band(isg_ctx *c, TileBand *tb, const std::vector<int> &id
     for (int k = t * out; k < std::min(ns_out, (t + 1) * out); k++)
       for (int u = 0; u < width; u++)
         w[((size_t)t * wmax + rel(t, k, u)) * out + (k - t * out)] += (float)wt[(size_t)k * stride + u];
+  // per group of kTileOut outputs, the window rows that carry any of its weights
+  const int subs = out / kTileOut;
+  std::vector<int2> span((size_t)tiles * subs);
+  for (int t = 0; t < tiles; t++)
+    for (int b = 0; b < subs; b++) {
+      int lo = wl[t], hi = 0;
+      for (int jj = 0; jj < wl[t]; jj++)
+        for (int i = b * kTileOut; i < (b + 1) * kTileOut; i++)
+          if (w[((size_t)t * wmax + jj) * out + i] != 0.f) {
+            lo = std::min(lo, jj);
+            hi = std::max(hi, jj + 1);
+          }
+      span[(size_t)t * subs + b] = make_int2(std::min(lo, hi), hi);
+    }
   tb->tiles = tiles;
   tb->wmax = wmax;
   tb->out = out;
   isg_status e;
-  if ((e = upload(c, &tb->w, w)) || (e = upload(c, &tb->a0, a0)) || (e = upload(c, &tb->wl, wl))) return e;
+  if ((e = upload(c, &tb->w, w)) || (e = upload(c, &tb->a0, a0)) || (e = upload(c, &tb->wl, wl)) ||
+      (e = upload(c, &tb->span, span)))
+    return e;
   return ISG_OK;
 }
 

@@ -21,6 +21,7 @@ constexpr int kTileOut = 8;
 struct TileBand {
   float *w = nullptr;  // [tiles][wmax][out]
   int *a0 = nullptr, *wl = nullptr;
+  int2 *span = nullptr;  // [tiles][out / kTileOut]: window rows [x, y) where a thread's kTileOut outputs have taps
   int tiles = 0, wmax = 0, out = kTileOut;
 };
 

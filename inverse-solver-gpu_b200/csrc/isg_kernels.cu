@@ -289,8 +289,9 @@ __global__ void __launch_bounds__(128) k_l2l_tile(TileArgs A) {
 #pragma unroll
     for (int q = 0; q < 4; q++) acc[i][q] = 0ull;
   const int wstep = TO / 2;
+  const int2 span = A.tb.span[tile * (TO / kTileOut) + sub];
 #pragma unroll 2
-  for (int jj = 0; jj < wl; jj++) {
+  for (int jj = span.x; jj < span.y; jj++) {
     const float2 z = sm[jj * ld + col];
     const f32x2 zz = pk2(z.x, z.y), zs = pk2(z.y, z.x);
     f32x2 v[4];
@@ -358,8 +359,9 @@ __global__ void __launch_bounds__(128) k_m2m_tile(TileArgs A) {
   const int col = threadIdx.x % cols, sub = threadIdx.x / cols;
   float2 acc[kTileOut][4] = {};
   const int wstep = TO / 4;
+  const int2 span = A.tb.span[tile * (TO / kTileOut) + sub];
 #pragma unroll 2
-  for (int jj = 0; jj < wl; jj++) {
+  for (int jj = span.x; jj < span.y; jj++) {
     float2 v[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) v[q] = sm[jj * ld + q * cols + col];
