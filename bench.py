@@ -253,6 +253,7 @@ def main():
     stream = torch.cuda.Stream(dev)
     engine = {"simt": isg.ENGINE_SIMT, "tensor": isg.ENGINE_TENSOR, "auto": isg.ENGINE_TENSOR}[args.engine]
     opts = isg.default_solve_opts(tol=TOL, maxit=300, engine=engine, check_every=2)
+    tuned = s.autotune(NTX, engine, stream=stream)  # launch shapes for this batch (untimed set-up)
 
     def step():
         return s.bicgs(x, g, b, opts=opts, stream=stream)
@@ -328,7 +329,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c64 (FP64 dots)", "data": "synthetic",
         "config": {**workload_config("simt" if engine == isg.ENGINE_SIMT else "tensor", False),
-                   "parallelism": f"tx-sharded x{world}" if world > 1 else "single GPU"},
+                   "parallelism": f"tx-sharded x{world}" if world > 1 else "single GPU", "autotuned": tuned},
         "mean_iterations": float(np.mean(iters)), "all_converged": not bad,
         "max_true_residual": max(i["true_residual"] for i in infos),
         "roofline": ({"bound": "tensor", "kernel": "k_tc_near (near field + L2P, 3xFP16 split tcgen05), 16 RHS",

@@ -241,6 +241,18 @@ isg_status isg_make_plane_waves(const isg_ctx *ctx, int ntx, int first, int coun
 isg_status isg_make_line_sources(const isg_ctx *ctx, int ntx, int first, int count, double radius, int order,
                                  double *inc);
 
+/* ---- launch-shape autotuner (no counterpart in the reference) ----
+ * Times the candidate launch shapes of the level-dependent kernels (M2L rows
+ * per thread, L2L and M2M columns per block, near-field tiles per tensor-core
+ * CTA) on the context's buffers with nrhs right-hand sides and keeps the
+ * fastest per level; later calls with at least nrhs / 4 RHS use them.  The
+ * outputs do not depend on the shapes.  Overwrites the context's multipole and
+ * local workspaces (no caller data). */
+isg_status isg_autotune(isg_ctx *ctx, int nrhs, int engine, isg_stream stream);
+/* The chosen shape: what 0 = M2L rows per thread, 1 = L2L columns, 2 = M2M
+ * columns (per level), 3 = near-field tiles per CTA; 0 = built-in choice. */
+isg_status isg_tuned(const isg_ctx *ctx, int what, int level, int *value);
+
 /* ---- learned warm start (no counterpart in the reference) ----
  * A Fourier neural operator on the pixel grid maps the contrast g and the
  * incident field b of a forward solve to an estimate of its total field; with

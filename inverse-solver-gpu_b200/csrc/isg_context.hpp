@@ -87,6 +87,9 @@ const int *order_perm(const isg_ctx *c, int order);
 isg_status tc_setup(isg_ctx *c);
 void tc_destroy(isg_ctx *c);
 bool tc_available(const isg_ctx *c);
+// Tiles per near-field CTA chosen by isg_autotune (0: built-in choice).
+void tc_set_near_pair(isg_ctx *c, int pair);
+int tc_near_pair(const isg_ctx *c);
 isg_status tc_p2m(isg_ctx *c, const BatchArgs &B, float2 *mul, cudaStream_t st);
 isg_status tc_near(isg_ctx *c, const NearArgs &A, cudaStream_t st);
 // Per-RHS partial sums written by tc_near (one per tile).

@@ -44,6 +44,10 @@ struct DevLevel {
   TileBand at;             // anterpolation into this level (L2L), tiled
   float2 *shmT = nullptr;  // [ns][4] shm transposed
   float2 *shlT = nullptr;  // [ns][4] shl transposed
+  // launch shapes picked by isg_autotune (0: the built-in choice)
+  int m2l_ty = 0;    // sibling-group rows per M2L thread
+  int l2l_cols = 0;  // columns per L2L tile block
+  int m2m_cols = 0;  // columns per M2M tile block
 };
 
 struct DevPlan {
@@ -60,6 +64,7 @@ struct DevPlan {
   int *hind = nullptr;       // [ns_0][hwidth]
   float *haw = nullptr;      // [ns_0][hwidth]
   int hwidth = 0;
+  int tuned_nrhs = 0;         // batch the tuned shapes were timed on; they apply from a quarter of it
   int *perm_tree = nullptr;   // blocked index -> tree index
   int *perm_raster = nullptr; // blocked index -> raster index
 };

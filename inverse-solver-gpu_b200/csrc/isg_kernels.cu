@@ -602,7 +602,8 @@ static TileArgs tile_args(const float2 *src, float2 *dst, size_t mp, size_t off_
 
 void launch_m2m(const DevPlan &P, int lvl, float2 *mul, int nrhs, const int *active, cudaStream_t st) {
   const DevLevel &p = P.lv[lvl], &c = P.lv[lvl + 1];
-  const TileArgs A = tile_args(mul, mul, P.mp, c.off, p.off, p.n, c.ns, p.ns, nrhs, p.mt, p.shmT, 32, active);
+  const int cap = (p.m2m_cols > 0 && 4 * nrhs >= P.tuned_nrhs) ? p.m2m_cols : 32;
+  const TileArgs A = tile_args(mul, mul, P.mp, c.off, p.off, p.n, c.ns, p.ns, nrhs, p.mt, p.shmT, cap, active);
   const TileSmem L(p.mt.wmax, 4 * A.cols + 1, p.mt.out, 4 * A.cols, A.cols, (size_t)p.mt.out * (A.cols + 1));
   const size_t smem = L.total * sizeof(float2);
   count_launch();
@@ -626,6 +627,7 @@ void launch_m2l(const DevPlan &P, int lvl, const float2 *mul, float2 *loc, int n
   // eight groups per thread when the grid stays large, fewer for small batches
   int ty = std::min(8, half);
   while (ty > 1 && (size_t)bx * ((half + ty - 1) / ty) * nrhs < 4 * 148) ty /= 2;
+  if (c.m2l_ty > 0 && 4 * nrhs >= P.tuned_nrhs) ty = std::min(c.m2l_ty, std::max(1, half));
   A.ty = ty;
   count_launch();
   k_m2l<<<dim3(bx, (half + ty - 1) / ty, nrhs), 128, 0, st>>>(A);
@@ -633,7 +635,8 @@ void launch_m2l(const DevPlan &P, int lvl, const float2 *mul, float2 *loc, int n
 
 void launch_l2l(const DevPlan &P, int lvl, float2 *loc, int nrhs, const int *active, cudaStream_t st) {
   const DevLevel &c = P.lv[lvl], &p = P.lv[lvl - 1];
-  const TileArgs A = tile_args(loc, loc, P.mp, p.off, c.off, p.n, p.ns, c.ns, nrhs, c.at, p.shlT, 64, active);
+  const int cap = (c.l2l_cols > 0 && 4 * nrhs >= P.tuned_nrhs) ? c.l2l_cols : 64;
+  const TileArgs A = tile_args(loc, loc, P.mp, p.off, c.off, p.n, p.ns, c.ns, nrhs, c.at, p.shlT, cap, active);
   const TileSmem L(c.at.wmax, A.cols + 1, c.at.out, A.cols, 4 * A.cols, (size_t)4 * c.at.out * (A.cols + 1), true);
   const size_t smem = L.total * sizeof(float2);
   count_launch();

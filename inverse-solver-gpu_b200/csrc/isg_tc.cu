@@ -661,9 +661,14 @@ struct TcPlan {
   float inv_c = 1;
   int *err = nullptr;
   bool ok = false;
+  int near_pair = 0;  // tiles per near-field CTA picked by isg_autotune (0: built-in choice)
 };
 
 bool tc_available(const isg_ctx *c) { return c->tc && c->tc->ok; }
+void tc_set_near_pair(isg_ctx *c, int pair) {
+  if (tc_available(c)) c->tc->near_pair = pair;
+}
+int tc_near_pair(const isg_ctx *c) { return tc_available(c) ? c->tc->near_pair : 0; }
 
 }  // namespace isg
 
@@ -794,6 +799,7 @@ isg_status tc_near(isg_ctx *c, const NearArgs &N, cudaStream_t st) {
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->opts.device);
   A.pair = (A.tiles * N.in.nrhs >= 2 * kPair * sms) ? kPair : 1;
+  if (T.near_pair > 0 && 4 * N.in.nrhs >= P.tuned_nrhs) A.pair = std::min(T.near_pair, kPair);
   const int pairs = A.tiles_x * ((tiles_y + A.pair - 1) / A.pair);
   k_tc_near<<<dim3(pairs, N.in.nrhs), 256, NearSmem::total, st>>>(A);
   return cuda_check(c, cudaGetLastError(), "tc near launch");

@@ -112,6 +112,8 @@ SIGNATURES = {
     "isg_make_phantom": (_I, [_P, ctypes.POINTER(Phantom), _P]),
     "isg_make_plane_waves": (_I, [_P, _I, _I, _I, _I, _P]),
     "isg_make_line_sources": (_I, [_P, _I, _I, _I, _D, _I, _P]),
+    "isg_autotune": (_I, [_P, _I, _I, _P]),
+    "isg_tuned": (_I, [_P, _I, _I, ctypes.POINTER(_I)]),
     "isg_default_fno_opts": (None, [ctypes.POINTER(FnoOpts)]),
     "isg_fno_create": (_I, [_P, ctypes.POINTER(FnoOpts)]),
     "isg_fno_param_count": (_L, [_P]),
@@ -291,6 +293,24 @@ class Solver:
                             device=rx.device)
         self._check(lib().isg_aggregateh(self._h, _ptr(x), _ptr(rx), R, order, _stream(stream)), "aggregateh")
         return x
+
+    # ---- launch-shape autotuner ----
+    def autotune(self, nrhs: int = 1, engine: int = ENGINE_TENSOR, stream=None) -> dict:
+        """Times candidate launch shapes on nrhs RHS and keeps the fastest; returns the choices."""
+        self._check(lib().isg_autotune(self._h, nrhs, engine, _stream(stream)), "autotune")
+        return self.tuned()
+
+    def tuned(self) -> dict:
+        v = ctypes.c_int()
+        out = {}
+        for what, name in enumerate(("m2l_rows", "l2l_cols", "m2m_cols")):
+            out[name] = []
+            for lvl in range(self.level):
+                self._check(lib().isg_tuned(self._h, what, lvl, ctypes.byref(v)), "tuned")
+                out[name].append(v.value)
+        self._check(lib().isg_tuned(self._h, 3, 0, ctypes.byref(v)), "tuned")
+        out["near_pair"] = v.value
+        return out
 
     # ---- learned warm start ----
     def fno_create(self, width: int = 32, modes: int = 12, layers: int = 4, batch: int = 4, seed: int = 1):
