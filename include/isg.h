@@ -180,6 +180,10 @@ typedef struct isg_dbim_opts {
   int warm_start;        /* 0: every solve starts from zero, as the reference; 1: each transmitter's
                             total-field and adjoint solves start from its fields of the previous
                             iteration (same tolerance; not in the reference) */
+  const char *checkpoint;  /* directory, or NULL: writes the reference's outputs there, cg_<i>.bin
+                            (contrast, raster order, complex128) and hist.txt (misfit, object error,
+                            regularisation cost, gradient norm, object norm per line;
+                            setup_born.cpp:171-242) after the first gradient and each iteration */
 } isg_dbim_opts;
 
 typedef struct isg_dbim_record {

@@ -10,6 +10,9 @@
 #include <random>
 #include <vector>
 
+#include <cstdio>
+#include <string>
+
 #include "isg_context.hpp"
 
 namespace isg {
@@ -273,6 +276,7 @@ void isg_default_dbim_opts(isg_dbim_opts *o) {
   isg_default_solve_opts(&o->solve);
   o->solve.tol = 1e-4;
   o->warm_start = 0;
+  o->checkpoint = nullptr;
 }
 
 isg_status isg_measure(isg_ctx *c, int ntx, const void *inc, const double *chi, int order, double noise,
@@ -354,6 +358,7 @@ isg_status isg_dbim(isg_ctx *c, int ntx, const void *inc, const void *mes, const
     return ISG_UNSUPPORTED;
   }
   D.warm = O.warm_start != 0;
+  bool wrote_hist = false;
   const size_t U = D.U, nm = (size_t)ntx * D.nrx;
   if ((e = D.alloc(&D.incb, (size_t)ntx * U)) || (e = D.alloc(&D.tot, (size_t)ntx * U)) ||
       (e = D.alloc(&D.X, (size_t)D.R * U)) || (e = D.alloc(&D.Y, (size_t)D.R * U)) ||
@@ -411,14 +416,39 @@ isg_status isg_dbim(isg_ctx *c, int ntx, const void *inc, const void *mes, const
     }
     for (size_t q = 0; q < nm; q++) D.mesd[q] = D.rhs[q] - D.mes[q];
   }
+  // setup_born.cpp:171-242 (write_error): the contrast in raster order as
+  // cg_<iteration>.bin (complex128) and one line of hist.txt per record
+  auto checkpoint = [&](int file_iter, const isg_dbim_record &r) -> isg_status {
+    std::vector<double2> h(U), raster(U);
+    cudaMemcpyAsync(h.data(), D.o, U * sizeof(double2), cudaMemcpyDeviceToHost, st);
+    isg_status e2 = cuda_check(c, cudaStreamSynchronize(st), "dbim checkpoint");
+    if (e2 != ISG_OK) return e2;
+    for (size_t n = 0; n < U; n++) raster[c->T.raster_of_blocked[n]] = h[n];
+    const std::string dir(O.checkpoint);
+    const std::string cg = dir + "/cg_" + std::to_string(file_iter) + ".bin";
+    FILE *f = std::fopen(cg.c_str(), "wb");
+    FILE *hf = std::fopen((dir + "/hist.txt").c_str(), wrote_hist ? "a" : "w");
+    const bool ok = f && hf && std::fwrite(raster.data(), sizeof(double2), U, f) == U &&
+                    std::fprintf(hf, "%e %e %e %e %e\n", r.misfit, r.object_error, r.reg_cost, r.grad_norm,
+                                 r.object_norm) > 0;
+    if (f) std::fclose(f);
+    if (hf) std::fclose(hf);
+    wrote_hist = true;
+    if (!ok) {
+      c->err = "dbim checkpoint: cannot write " + cg + " or hist.txt";
+      return ISG_BAD_ARG;
+    }
+    return ISG_OK;
+  };
   auto record = [&](int idx, double alpha, zd beta) -> isg_status {
-    if (!hist) return ISG_OK;
+    if (!hist && !O.checkpoint) return ISG_OK;
     double t[3];
     isg_status e2 = D.sums(D.od, D.o, D.otrue, 0, t);
     if (e2 != ISG_OK) return e2;
     double err = 0;
     for (auto &v : D.mesd) err += std::norm(v);
-    isg_dbim_record &r = hist[idx];
+    isg_dbim_record local{};
+    isg_dbim_record &r = hist ? hist[idx] : local;
     r.misfit = err / mesnorm;
     r.object_error = chi_true ? t[2] / objnorm : -1.0;
     r.reg_cost = O.regular * O.regular * t[1] / mesnorm;
@@ -429,6 +459,8 @@ isg_status isg_dbim(isg_ctx *c, int ntx, const void *inc, const void *mes, const
     r.beta_im = beta.imag();
     r.solves = D.solves;
     r.iterations = D.iters;
+    // write_error(0) after the first gradient, write_error(iter) after each iteration
+    if (O.checkpoint) return checkpoint(idx == 0 ? 0 : idx - 1, r);
     return ISG_OK;
   };
   if ((e = D.gradient(O.regular)) != ISG_OK) return e;

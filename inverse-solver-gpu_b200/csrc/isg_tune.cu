@@ -1,6 +1,6 @@
 // Launch-shape autotuner: times the candidate shapes of the level-dependent
 // kernels on this context's own buffers and keeps the fastest per level.
-//   M2L   sibling-group rows per thread          1, 2, 4, 8, 16
+//   M2L   sibling-group rows per thread          1, 2, 4, ..., 64
 //   L2L   columns (RHS x parent) per tile block  32, 64
 //   M2M   columns per tile block (SIMT path)     32, 64
 //   near  16x8-leaf tiles per tensor-core CTA    1, 2
@@ -50,7 +50,7 @@ isg_status isg_autotune(isg_ctx *c, int nrhs, int engine, isg_stream stream) {
     DevLevel &d = P.lv[i];
     int best = 0;
     float tbest = FLT_MAX;
-    for (int ty : {1, 2, 4, 8, 16}) {
+    for (int ty : {1, 2, 4, 8, 16, 32, 64}) {
       if (ty > std::max(1, d.n / 2)) break;
       d.m2l_ty = ty;
       const float t = time_launch(st, e0, e1, [&] { launch_m2l(P, i, c->mul, c->loc, nrhs, nullptr, i >= 3, st); });

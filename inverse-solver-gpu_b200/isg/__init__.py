@@ -56,7 +56,7 @@ class SolveInfo(ctypes.Structure):
 
 class DbimOpts(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int), ("regular", ctypes.c_double), ("start_from_chi", ctypes.c_int),
-                ("solve", SolveOpts), ("warm_start", ctypes.c_int)]
+                ("solve", SolveOpts), ("warm_start", ctypes.c_int), ("checkpoint", ctypes.c_char_p)]
 
 
 class DbimRecord(ctypes.Structure):
@@ -373,8 +373,8 @@ class Solver:
         return mes
 
     def dbim(self, inc, mes, chi=None, chi_true=None, iterations: int = 3, regular: float = 0.0,
-             order: int = ORDER_TREE, start_from_chi: bool = False, warm_start: bool = False, stream=None,
-             **solve):
+             order: int = ORDER_TREE, start_from_chi: bool = False, warm_start: bool = False,
+             checkpoint: str | None = None, stream=None, **solve):
         """The reference's inversion loop (mom.cpp:222-399); returns (chi, history records)."""
         import torch
         ntx = 1 if inc.dim() == 1 else inc.shape[0]
@@ -384,6 +384,7 @@ class Solver:
         lib().isg_default_dbim_opts(ctypes.byref(o))
         o.iterations, o.regular, o.start_from_chi = iterations, regular, int(start_from_chi)
         o.warm_start = int(warm_start)
+        o.checkpoint = checkpoint.encode() if checkpoint else None
         for k, v in solve.items():
             setattr(o.solve, k, v)
         hist = (DbimRecord * (iterations + 1))()

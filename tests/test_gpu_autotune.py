@@ -22,7 +22,7 @@ def test_autotune_keeps_the_operator(engine):
     x = torch.from_numpy((rng.normal(size=(8, s.numunk)) + 1j * rng.normal(size=(8, s.numunk))).astype(np.complex64)).cuda()
     before = s.matvec(x, g, engine=engine).cpu().numpy()
     got = s.autotune(8, engine)
-    assert all(v in (1, 2, 4, 8, 16) for v in got["m2l_rows"][2:])
+    assert all(v in (1, 2, 4, 8, 16, 32, 64) for v in got["m2l_rows"][2:])
     assert all(v in (32, 64) for v in got["l2l_cols"][3:])
     assert all(v in (32, 64) for v in got["m2m_cols"][2:-1])
     assert got["near_pair"] in ((1, 2) if engine == isg.ENGINE_TENSOR else (0,))

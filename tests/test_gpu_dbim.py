@@ -87,3 +87,31 @@ def test_sharded_driver_on_one_gpu_matches_isg_dbim():
     m1 = np.array([h["misfit"] for h in hist])
     m2 = np.array([h["misfit"] for h in hist2])
     assert np.max(np.abs(m2 - m1) / m1) < 1e-3, (m1, m2)
+
+
+def test_dbim_checkpoint_files_follow_the_reference(tmp_path):
+    """With a checkpoint directory the loop writes what the reference's
+    write_error writes (setup_born.cpp:171-242): cg_<i>.bin, the contrast in
+    raster order as complex128, and hist.txt, one line of five numbers per
+    record.  The last file is the returned contrast, the history lines are the
+    returned records, and the reference's own cg_2.bin of the same run agrees
+    to the parity tolerance of the history test (2e-3)."""
+    import torch
+    d = dict(np.load(GOLDEN))
+    ntx = int(d["ntx"])
+    s = isg.Solver(int(d["level"]), numrx=int(d["numrx"]), max_rhs=ntx)
+    chi_true = torch.from_numpy(d["phantom"].astype(np.float64) * 0.1 + 0j).cuda()
+    inc = torch.from_numpy(s.plane_waves(ntx, order=isg.ORDER_RASTER).astype(np.complex64)).cuda()
+    tol = float(d["tol"])
+    mes = s.measure(inc, chi_true, order=isg.ORDER_RASTER, tol=tol, engine=isg.ENGINE_TENSOR)
+    chi, hist = s.dbim(inc, mes, chi_true=chi_true, iterations=3, order=isg.ORDER_RASTER, tol=tol,
+                       engine=isg.ENGINE_TENSOR, checkpoint=str(tmp_path))
+    files = sorted(p.name for p in tmp_path.iterdir())
+    assert files == ["cg_0.bin", "cg_1.bin", "cg_2.bin", "hist.txt"]
+    cg2 = np.fromfile(tmp_path / "cg_2.bin", dtype=np.complex128)
+    assert np.array_equal(cg2, chi.cpu().numpy())
+    assert rel(cg2, d["cg2"]) < 2e-3
+    lines = np.loadtxt(tmp_path / "hist.txt")
+    assert lines.shape == (4, 5)
+    want = np.array([[h["misfit"], h["object_error"], h["reg_cost"], h["grad_norm"], h["object_norm"]] for h in hist])
+    assert np.allclose(lines, want, rtol=1e-5)
