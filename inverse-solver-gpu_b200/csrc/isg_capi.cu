@@ -368,6 +368,13 @@ isg_status isg_setup_gpu(isg_ctx *c) {
   if ((e = cuda_check(c, cudaMallocHost(&c->h_count, sizeof(int)), "cudaMallocHost"))) return e;
   if ((e = cuda_check(c, cudaMemset(c->mul, 0, R * P.mp * sizeof(float2)), "memset"))) return e;
   if ((e = cuda_check(c, cudaMemset(c->loc, 0, R * P.mp * sizeof(float2)), "memset"))) return e;
+  {
+    int nsmax = 1;
+    for (int i = 0; i < L; i++) nsmax = std::max(nsmax, T.nsamp[i]);
+    if ((e = dalloc(c, &P.zeros, (size_t)nsmax)) ||
+        (e = cuda_check(c, cudaMemset(P.zeros, 0, (size_t)nsmax * sizeof(float2)), "memset")))
+      return e;
+  }
   if ((e = cuda_check(c, kernels_setup(), "kernel attributes")) != ISG_OK) return e;
   if ((e = tc_setup(c)) != ISG_OK) return e;
   if ((e = band_setup(c)) != ISG_OK) return e;

@@ -65,6 +65,7 @@ struct DevPlan {
   float *haw = nullptr;      // [ns_0][hwidth]
   int hwidth = 0;
   int tuned_nrhs = 0;         // batch the tuned shapes were timed on; they apply from a quarter of it
+  float2 *zeros = nullptr;    // [max ns] zeros: what a clipped M2L column reads
   int *perm_tree = nullptr;   // blocked index -> tree index
   int *perm_raster = nullptr; // blocked index -> raster index
 };

@@ -88,21 +88,83 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // the same six-column window, each with 27 of the 40 translation weights
 // T[(dy+3)*7+dx+3][k] whose offset is not inside the 3x3.  A thread owns one
 // sample k of one column of sibling groups: it keeps the 40 weights in
-// registers, slides the 6x6 window of multipoles down `ty` groups (two new
-// rows per step, read straight from L1/L2 and prefetched one step ahead) and
-// writes (or adds to, after L2L) the four siblings' locals per step: 108
-// complex FMAs per 12 loads.
-// Consecutive threads take consecutive samples, so every load and store is
-// coalesced along the cluster's samples.
+// registers and slides the window down `ty` groups, two new rows per step,
+// fetched one step ahead into a ring of eight row slots.  The step loop is
+// unrolled four times so every slot index is a compile-time constant (the
+// ring turns once per four steps): no register moves, and the four siblings'
+// locals accumulate in place (from the prefetched old values after L2L).
+// Rows outside the grid are the same for the whole block (a branch); a
+// column outside the grid reads a ring of zeros with row stride 0, so no load
+// needs a select.  108 complex FMAs per 12 loads; consecutive threads take
+// consecutive samples, so every load and store is coalesced.
 struct M2lArgs {
   const float2 *mul;
   float2 *loc;
   size_t mp, off;
-  int n, ns, ty, accumulate;
+  int n, ns, ty;
   const float2 *T;
   const int *active;
+  const float2 *zeros;  // at least ns zeros
 };
 
+// One thread's six source columns: base address and bytes per cluster row.
+struct M2lCols {
+  const char *base[6];
+  unsigned stride[6];
+};
+
+__device__ __forceinline__ void m2l_row(const M2lCols &C, int row, int n, float2 (&dst)[6]) {
+  if (row >= 0 && row < n) {
+#pragma unroll
+    for (int j = 0; j < 6; j++)
+      dst[j] = __ldg((const float2 *)(C.base[j] + (unsigned long long)(unsigned)row * C.stride[j]));
+  } else {
+#pragma unroll
+    for (int j = 0; j < 6; j++) dst[j] = make_float2(0.f, 0.f);
+  }
+}
+
+// The sibling group's locals at group row a (read before adding to them).
+template <bool ACC>
+__device__ __forceinline__ void m2l_old(const float2 *out, size_t row_stride, int ns, int b, int a,
+                                        float2 (&dst)[2][2]) {
+#pragma unroll
+  for (int oy = 0; oy < 2; oy++)
+#pragma unroll
+    for (int ox = 0; ox < 2; ox++)
+      dst[oy][ox] = ACC ? out[(size_t)(2 * a + oy) * row_stride + (size_t)(2 * b + ox) * ns] : make_float2(0.f, 0.f);
+}
+
+// Step S (mod 4) of the ring: group row a, window rows 2a-2+i in slot (2S+i) & 7.
+template <int S, bool ACC>
+__device__ __forceinline__ void m2l_step(const M2lArgs &A, const M2lCols &C, const float2 (&tw)[7][7],
+                                         float2 (&w)[8][6], float2 (&ob)[2][2][2], float2 *out, size_t row_stride,
+                                         int b, int a, int a1) {
+  if (a + 1 < a1) {
+    m2l_row(C, 2 * a + 4, A.n, w[(2 * S + 6) & 7]);
+    m2l_row(C, 2 * a + 5, A.n, w[(2 * S + 7) & 7]);
+    m2l_old<ACC>(out, row_stride, A.ns, b, a + 1, ob[(S + 1) & 1]);
+  }
+  float2(&acc)[2][2] = ob[S & 1];
+#pragma unroll
+  for (int i = 0; i < 6; i++)
+#pragma unroll
+    for (int j = 0; j < 6; j++)
+#pragma unroll
+      for (int oy = 0; oy < 2; oy++)
+#pragma unroll
+        for (int ox = 0; ox < 2; ox++) {
+          const int dy = i - 2 - oy, dx = j - 2 - ox;  // source minus target
+          if (dy >= -1 && dy <= 1 && dx >= -1 && dx <= 1) continue;
+          cfma(acc[oy][ox], tw[dy + 3][dx + 3], w[(2 * S + i) & 7][j]);
+        }
+#pragma unroll
+  for (int oy = 0; oy < 2; oy++)
+#pragma unroll
+    for (int ox = 0; ox < 2; ox++) out[(size_t)(2 * a + oy) * row_stride + (size_t)(2 * b + ox) * A.ns] = acc[oy][ox];
+}
+
+template <bool ACC>
 __global__ void __launch_bounds__(128, 2) k_m2l(M2lArgs A) {
   const int rhs = blockIdx.z;
   if (A.active && !A.active[rhs]) return;
@@ -121,73 +183,27 @@ __global__ void __launch_bounds__(128, 2) k_m2l(M2lArgs A) {
   const float2 *m = A.mul + (size_t)rhs * A.mp + A.off + k;
   float2 *out = A.loc + (size_t)rhs * A.mp + A.off + k;
   const size_t row_stride = (size_t)A.n * ns;
-  int cofs[6];
-  bool cok[6];
+  M2lCols C;
 #pragma unroll
   for (int j = 0; j < 6; j++) {
     const int col = 2 * b - 2 + j;
-    cok[j] = col >= 0 && col < A.n;
-    cofs[j] = col * ns;
+    const bool ok = col >= 0 && col < A.n;
+    C.base[j] = ok ? (const char *)(m + (size_t)col * ns) : (const char *)(A.zeros + k);
+    C.stride[j] = ok ? (unsigned)(row_stride * sizeof(float2)) : 0u;
   }
-  auto load_row = [&](int row, float2 (&dst)[6]) {
-    const bool rok = row >= 0 && row < A.n;
-    const float2 *rp = m + (ptrdiff_t)(rok ? row : 0) * (ptrdiff_t)row_stride;
+  float2 w[8][6], ob[2][2][2];
 #pragma unroll
-    for (int j = 0; j < 6; j++) dst[j] = (rok && cok[j]) ? __ldg(rp + cofs[j]) : make_float2(0.f, 0.f);
-  };
-  // the sibling group's current locals (added to when accumulating), one step ahead
-  auto load_old = [&](int a, float2 (&dst)[2][2]) {
-#pragma unroll
-    for (int oy = 0; oy < 2; oy++)
-#pragma unroll
-      for (int ox = 0; ox < 2; ox++)
-        dst[oy][ox] = A.accumulate ? out[(ptrdiff_t)(2 * a + oy) * (ptrdiff_t)row_stride + (2 * b + ox) * ns]
-                                   : make_float2(0.f, 0.f);
-  };
-  float2 w[6][6], pre[2][6], old[2][2];
-#pragma unroll
-  for (int i = 0; i < 4; i++) load_row(2 * a0 - 2 + i, w[i]);
-  load_row(2 * a0 + 2, pre[0]);
-  load_row(2 * a0 + 3, pre[1]);
-  load_old(a0, old);
+  for (int i = 0; i < 6; i++) m2l_row(C, 2 * a0 - 2 + i, A.n, w[i]);
+  m2l_old<ACC>(out, row_stride, ns, b, a0, ob[0]);
 #pragma unroll 1
-  for (int a = a0; a < a1; a++) {
-#pragma unroll
-    for (int j = 0; j < 6; j++) {
-      w[4][j] = pre[0][j];
-      w[5][j] = pre[1][j];
-    }
-    float2 acc[2][2];
-#pragma unroll
-    for (int oy = 0; oy < 2; oy++)
-#pragma unroll
-      for (int ox = 0; ox < 2; ox++) acc[oy][ox] = old[oy][ox];
-    if (a + 1 < a1) {
-      load_row(2 * a + 4, pre[0]);
-      load_row(2 * a + 5, pre[1]);
-      load_old(a + 1, old);
-    }
-#pragma unroll
-    for (int i = 0; i < 6; i++)
-#pragma unroll
-      for (int j = 0; j < 6; j++)
-#pragma unroll
-        for (int oy = 0; oy < 2; oy++)
-#pragma unroll
-          for (int ox = 0; ox < 2; ox++) {
-            const int dy = i - 2 - oy, dx = j - 2 - ox;  // source minus target
-            if (dy >= -1 && dy <= 1 && dx >= -1 && dx <= 1) continue;
-            cfma(acc[oy][ox], tw[dy + 3][dx + 3], w[i][j]);
-          }
-#pragma unroll
-    for (int oy = 0; oy < 2; oy++)
-#pragma unroll
-      for (int ox = 0; ox < 2; ox++)
-        out[(ptrdiff_t)(2 * a + oy) * (ptrdiff_t)row_stride + (2 * b + ox) * ns] = acc[oy][ox];
-#pragma unroll
-    for (int i = 0; i < 4; i++)
-#pragma unroll
-      for (int j = 0; j < 6; j++) w[i][j] = w[i + 2][j];
+  for (int a = a0; a < a1; a += 4) {
+    m2l_step<0, ACC>(A, C, tw, w, ob, out, row_stride, b, a, a1);
+    if (a + 1 >= a1) break;
+    m2l_step<1, ACC>(A, C, tw, w, ob, out, row_stride, b, a + 1, a1);
+    if (a + 2 >= a1) break;
+    m2l_step<2, ACC>(A, C, tw, w, ob, out, row_stride, b, a + 2, a1);
+    if (a + 3 >= a1) break;
+    m2l_step<3, ACC>(A, C, tw, w, ob, out, row_stride, b, a + 3, a1);
   }
 }
 
@@ -622,7 +638,7 @@ void launch_m2l(const DevPlan &P, int lvl, const float2 *mul, float2 *loc, int n
   A.ns = c.ns;
   A.T = c.T;
   A.active = active;
-  A.accumulate = accumulate ? 1 : 0;
+  A.zeros = P.zeros;
   const int half = c.n / 2, bx = (half * c.ns + 127) / 128;
   // eight groups per thread when the grid stays large, fewer for small batches
   int ty = std::min(8, half);
@@ -630,7 +646,11 @@ void launch_m2l(const DevPlan &P, int lvl, const float2 *mul, float2 *loc, int n
   if (c.m2l_ty > 0 && 4 * nrhs >= P.tuned_nrhs) ty = std::min(c.m2l_ty, std::max(1, half));
   A.ty = ty;
   count_launch();
-  k_m2l<<<dim3(bx, (half + ty - 1) / ty, nrhs), 128, 0, st>>>(A);
+  const dim3 grid(bx, (half + ty - 1) / ty, nrhs);
+  if (accumulate)
+    k_m2l<true><<<grid, 128, 0, st>>>(A);
+  else
+    k_m2l<false><<<grid, 128, 0, st>>>(A);
 }
 
 void launch_l2l(const DevPlan &P, int lvl, float2 *loc, int nrhs, const int *active, cudaStream_t st) {
