@@ -590,7 +590,7 @@ isg_status isg_time_stages(isg_ctx *c, int nrhs, int engine, int reps, double *m
       if (!(tc && band_m2m(c, i, c->mul, nrhs, nullptr, st, &be))) launch_m2m(P, i, c->mul, nrhs, nullptr, st);
     cudaEventRecord(ev[2], st);
     for (int i = 2; i < P.L; i++) {
-      if (i >= 3) launch_l2l(P, i, c->loc, nrhs, nullptr, st);
+      if (i >= 3 && !(tc && band_l2l(c, i, c->loc, nrhs, nullptr, st, &be))) launch_l2l(P, i, c->loc, nrhs, nullptr, st);
       launch_m2l(P, i, c->mul, c->loc, nrhs, nullptr, i >= 3, st);
     }
     cudaEventRecord(ev[3], st);

@@ -101,6 +101,9 @@ int tc_error(isg_ctx *c);
 isg_status band_setup(isg_ctx *c);
 void band_destroy(isg_ctx *c);
 bool band_m2m(isg_ctx *c, int lvl, float2 *mul, int nrhs, const int *active, cudaStream_t st, isg_status *e);
+// L2L into child level lvl on the tensor cores (overwrites its locals); false
+// when the level is not covered (its rings have more than 128 samples).
+bool band_l2l(isg_ctx *c, int lvl, float2 *loc, int nrhs, const int *active, cudaStream_t st, isg_status *e);
 // Learned warm start (isg_fno.cu).
 isg_status fno_create(isg_ctx *c, const isg_fno_opts *o);
 void fno_destroy(isg_ctx *c);

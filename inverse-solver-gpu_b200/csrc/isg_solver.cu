@@ -370,9 +370,10 @@ isg_status run_matvec(isg_ctx *c, const float2 *x, const float2 *g, int64_t gs, 
   // level by level: the parent's locals anterpolated over the level (L2L),
   // then the level's own far-field translations added (M2L)
   for (int i = 2; i < P.L; i++) {
-    if (i >= 3) launch_l2l(P, i, c->loc, nrhs, active, st);
+    if (i >= 3 && !(tc && band_l2l(c, i, c->loc, nrhs, active, st, &be))) launch_l2l(P, i, c->loc, nrhs, active, st);
     launch_m2l(P, i, c->mul, c->loc, nrhs, active, i >= 3, st);
   }
+  if (be != ISG_OK) return be;
   NearArgs A;
   A.in = pre ? Bg : B;
   A.x_epi = pre ? x : nullptr;

@@ -11,8 +11,19 @@
 // one or more RHS; ring values are split into FP16 hi/lo after a power-of-two
 // scale per CTA (3 products, FP32 accumulation in TMEM).  The child shift
 // phases are folded into the epilogue (sum over the four children), exactly as
-// in the reference.  (Anterpolation, whose windows are about twice as wide,
-// runs on the SIMT tiled kernel: measured faster there.)
+// in the reference.
+//
+// L2L (kernels.cu:138-190, solve.cpp:150-168) on the tensor cores, for the
+// levels whose rings have at most 128 samples (the leaves and their parents,
+// most of the tree's samples): persistent CTAs keep the level's whole
+// anterpolation matrix (128 child samples x the parent ring, FP16 hi/lo) in
+// shared memory and walk items of 32 (or 16) parents.  An item's parent rings
+// arrive by cp.async while the previous item is multiplied and written; each
+// CTA forms the four shifted copies shl[q][j] z[j] of every ring directly in
+// the FP16 hi/lo operand layout (256 MMA columns = 32 parents x 4 children x
+// re, im), and the epilogue writes each child ring from TMEM with the child
+// sample on the lane, so every store is coalesced.  Coarser levels keep the
+// SIMT tiled kernel.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -220,6 +231,188 @@ __global__ void __launch_bounds__(256, 2) k_tc_band(BandArgs A) {
   if (warp == 0) tmem_dealloc(tmem, 256);
 }
 
+// ---- L2L ----
+constexpr int kErrL2l = 122;
+
+struct L2lArgs {
+  float2 *loc;  // every level's locals; parent rings at off_in, child rings at off_out
+  size_t mp, off_in, off_out;
+  int n_p, ns_in, ns_out, Kp, ppi;  // padded K, parents per item
+  const uint8_t *A;                 // [128 x Kp] FP16 hi then lo, K-major core matrices
+  const float2 *shl;                // [ns_in][4] local shifts of the parent level
+  float inv_a, shl_max;
+  int nparents, items_per_rhs, nitems;
+  const int *active;
+  int *err;
+};
+
+// Shared-memory carve-up (bytes): A hi/lo, B hi/lo, staged rings [ppi][Kp]
+// float2, shifts [Kp][4] float2, barriers and scratch.
+struct L2lSmem {
+  size_t a, b, z, sh, bar, total;
+  __host__ __device__ L2lSmem(int Kp, int ppi) {
+    a = 0;
+    b = a + (size_t)512 * Kp;
+    z = b + (size_t)2 * (8 * ppi) * Kp * 2;
+    sh = z + (size_t)ppi * Kp * 8;
+    bar = sh + (size_t)Kp * 32;
+    total = bar + 64;
+  }
+};
+
+__global__ void __launch_bounds__(256, 1) k_tc_l2l(L2lArgs A) {
+  extern __shared__ __align__(1024) char sm[];
+  const L2lSmem L(A.Kp, A.ppi);
+  const int N = 8 * A.ppi, Kp = A.Kp, kc = Kp / 8;
+  char *ahi = sm + L.a, *bhi = sm + L.b, *blo = bhi + (size_t)N * Kp * 2;
+  float2 *zst = (float2 *)(sm + L.z);
+  float2 *shs = (float2 *)(sm + L.sh);
+  uint64_t *abar = (uint64_t *)(sm + L.bar);
+  uint64_t *done = abar + 1;
+  uint32_t *tslot = (uint32_t *)(abar + 2);
+  float *fscr = (float *)(abar + 3);  // [8]
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    mbar_init(abar, 1);
+    mbar_init(done, 1);
+    fence_mbar_init();
+  }
+  if (warp == 0) tmem_alloc(tslot, N);
+  // shifts and the zero tails of the ring staging (cp.async never writes past ns_in)
+  for (int e = threadIdx.x; e < Kp * 4; e += blockDim.x)
+    shs[e] = (e >> 2) < A.ns_in ? __ldg(A.shl + e) : make_float2(0.f, 0.f);
+  for (int e = threadIdx.x; e < A.ppi * (Kp - A.ns_in); e += blockDim.x) {
+    const int pl = e / (Kp - A.ns_in), j = A.ns_in + e % (Kp - A.ns_in);
+    zst[pl * Kp + j] = make_float2(0.f, 0.f);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+  if (threadIdx.x == 0) {
+    mbar_expect_tx(abar, 512 * Kp);
+    bulk_g2s(ahi, A.A, 512 * Kp, abar);
+  }
+  auto active_item = [&](int w) {
+    while (w < A.nitems && A.active && !A.active[w / A.items_per_rhs]) w += gridDim.x;
+    return w;
+  };
+  // an item's parent rings into the staging buffer, 16 bytes per copy
+  const int pieces = A.ns_in / 2;
+  auto stage = [&](int w) {
+    const int rhs = w / A.items_per_rhs, p0 = (w % A.items_per_rhs) * A.ppi;
+    const float2 *base = A.loc + (size_t)rhs * A.mp + A.off_in;
+    for (int e = threadIdx.x; e < A.ppi * pieces; e += blockDim.x) {
+      const int pl = e / pieces, c = e - pl * pieces, P = p0 + pl;
+      const bool ok = P < A.nparents;
+      cp_async16z(zst + pl * Kp + 2 * c, base + (size_t)(ok ? P : 0) * A.ns_in + 2 * c, ok);
+    }
+  };
+  const uint32_t sbase = smem_u32(sm);
+  const uint32_t idesc = idesc_f16_f32(128, N);
+  const uint32_t sbo = (uint32_t)kc * 128;
+  bool ok = mbar_wait(abar, 0, A.err, kErrL2l);
+  int parity = 0;
+  int w = active_item(blockIdx.x);
+  if (w < A.nitems) stage(w);
+  cp_async_wait_all();
+  __syncthreads();
+  while (w < A.nitems) {
+    // power-of-two scale of this item's shifted rings
+    float mx = 0.f;
+    for (int e = threadIdx.x; e < A.ppi * pieces; e += blockDim.x) {
+      const int pl = e / pieces, c = e - pl * pieces;
+      const float4 v = *(const float4 *)(zst + pl * Kp + 2 * c);
+      mx = fmaxf(mx, fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w))));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) fscr[warp] = mx;
+    __syncthreads();
+    float m2 = 0.f;
+    for (int k = 0; k < 8; k++) m2 = fmaxf(m2, fscr[k]);
+    const float s = pow2_scale(1.5f * A.shl_max * m2);
+    // B operand: row n = 8 parent + 2 q + c holds component c of shl[q][j] z[j] s;
+    // a unit is one row of one core matrix (8 samples), 8 consecutive threads fill it
+    for (int u = threadIdx.x; u < A.ppi * Kp; u += blockDim.x) {
+      const int r = u & 7, cm = u >> 3, pl = cm / kc, j0 = (cm - pl * kc) * 8;
+      const int q = r >> 1, c = r & 1;
+      float v[8];
+#pragma unroll
+      for (int e = 0; e < 8; e++) {
+        const float2 z = zst[pl * Kp + j0 + e], sh = shs[(j0 + e) * 4 + q];
+        v[e] = c ? fmaf(sh.x, z.y, sh.y * z.x) : fmaf(sh.x, z.x, -sh.y * z.y);
+      }
+      __align__(16) __half h[8], l[8];
+#pragma unroll
+      for (int e = 0; e < 8; e++) split_f16(v[e] * s, h[e], l[e]);
+      *(uint4 *)(bhi + (size_t)cm * 128 + r * 16) = *(uint4 *)h;
+      *(uint4 *)(blo + (size_t)cm * 128 + r * 16) = *(uint4 *)l;
+    }
+    fence_proxy_async();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      tc_fence_after();
+      if (ok)
+        for (int ks = 0; ks < Kp / 16; ks++) {
+          const uint64_t ah = smem_desc(sbase + (uint32_t)L.a + ks * 256, 128, sbo);
+          const uint64_t al = smem_desc(sbase + (uint32_t)L.a + 256 * Kp + ks * 256, 128, sbo);
+          const uint64_t bh = smem_desc(smem_u32(bhi) + ks * 256, 128, sbo);
+          const uint64_t bl = smem_desc(smem_u32(blo) + ks * 256, 128, sbo);
+          mma_f16(tmem, ah, bh, idesc, ks ? 1 : 0);
+          mma_f16(tmem, ah, bl, idesc, 1);
+          mma_f16(tmem, al, bh, idesc, 1);
+        }
+      mma_commit(done);
+    }
+    // the next item's rings, in flight while this one is multiplied and written
+    const int rhs = w / A.items_per_rhs, p0 = (w % A.items_per_rhs) * A.ppi;
+    const int nxt = active_item(w + gridDim.x);
+    if (nxt < A.nitems) stage(nxt);
+    ok = mbar_wait(done, parity, A.err, kErrL2l) && ok;
+    parity ^= 1;
+    tc_fence_after();
+    // epilogue: lane = child sample, 16 columns = 2 parents x 4 children x (re, im)
+    const float inv = A.inv_a / s;
+    const int qd = warp & 3, hcol = warp >> 2, km = 32 * qd + lane;
+    const int nch = N / 32;  // 16-column chunks per warp
+    float2 *obase = A.loc + (size_t)rhs * A.mp + A.off_out + km;
+    const int nc = 2 * A.n_p;
+    for (int ch = 0; ch < nch; ch++) {
+      const int col0 = hcol * (N / 2) + 16 * ch;
+      float d[16];
+      tmem_ld16(tmem + ((uint32_t)(32 * qd) << 16) + col0, d);
+      if (!ok || km >= A.ns_out) continue;
+#pragma unroll
+      for (int u = 0; u < 2; u++) {
+        const int P = p0 + col0 / 8 + u;
+        if (P >= A.nparents) continue;
+        const int py = P / A.n_p, px = P - py * A.n_p;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const size_t cl = (size_t)(2 * py + (q >> 1)) * nc + 2 * px + (q & 1);
+          obase[cl * A.ns_out] = make_float2(d[8 * u + 2 * q] * inv, d[8 * u + 2 * q + 1] * inv);
+        }
+      }
+    }
+    cp_async_wait_all();
+    tc_fence_before();
+    __syncthreads();  // staging, B and TMEM are reused by the next item
+    w = nxt;
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, N);
+}
+
+// One L2L transition on the tensor cores (child level `lvl`).
+struct L2lPlan {
+  uint8_t *A = nullptr;  // device
+  int Kp = 0, ppi = 0;
+  float inv_a = 1, shl_max = 1;
+  bool ok = false;
+};
+
 // One level transition: weight chunks and per-tile windows.
 struct Transition {
   int mtiles = 0;
@@ -249,8 +442,63 @@ void pack_chunk(std::vector<uint8_t> &buf, size_t at, int k0, double scale, F re
 
 struct BandPlan {
   Transition m2m[kMaxLevels];  // indexed by parent level
+  L2lPlan l2l[kMaxLevels];     // indexed by child level
   std::vector<void *> allocs;
+  int sms = 148;
 };
+
+// The [128 x Kp] anterpolation matrix of child level i (rows: child samples,
+// columns: parent samples) as FP16 hi then lo in the K-major core-matrix
+// layout, after a power-of-two scale; shl_max = max |shiftloc| of the parent.
+static isg_status build_l2l(isg_ctx *c, int i, size_t smem_cap) {
+  const HostTables &H = c->T;
+  const int ns_out = H.nsamp[i], ns_in = H.nsamp[i - 1], W = 2 * H.ninter, taps = H.antcount[i];
+  L2lPlan &T = c->band->l2l[i];
+  if (ns_out > 128) return ISG_OK;
+  const int Kp = (ns_in + 15) / 16 * 16;
+  int ppi = 0;
+  for (int cand : {32, 16, 8})
+    if (L2lSmem(Kp, cand).total <= smem_cap) {
+      ppi = cand;
+      break;
+    }
+  const int nparents = 1 << (2 * (i - 1));
+  if (!ppi || nparents % ppi) return ISG_OK;
+  std::vector<double> dense((size_t)128 * Kp, 0.0);
+  double mw = 0;
+  for (int k = 0; k < ns_out; k++)
+    for (int t = 0; t < taps; t++) {
+      const int j = H.antind[i][(size_t)k * W + t];
+      dense[(size_t)k * Kp + j] += H.anterp[i][(size_t)k * W + t];
+    }
+  for (double v : dense) mw = std::max(mw, std::abs(v));
+  int e2;
+  std::frexp(mw > 0 ? mw : 1.0, &e2);
+  const double sa = std::ldexp(1.0, 14 - e2);
+  std::vector<uint8_t> buf((size_t)512 * Kp, 0);
+  __half *hi = (__half *)buf.data(), *lo = (__half *)(buf.data() + (size_t)256 * Kp);
+  for (int m = 0; m < 128; m++)
+    for (int k = 0; k < Kp; k++) {
+      const double v = dense[(size_t)m * Kp + k] * sa;
+      const __half h = __double2half(v);
+      const __half l = __double2half(v - (double)__half2float(h));
+      const size_t idx = ((size_t)(m / 8) * (Kp / 8) + k / 8) * 64 + (m % 8) * 8 + (k % 8);
+      hi[idx] = h;
+      lo[idx] = l;
+    }
+  double smax = 0;
+  for (const cd &z : H.shiftloc[i - 1]) smax = std::max(smax, std::abs(z));
+  isg_status e;
+  if ((e = cuda_check(c, cudaMalloc(&T.A, buf.size()), "l2l alloc")) != ISG_OK) return e;
+  if ((e = cuda_check(c, cudaMemcpy(T.A, buf.data(), buf.size(), cudaMemcpyHostToDevice), "l2l upload")) != ISG_OK)
+    return e;
+  T.Kp = Kp;
+  T.ppi = ppi;
+  T.inv_a = (float)(1.0 / sa);
+  T.shl_max = (float)std::max(smax, 1e-30);
+  T.ok = true;
+  return ISG_OK;
+}
 
 // Builds one transition from rows of taps (index into the input ring, weight).
 static isg_status build_transition(isg_ctx *c, Transition &T, int ns_out, int ns_in,
@@ -339,6 +587,21 @@ isg_status band_setup(isg_ctx *c) {
         rows[k].push_back({H.intind[i][(size_t)k * ni + t], H.interp[i][(size_t)k * ni + t]});
     if ((e = build_transition(c, c->band->m2m[i], nsp, nsc, rows)) != ISG_OK) return e;
   }
+  int dev = 0, optin = 0;
+  cudaFuncAttributes fa;
+  if ((e = cuda_check(c, cudaGetDevice(&dev), "device")) != ISG_OK ||
+      (e = cuda_check(c, cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev), "attr")) !=
+          ISG_OK ||
+      (e = cuda_check(c, cudaDeviceGetAttribute(&c->band->sms, cudaDevAttrMultiProcessorCount, dev), "attr")) !=
+          ISG_OK ||
+      (e = cuda_check(c, cudaFuncGetAttributes(&fa, k_tc_l2l), "l2l attr")) != ISG_OK)
+    return e;
+  const size_t cap = (size_t)optin - fa.sharedSizeBytes;
+  for (int i = 3; i < L; i++)  // L2L into child level i
+    if ((e = build_l2l(c, i, cap)) != ISG_OK) return e;
+  if ((e = cuda_check(c, cudaFuncSetAttribute(k_tc_l2l, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap),
+                      "l2l attr")) != ISG_OK)
+    return e;
   return cuda_check(c, cudaFuncSetAttribute(k_tc_band, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem),
                     "band attr");
 }
@@ -352,6 +615,7 @@ void band_destroy(isg_ctx *c) {
     cudaFree(T->kw0);
     cudaFree(T->nchunk);
     cudaFree(T->chunk0);
+    cudaFree(c->band->l2l[i].A);
   }
   delete c->band;
   c->band = nullptr;
@@ -393,5 +657,34 @@ bool band_m2m(isg_ctx *c, int lvl, float2 *mul, int nrhs, const int *active, cud
   return true;
 }
 
+
+bool band_l2l(isg_ctx *c, int lvl, float2 *loc, int nrhs, const int *active, cudaStream_t st, isg_status *e) {
+  if (!c->band || lvl >= kMaxLevels || !c->band->l2l[lvl].ok) return false;
+  const L2lPlan &T = c->band->l2l[lvl];
+  const DevLevel &p = c->P.lv[lvl - 1], &ch = c->P.lv[lvl];
+  L2lArgs A;
+  A.loc = loc;
+  A.mp = c->P.mp;
+  A.off_in = p.off;
+  A.off_out = ch.off;
+  A.n_p = p.n;
+  A.ns_in = p.ns;
+  A.ns_out = ch.ns;
+  A.Kp = T.Kp;
+  A.ppi = T.ppi;
+  A.A = T.A;
+  A.shl = p.shlT;
+  A.inv_a = T.inv_a;
+  A.shl_max = T.shl_max;
+  A.nparents = p.n * p.n;
+  A.items_per_rhs = A.nparents / T.ppi;
+  A.nitems = A.items_per_rhs * nrhs;
+  A.active = active;
+  A.err = c->tc_err_flag();
+  count_launch();
+  k_tc_l2l<<<std::min(A.nitems, c->band->sms), 256, L2lSmem(T.Kp, T.ppi).total, st>>>(A);
+  *e = cuda_check(c, cudaGetLastError(), "l2l launch");
+  return true;
+}
 
 }  // namespace isg
