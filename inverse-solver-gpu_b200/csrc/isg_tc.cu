@@ -222,23 +222,23 @@ __global__ void __launch_bounds__(256, 1) k_tc_near(TcNearArgs A) {
     const uint32_t sbase = smem_u32(sm);
     if (threadIdx.x == 0) {
       tc_fence_after();
+      const uint64_t ah0 = smem_desc(sbase + NearSmem::hi, kLboA, kSboA);
+      const uint64_t al0 = smem_desc(sbase + NearSmem::lo, kLboA, kSboA);
+      const uint64_t bh0 = smem_desc(sbase + NearSmem::stages, 128, 512);
+      const uint64_t bl0 = smem_desc(sbase + NearSmem::stages + kStageHalf, 128, 512);
       for (int t = 0; t < kNearStages; t++) {
         const int b = t % kNB;
         if (!mbar_wait(&full[b], (t / kNB) & 1, A.err, kErrNearFull)) break;
         const int s = t >> 2, c = t & 3, dr = s / 3 - 1, dc = s % 3 - 1;
-        const uint32_t bst = sbase + NearSmem::stages + b * kStageBytes;
 #pragma unroll
         for (int ks = 0; ks < 2; ks++) {
-          const uint64_t bhi = smem_desc(bst + ks * 256, 128, 512);
-          const uint64_t blo = smem_desc(bst + kStageHalf + ks * 256, 128, 512);
+          const uint32_t boff = b * kStageBytes + ks * 256;
           for (int u = 0; u < ntile; u++) {
             const uint32_t aoff = (u * kTY + 1 + dr) * kSboA + (1 + dc) * 16 + (uint32_t)(c * 4 + ks * 2) * kLboA;
-            const uint64_t ahi = smem_desc(sbase + NearSmem::hi + aoff, kLboA, kSboA);
-            const uint64_t alo = smem_desc(sbase + NearSmem::lo + aoff, kLboA, kSboA);
             const uint32_t d = tmem + 128 * u;
-            mma_f16(d, ahi, bhi, idesc, (t | ks) ? 1 : 0);
-            mma_f16(d, ahi, blo, idesc, 1);
-            mma_f16(d, alo, bhi, idesc, 1);
+            mma_f16(d, desc_add(ah0, aoff), desc_add(bh0, boff), idesc, (t | ks) ? 1 : 0);
+            mma_f16(d, desc_add(ah0, aoff), desc_add(bl0, boff), idesc, 1);
+            mma_f16(d, desc_add(al0, aoff), desc_add(bh0, boff), idesc, 1);
           }
         }
         mma_commit(&empty[b]);
@@ -306,23 +306,23 @@ __global__ void __launch_bounds__(256, 1) k_tc_near(TcNearArgs A) {
     loaders_bar();
     if (threadIdx.x == 0) {
       tc_fence_after();
+      const uint64_t ah0 = smem_desc(sbase + NearSmem::hi, 128, kSboL);
+      const uint64_t al0 = smem_desc(sbase + NearSmem::lo, 128, kSboL);
+      const uint64_t bh0 = smem_desc(sbase + NearSmem::stages, 128, 512);
+      const uint64_t bl0 = smem_desc(sbase + NearSmem::stages + kStageHalf, 128, 512);
       for (int t = kNearStages; t < nstages; t++) {
         const int b = t % kNB;
         if (!mbar_wait(&full[b], (t / kNB) & 1, A.err, kErrNearFull)) break;
         const int c = t - kNearStages;
-        const uint32_t bst = sbase + NearSmem::stages + b * kStageBytes;
 #pragma unroll
         for (int ks = 0; ks < 2; ks++) {
-          const uint64_t bhi = smem_desc(bst + ks * 256, 128, 512);
-          const uint64_t blo = smem_desc(bst + kStageHalf + ks * 256, 128, 512);
+          const uint32_t boff = b * kStageBytes + ks * 256;
           for (int u = 0; u < ntile; u++) {
             const uint32_t aoff = u * kL2pTile + (uint32_t)(c * 4 + ks * 2) * 128;
-            const uint64_t ahi = smem_desc(sbase + NearSmem::hi + aoff, 128, kSboL);
-            const uint64_t alo = smem_desc(sbase + NearSmem::lo + aoff, 128, kSboL);
             const uint32_t d = tmem + 256 + 128 * u;
-            mma_f16(d, ahi, bhi, idesc, (c | ks) ? 1 : 0);
-            mma_f16(d, ahi, blo, idesc, 1);
-            mma_f16(d, alo, bhi, idesc, 1);
+            mma_f16(d, desc_add(ah0, aoff), desc_add(bh0, boff), idesc, (c | ks) ? 1 : 0);
+            mma_f16(d, desc_add(ah0, aoff), desc_add(bl0, boff), idesc, 1);
+            mma_f16(d, desc_add(al0, aoff), desc_add(bh0, boff), idesc, 1);
           }
         }
         mma_commit(&empty[b]);
@@ -562,20 +562,20 @@ __global__ void __launch_bounds__(256, 1) k_tc_p2m(TcP2mArgs A) {
     __syncthreads();
     if (threadIdx.x == 0) {
       tc_fence_after();
-      if (ok)
+      if (ok) {
+        const uint64_t ah0 = smem_desc(sbase + P2mSmem::hi, 128, 2048);
+        const uint64_t al0 = smem_desc(sbase + P2mSmem::lo, 128, 2048);
+        const uint64_t bh0 = smem_desc(sbase + P2mSmem::b, 128, 512);
+        const uint64_t bl0 = smem_desc(sbase + P2mSmem::b + A.stage_bytes / 2, 128, 512);
         for (int c = 0; c < 4; c++)
 #pragma unroll
           for (int ks = 0; ks < 2; ks++) {
-            const uint32_t aoff = (uint32_t)(c * 4 + ks * 2) * 128;
-            const uint64_t ahi = smem_desc(sbase + P2mSmem::hi + aoff, 128, 2048);
-            const uint64_t alo = smem_desc(sbase + P2mSmem::lo + aoff, 128, 2048);
-            const uint32_t bst = sbase + P2mSmem::b + c * A.stage_bytes + ks * 256;
-            const uint64_t bhi = smem_desc(bst, 128, 512);
-            const uint64_t blo = smem_desc(bst + A.stage_bytes / 2, 128, 512);
-            mma_f16(tmem, ahi, bhi, idesc, (c | ks) ? 1 : 0);
-            mma_f16(tmem, ahi, blo, idesc, 1);
-            mma_f16(tmem, alo, bhi, idesc, 1);
+            const uint32_t aoff = (uint32_t)(c * 4 + ks * 2) * 128, boff = c * A.stage_bytes + ks * 256;
+            mma_f16(tmem, desc_add(ah0, aoff), desc_add(bh0, boff), idesc, (c | ks) ? 1 : 0);
+            mma_f16(tmem, desc_add(ah0, aoff), desc_add(bl0, boff), idesc, 1);
+            mma_f16(tmem, desc_add(al0, aoff), desc_add(bh0, boff), idesc, 1);
           }
+      }
       mma_commit(done);
     }
     // the next item's input, in flight while this one is multiplied and written

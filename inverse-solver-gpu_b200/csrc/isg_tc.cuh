@@ -80,6 +80,10 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint
   return d;                // base offset 0, relative LBO, swizzle none
 }
 
+// The descriptor of the same matrix layout `bytes` further on (bytes a multiple
+// of 16, the start address staying below 256 KB): only the start field moves.
+__device__ __forceinline__ uint64_t desc_add(uint64_t d, uint32_t bytes) { return d + (bytes >> 4); }
+
 // Instruction descriptor of kind::f16 with F16 A and B, F32 accumulation,
 // both operands K-major.
 __host__ __device__ constexpr uint32_t idesc_f16_f32(int M, int N) {

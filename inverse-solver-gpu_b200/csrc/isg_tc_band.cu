@@ -172,15 +172,16 @@ __global__ void __launch_bounds__(256, 2) k_tc_band(BandArgs A) {
     if (threadIdx.x == 0) {
       tc_fence_after();
       if (mbar_wait(abar, ch & 1, A.err, kErrBand)) {
+        const uint64_t ah = smem_desc(sbase, 128, (kKC / 8) * 128);
+        const uint64_t al = smem_desc(sbase + kAHalf, 128, (kKC / 8) * 128);
+        const uint64_t bh = smem_desc(sbase + 2 * kAHalf, 128, (kKC / 8) * 128);
+        const uint64_t bl = smem_desc(sbase + 2 * kAHalf + kBHalf, 128, (kKC / 8) * 128);
 #pragma unroll
         for (int ks = 0; ks < kKC / 16; ks++) {
-          const uint64_t ah = smem_desc(sbase + ks * 256, 128, (kKC / 8) * 128);
-          const uint64_t al = smem_desc(sbase + kAHalf + ks * 256, 128, (kKC / 8) * 128);
-          const uint64_t bh = smem_desc(sbase + 2 * kAHalf + ks * 256, 128, (kKC / 8) * 128);
-          const uint64_t bl = smem_desc(sbase + 2 * kAHalf + kBHalf + ks * 256, 128, (kKC / 8) * 128);
-          mma_f16(tmem, ah, bh, idesc, (ch | ks) ? 1 : 0);
-          mma_f16(tmem, ah, bl, idesc, 1);
-          mma_f16(tmem, al, bh, idesc, 1);
+          const uint32_t k = ks * 256;
+          mma_f16(tmem, desc_add(ah, k), desc_add(bh, k), idesc, (ch | ks) ? 1 : 0);
+          mma_f16(tmem, desc_add(ah, k), desc_add(bl, k), idesc, 1);
+          mma_f16(tmem, desc_add(al, k), desc_add(bh, k), idesc, 1);
         }
       }
       mma_commit(mbar);
@@ -237,92 +238,117 @@ constexpr int kErrL2l = 122;
 struct L2lArgs {
   float2 *loc;  // every level's locals; parent rings at off_in, child rings at off_out
   size_t mp, off_in, off_out;
-  int n_p, ns_in, ns_out, Kp, ppi;  // padded K, parents per item
-  const uint8_t *A;                 // [128 x Kp] FP16 hi then lo, K-major core matrices
-  const float2 *shl;                // [ns_in][4] local shifts of the parent level
+  int lg_np, ns_in, ns_out, Kp, ppi;  // log2 parents per side, padded K, parents per item
+  unsigned kc_magic;                  // ceil(2^32 / (Kp / 8)): division by Kp / 8 as a high multiply
+  const uint8_t *A;                   // [128 x Kp] FP16 hi then lo, K-major core matrices
+  const float2 *shl;                  // [ns_in][4] local shifts of the parent level
   float inv_a, shl_max;
   int nparents, items_per_rhs, nitems;
   const int *active;
   int *err;
 };
 
-// Shared-memory carve-up (bytes): A hi/lo, B hi/lo, staged rings [ppi][Kp]
-// float2, shifts [Kp][4] float2, barriers and scratch.
+// Shared-memory carve-up (bytes): A hi/lo; B hi/lo (8 rows per parent: 4
+// children x re, im); the item's rings staged as [parent][Kp / 8] groups of 8
+// samples, each group padded to 80 bytes; the shifts as [4][Kp + 2] float2
+// (child-major, padded); barriers and scratch.  The paddings put the groups
+// that one warp reads on distinct banks.
 struct L2lSmem {
   size_t a, b, z, sh, bar, total;
   __host__ __device__ L2lSmem(int Kp, int ppi) {
     a = 0;
     b = a + (size_t)512 * Kp;
-    z = b + (size_t)2 * (8 * ppi) * Kp * 2;
-    sh = z + (size_t)ppi * Kp * 8;
-    bar = sh + (size_t)Kp * 32;
-    total = bar + 64;
+    z = b + (size_t)32 * ppi * Kp;
+    sh = z + (size_t)10 * ppi * Kp;
+    bar = sh + (size_t)32 * (Kp + 2);
+    total = bar + 128;
   }
 };
 
-__global__ void __launch_bounds__(256, 1) k_tc_l2l(L2lArgs A) {
+// Splits (a, b), already scaled into the FP16 range, into packed hi and lo halves.
+__device__ __forceinline__ void split2(float a, float b, __half2 &hi, __half2 &lo) {
+  hi = __floats2half2_rn(a, b);
+  const float2 h = __half22float2(hi);
+  lo = __floats2half2_rn(a - h.x, b - h.y);
+}
+
+constexpr int kL2lThreads = 512;
+constexpr int kL2lConvWarps = kL2lThreads / 32 - 1;  // the last warp issues the MMAs
+constexpr int kL2lConv = 32 * kL2lConvWarps;
+
+// Named barriers 1..15 (0 is __syncthreads): sync waits for `count` threads,
+// arrive only signals.
+__device__ __forceinline__ void named_sync(int id, int count) {
+  asm volatile("bar.sync %0, %1;\n" ::"r"(id), "r"(count) : "memory");
+}
+__device__ __forceinline__ void named_arrive(int id, int count) {
+  asm volatile("bar.arrive %0, %1;\n" ::"r"(id), "r"(count) : "memory");
+}
+
+__global__ void __launch_bounds__(kL2lThreads, 1) k_tc_l2l(L2lArgs A) {
   extern __shared__ __align__(1024) char sm[];
   const L2lSmem L(A.Kp, A.ppi);
-  const int N = 8 * A.ppi, Kp = A.Kp, kc = Kp / 8;
-  char *ahi = sm + L.a, *bhi = sm + L.b, *blo = bhi + (size_t)N * Kp * 2;
-  float2 *zst = (float2 *)(sm + L.z);
+  const int N = 8 * A.ppi, Kp = A.Kp, kc = Kp / 8, NH = N / 2;
+  char *bhi = sm + L.b, *blo = bhi + (size_t)N * Kp * 2;
+  float4 *zst = (float4 *)(sm + L.z);  // 5 float4 per group of 8 samples (the fifth is padding)
   float2 *shs = (float2 *)(sm + L.sh);
   uint64_t *abar = (uint64_t *)(sm + L.bar);
-  uint64_t *done = abar + 1;
-  uint32_t *tslot = (uint32_t *)(abar + 2);
-  float *fscr = (float *)(abar + 3);  // [8]
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint64_t *done = abar + 1;  // [2]: one per column half
+  uint32_t *tslot = (uint32_t *)(abar + 3);
+  float *fscr = (float *)(abar + 4);  // [kL2lThreads / 32]
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = kL2lThreads / 32;
   if (threadIdx.x == 0) {
     mbar_init(abar, 1);
     mbar_init(done, 1);
+    mbar_init(done + 1, 1);
     fence_mbar_init();
   }
   if (warp == 0) tmem_alloc(tslot, N);
-  // shifts and the zero tails of the ring staging (cp.async never writes past ns_in)
-  for (int e = threadIdx.x; e < Kp * 4; e += blockDim.x)
-    shs[e] = (e >> 2) < A.ns_in ? __ldg(A.shl + e) : make_float2(0.f, 0.f);
-  for (int e = threadIdx.x; e < A.ppi * (Kp - A.ns_in); e += blockDim.x) {
-    const int pl = e / (Kp - A.ns_in), j = A.ns_in + e % (Kp - A.ns_in);
-    zst[pl * Kp + j] = make_float2(0.f, 0.f);
+  for (int e = threadIdx.x; e < 4 * (Kp + 2); e += blockDim.x) {
+    const int q = e / (Kp + 2), j = e - q * (Kp + 2);
+    shs[e] = j < A.ns_in ? __ldg(A.shl + 4 * j + q) : make_float2(0.f, 0.f);
   }
+  const int ngroups = A.ppi * kc;
+  for (int e = threadIdx.x; e < 5 * ngroups; e += blockDim.x) zst[e] = make_float4(0.f, 0.f, 0.f, 0.f);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tslot;
   if (threadIdx.x == 0) {
     mbar_expect_tx(abar, 512 * Kp);
-    bulk_g2s(ahi, A.A, 512 * Kp, abar);
+    bulk_g2s(sm + L.a, A.A, 512 * Kp, abar);
   }
   auto active_item = [&](int w) {
     while (w < A.nitems && A.active && !A.active[w / A.items_per_rhs]) w += gridDim.x;
     return w;
   };
-  // an item's parent rings into the staging buffer, 16 bytes per copy
+  // an item's parent rings into the staging groups, 16 bytes (2 samples) per copy
   const int pieces = A.ns_in / 2;
-  auto stage = [&](int w) {
+  auto stage = [&](int w, int t, int nt) {
     const int rhs = w / A.items_per_rhs, p0 = (w % A.items_per_rhs) * A.ppi;
     const float2 *base = A.loc + (size_t)rhs * A.mp + A.off_in;
-    for (int e = threadIdx.x; e < A.ppi * pieces; e += blockDim.x) {
-      const int pl = e / pieces, c = e - pl * pieces, P = p0 + pl;
+    for (int pl = t >> 5; pl < A.ppi; pl += nt >> 5) {
+      const int P = p0 + pl;
       const bool ok = P < A.nparents;
-      cp_async16z(zst + pl * Kp + 2 * c, base + (size_t)(ok ? P : 0) * A.ns_in + 2 * c, ok);
+      const float2 *ring = base + (size_t)(ok ? P : 0) * A.ns_in;
+      for (int c = lane; c < pieces; c += 32) cp_async16z(zst + (pl * kc + (c >> 2)) * 5 + (c & 3), ring + 2 * c, ok);
     }
   };
   const uint32_t sbase = smem_u32(sm);
-  const uint32_t idesc = idesc_f16_f32(128, N);
+  const uint32_t idesc = idesc_f16_f32(128, NH);
   const uint32_t sbo = (uint32_t)kc * 128;
+  const int nc = 2 << A.lg_np, npm = (1 << A.lg_np) - 1;
   bool ok = mbar_wait(abar, 0, A.err, kErrL2l);
   int parity = 0;
   int w = active_item(blockIdx.x);
-  if (w < A.nitems) stage(w);
+  if (w < A.nitems) stage(w, threadIdx.x, kL2lThreads);
   cp_async_wait_all();
   __syncthreads();
   while (w < A.nitems) {
     // power-of-two scale of this item's shifted rings
     float mx = 0.f;
-    for (int e = threadIdx.x; e < A.ppi * pieces; e += blockDim.x) {
-      const int pl = e / pieces, c = e - pl * pieces;
-      const float4 v = *(const float4 *)(zst + pl * Kp + 2 * c);
+    for (int e = threadIdx.x; e < 5 * ngroups; e += blockDim.x) {
+      const float4 v = zst[e];
       mx = fmaxf(mx, fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w))));
     }
 #pragma unroll
@@ -330,71 +356,112 @@ __global__ void __launch_bounds__(256, 1) k_tc_l2l(L2lArgs A) {
     if (lane == 0) fscr[warp] = mx;
     __syncthreads();
     float m2 = 0.f;
-    for (int k = 0; k < 8; k++) m2 = fmaxf(m2, fscr[k]);
+    for (int k = 0; k < nwarps; k++) m2 = fmaxf(m2, fscr[k]);
     const float s = pow2_scale(1.5f * A.shl_max * m2);
-    // B operand: row n = 8 parent + 2 q + c holds component c of shl[q][j] z[j] s;
-    // a unit is one row of one core matrix (8 samples), 8 consecutive threads fill it
-    for (int u = threadIdx.x; u < A.ppi * Kp; u += blockDim.x) {
-      const int r = u & 7, cm = u >> 3, pl = cm / kc, j0 = (cm - pl * kc) * 8;
-      const int q = r >> 1, c = r & 1;
-      float v[8];
-#pragma unroll
-      for (int e = 0; e < 8; e++) {
-        const float2 z = zst[pl * Kp + j0 + e], sh = shs[(j0 + e) * 4 + q];
-        v[e] = c ? fmaf(sh.x, z.y, sh.y * z.x) : fmaf(sh.x, z.x, -sh.y * z.y);
-      }
-      __align__(16) __half h[8], l[8];
-#pragma unroll
-      for (int e = 0; e < 8; e++) split_f16(v[e] * s, h[e], l[e]);
-      *(uint4 *)(bhi + (size_t)cm * 128 + r * 16) = *(uint4 *)h;
-      *(uint4 *)(blo + (size_t)cm * 128 + r * 16) = *(uint4 *)l;
-    }
-    fence_proxy_async();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      tc_fence_after();
-      if (ok)
-        for (int ks = 0; ks < Kp / 16; ks++) {
-          const uint64_t ah = smem_desc(sbase + (uint32_t)L.a + ks * 256, 128, sbo);
-          const uint64_t al = smem_desc(sbase + (uint32_t)L.a + 256 * Kp + ks * 256, 128, sbo);
-          const uint64_t bh = smem_desc(smem_u32(bhi) + ks * 256, 128, sbo);
-          const uint64_t bl = smem_desc(smem_u32(blo) + ks * 256, 128, sbo);
-          mma_f16(tmem, ah, bh, idesc, ks ? 1 : 0);
-          mma_f16(tmem, ah, bl, idesc, 1);
-          mma_f16(tmem, al, bh, idesc, 1);
-        }
-      mma_commit(done);
-    }
-    // the next item's rings, in flight while this one is multiplied and written
-    const int rhs = w / A.items_per_rhs, p0 = (w % A.items_per_rhs) * A.ppi;
     const int nxt = active_item(w + gridDim.x);
-    if (nxt < A.nitems) stage(nxt);
-    ok = mbar_wait(done, parity, A.err, kErrL2l) && ok;
-    parity ^= 1;
-    tc_fence_after();
-    // epilogue: lane = child sample, 16 columns = 2 parents x 4 children x (re, im)
+    if (warp < kL2lConvWarps) {
+      // B rows 8 parent + 2 q + (re, im) = shl[q][j] z[j] s.  A unit is one child q
+      // of one core-matrix group (8 samples of one parent): both rows, hi and lo.
+      // Each thread keeps two units in flight; each finished half is handed to
+      // the MMA warp through a named barrier it only arrives at.
+      const int ct = threadIdx.x;
+      for (int h = 0; h < 2; h++) {
+        const int u0 = h * 2 * ngroups, u1 = u0 + 2 * ngroups;
+        for (int ub = u0 + ct; ub < u1; ub += 2 * kL2lConv) {
+          float4 zv[2][4], sv[2][4];
+          int cmk[2], qk[2];
+#pragma unroll
+          for (int k = 0; k < 2; k++) {
+            const int u = min(ub + k * kL2lConv, u1 - 1);
+            qk[k] = u & 3;
+            cmk[k] = u >> 2;
+            const int j0 = 8 * (cmk[k] - (int)__umulhi((unsigned)cmk[k], A.kc_magic) * kc);
+            const float4 *sp = (const float4 *)(shs + qk[k] * (Kp + 2) + j0);
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+              zv[k][i] = zst[cmk[k] * 5 + i];
+              sv[k][i] = sp[i];
+            }
+          }
+#pragma unroll
+          for (int k = 0; k < 2; k++) {
+            __half2 hr[4], lr[4], hm[4], lm[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+              const float4 z = zv[k][i], sh = sv[k][i];
+              const float re0 = fmaf(sh.x, z.x, -sh.y * z.y), im0 = fmaf(sh.x, z.y, sh.y * z.x);
+              const float re1 = fmaf(sh.z, z.z, -sh.w * z.w), im1 = fmaf(sh.z, z.w, sh.w * z.z);
+              split2(re0 * s, re1 * s, hr[i], lr[i]);
+              split2(im0 * s, im1 * s, hm[i], lm[i]);
+            }
+            if (ub + k * kL2lConv < u1) {
+              const size_t o = (size_t)cmk[k] * 128 + qk[k] * 32;
+              *(uint4 *)(bhi + o) = *(uint4 *)hr;
+              *(uint4 *)(bhi + o + 16) = *(uint4 *)hm;
+              *(uint4 *)(blo + o) = *(uint4 *)lr;
+              *(uint4 *)(blo + o + 16) = *(uint4 *)lm;
+            }
+          }
+        }
+        fence_proxy_async();
+        named_arrive(1 + h, kL2lThreads);
+      }
+      // every unit is converted: the staging buffer takes the next item's rings
+      named_sync(3, kL2lConv);
+      if (nxt < A.nitems) stage(nxt, ct, kL2lConv);
+    } else {
+      // the MMA warp: one elected lane issues each half once it is converted
+      for (int h = 0; h < 2; h++) {
+        named_sync(1 + h, kL2lThreads);
+        if (lane == 0) {
+          tc_fence_after();
+          if (ok) {
+            const uint32_t bo = (uint32_t)h * 8 * A.ppi * Kp;  // bytes of one half of B
+            const uint64_t ah = smem_desc(sbase + (uint32_t)L.a, 128, sbo);
+            const uint64_t al = smem_desc(sbase + (uint32_t)L.a + 256 * Kp, 128, sbo);
+            const uint64_t bh = smem_desc(smem_u32(bhi) + bo, 128, sbo);
+            const uint64_t bl = smem_desc(smem_u32(blo) + bo, 128, sbo);
+            const uint32_t d = tmem + (uint32_t)(h * NH);
+            for (int ks = 0; ks < Kp / 16; ks++) {
+              const uint32_t k = ks * 256;
+              mma_f16(d, desc_add(ah, k), desc_add(bh, k), idesc, ks ? 1 : 0);
+              mma_f16(d, desc_add(ah, k), desc_add(bl, k), idesc, 1);
+              mma_f16(d, desc_add(al, k), desc_add(bh, k), idesc, 1);
+            }
+          }
+          mma_commit(done + h);
+        }
+        __syncwarp();
+      }
+    }
+    const int rhs = w / A.items_per_rhs, p0 = (w % A.items_per_rhs) * A.ppi;
+    // epilogue per half: lane = child sample, 16 columns = 2 parents x 4 children x (re, im);
+    // warp = (column quarter, lane quarter)
     const float inv = A.inv_a / s;
-    const int qd = warp & 3, hcol = warp >> 2, km = 32 * qd + lane;
-    const int nch = N / 32;  // 16-column chunks per warp
+    const int qd = warp & 3, cq = warp >> 2, km = 32 * qd + lane;
     float2 *obase = A.loc + (size_t)rhs * A.mp + A.off_out + km;
-    const int nc = 2 * A.n_p;
-    for (int ch = 0; ch < nch; ch++) {
-      const int col0 = hcol * (N / 2) + 16 * ch;
-      float d[16];
-      tmem_ld16(tmem + ((uint32_t)(32 * qd) << 16) + col0, d);
-      if (!ok || km >= A.ns_out) continue;
+    const int so = A.ns_out, qoff[4] = {0, so, nc * so, nc * so + so};
+    for (int h = 0; h < 2; h++) {
+      ok = mbar_wait(done + h, parity, A.err, kErrL2l) && ok;
+      tc_fence_after();
+      for (int ch = 0; ch < NH / 64; ch++) {
+        const int col0 = h * NH + cq * (NH / 4) + 16 * ch;
+        float d[16];
+        tmem_ld16(tmem + ((uint32_t)(32 * qd) << 16) + col0, d);
+        if (!ok || km >= A.ns_out) continue;
 #pragma unroll
-      for (int u = 0; u < 2; u++) {
-        const int P = p0 + col0 / 8 + u;
-        if (P >= A.nparents) continue;
-        const int py = P / A.n_p, px = P - py * A.n_p;
+        for (int u = 0; u < 2; u++) {
+          const int P = p0 + col0 / 8 + u;
+          if (P >= A.nparents) continue;
+          const int py = P >> A.lg_np, px = P & npm;
+          const int base = (2 * py * nc + 2 * px) * so;
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-          const size_t cl = (size_t)(2 * py + (q >> 1)) * nc + 2 * px + (q & 1);
-          obase[cl * A.ns_out] = make_float2(d[8 * u + 2 * q] * inv, d[8 * u + 2 * q + 1] * inv);
+          for (int q = 0; q < 4; q++)
+            obase[base + qoff[q]] = make_float2(d[8 * u + 2 * q] * inv, d[8 * u + 2 * q + 1] * inv);
         }
       }
     }
+    parity ^= 1;
     cp_async_wait_all();
     tc_fence_before();
     __syncthreads();  // staging, B and TMEM are reused by the next item
@@ -409,6 +476,7 @@ __global__ void __launch_bounds__(256, 1) k_tc_l2l(L2lArgs A) {
 struct L2lPlan {
   uint8_t *A = nullptr;  // device
   int Kp = 0, ppi = 0;
+  unsigned kc_magic = 0;
   float inv_a = 1, shl_max = 1;
   bool ok = false;
 };
@@ -457,7 +525,7 @@ static isg_status build_l2l(isg_ctx *c, int i, size_t smem_cap) {
   if (ns_out > 128) return ISG_OK;
   const int Kp = (ns_in + 15) / 16 * 16;
   int ppi = 0;
-  for (int cand : {32, 16, 8})
+  for (int cand : {32, 16})
     if (L2lSmem(Kp, cand).total <= smem_cap) {
       ppi = cand;
       break;
@@ -492,6 +560,11 @@ static isg_status build_l2l(isg_ctx *c, int i, size_t smem_cap) {
   if ((e = cuda_check(c, cudaMalloc(&T.A, buf.size()), "l2l alloc")) != ISG_OK) return e;
   if ((e = cuda_check(c, cudaMemcpy(T.A, buf.data(), buf.size(), cudaMemcpyHostToDevice), "l2l upload")) != ISG_OK)
     return e;
+  const unsigned kc = (unsigned)(Kp / 8);
+  const unsigned magic = (unsigned)((((unsigned long long)1 << 32) + kc - 1) / kc);
+  for (unsigned cm = 0; cm < (unsigned)(ppi * Kp / 8); cm++)
+    if ((unsigned)(((unsigned long long)cm * magic) >> 32) != cm / kc) return ISG_OK;  // not exact: SIMT L2L
+  T.kc_magic = magic;
   T.Kp = Kp;
   T.ppi = ppi;
   T.inv_a = (float)(1.0 / sa);
@@ -667,10 +740,12 @@ bool band_l2l(isg_ctx *c, int lvl, float2 *loc, int nrhs, const int *active, cud
   A.mp = c->P.mp;
   A.off_in = p.off;
   A.off_out = ch.off;
-  A.n_p = p.n;
+  A.lg_np = 0;
+  while ((1 << A.lg_np) < p.n) A.lg_np++;
   A.ns_in = p.ns;
   A.ns_out = ch.ns;
   A.Kp = T.Kp;
+  A.kc_magic = T.kc_magic;
   A.ppi = T.ppi;
   A.A = T.A;
   A.shl = p.shlT;
@@ -682,7 +757,7 @@ bool band_l2l(isg_ctx *c, int lvl, float2 *loc, int nrhs, const int *active, cud
   A.active = active;
   A.err = c->tc_err_flag();
   count_launch();
-  k_tc_l2l<<<std::min(A.nitems, c->band->sms), 256, L2lSmem(T.Kp, T.ppi).total, st>>>(A);
+  k_tc_l2l<<<std::min(A.nitems, c->band->sms), kL2lThreads, L2lSmem(T.Kp, T.ppi).total, st>>>(A);
   *e = cuda_check(c, cudaGetLastError(), "l2l launch");
   return true;
 }
