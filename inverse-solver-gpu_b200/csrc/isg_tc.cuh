@@ -39,6 +39,23 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *e
   return false;
 }
 
+// The same wait, also giving up (without raising the flag again) once another
+// role of the CTA has set *abort; on expiry it sets *abort itself.
+__device__ __forceinline__ bool mbar_wait_or(uint64_t *bar, uint32_t parity, volatile int *abort, int *err, int code,
+                                             long limit = 20000000L) {
+  for (long i = 0; i < limit; i++) {
+    if (mbar_test(bar, parity)) return true;
+    if (*abort) return false;
+    if (i > 64) __nanosleep(32);
+  }
+  *abort = 1;
+  if (err) atomicExch(err, code);
+  return false;
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+
 // 16-byte asynchronous global -> shared copy; zero-fills when !valid.
 __device__ __forceinline__ void cp_async16z(void *smem, const void *gmem, bool valid) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(smem)), "l"(gmem),

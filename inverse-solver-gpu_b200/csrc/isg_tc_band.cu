@@ -472,6 +472,255 @@ __global__ void __launch_bounds__(kL2lThreads, 1) k_tc_l2l(L2lArgs A) {
   if (warp == 0) tmem_dealloc(tmem, N);
 }
 
+// ---- M2M, persistent, for parents of at most 128 samples ----
+// The same shape as the L2L kernel, transposed roles: A = the interpolation
+// matrix [128 parent samples x Kp child samples] resident in shared memory;
+// an item is 32 (or 16) parents of one RHS, B rows 8 parent + 2 q + (re, im)
+// hold child q's ring (the children's own samples, no shift before the
+// product), and the epilogue forms sum_q shm[q][k] D_q[k] for each parent
+// sample k on its lane.  The operand scale comes from the child level's
+// maximum per RHS (written by the kernel that produced the children), and the
+// kernel writes the parent level's maximum for the next transition.
+constexpr int kErrM2m = 123;
+
+struct M2mArgs {
+  float2 *mul;  // every level's multipoles; children at off_in, parents at off_out
+  size_t mp, off_in, off_out;
+  int lg_np, ns_in, ns_out, Kp, ppi;
+  unsigned kc_magic;
+  const uint8_t *A;    // [128 x Kp] FP16 hi then lo
+  const float2 *shm;   // [4][ns_out] multipole shifts of the parent level
+  float inv_a;
+  int nparents, items_per_rhs, nitems;
+  const int *active;
+  int *err;
+  unsigned *levmax;
+  int lvl_in, lvl_out;
+};
+
+// Pipelined over items in three roles, each item's buffers alternating
+// between two sets: converter warps turn staged rings into B[b] while the MMA
+// warp multiplies B[1-b] into TMEM accumulator 1-b and the epilogue warps
+// drain the accumulator of the item before.  Hand-offs are mbarriers:
+// zfull (bulk copies landed), bfull / bfree (operand written / consumed),
+// tfull / tfree (accumulator written / read out).  Every wait is bounded and
+// gives up once any role has given up.
+constexpr int kPipeConvWarps = 7;  // warps 0..6
+constexpr int kPipeMmaWarp = 7;    // warp 7
+constexpr int kPipeEpiWarp0 = 8;   // warps 8..15
+constexpr int kPipeConv = 32 * kPipeConvWarps;
+constexpr int kPipeEpi = kL2lThreads - 32 * kPipeEpiWarp0;
+
+// A hi/lo; B[2] hi/lo; staged child rings [2][2 rows][2 ppi clusters][ns]
+// (the item's parents are consecutive in one row, so each child row is one
+// contiguous run), each buffer followed by Kp zero samples; barriers and flags.
+struct M2mSmem {
+  size_t a, b, bbuf, z, zbuf, bar, total;
+  __host__ __device__ M2mSmem(int Kp, int ppi, int ns) {
+    a = 0;
+    b = a + (size_t)512 * Kp;
+    bbuf = (size_t)32 * ppi * Kp;
+    z = b + 2 * bbuf;
+    zbuf = ((size_t)(4 * ppi * ns + Kp) * 8 + 127) & ~(size_t)127;
+    bar = z + 2 * zbuf;
+    total = bar + 256;
+  }
+};
+
+__global__ void __launch_bounds__(kL2lThreads, 1) k_tc_m2m(M2mArgs A) {
+  extern __shared__ __align__(1024) char sm[];
+  const M2mSmem L(A.Kp, A.ppi, A.ns_in);
+  const int N = 8 * A.ppi, Kp = A.Kp, kc = Kp / 8, zs = A.ns_in;
+  uint64_t *bars = (uint64_t *)(sm + L.bar);
+  uint64_t *abar = bars, *zfull = bars + 1, *bfull = bars + 3, *bfree = bars + 5, *tfull = bars + 7,
+           *tfree = bars + 9;
+  uint32_t *tslot = (uint32_t *)(bars + 11);
+  volatile int *abort = (volatile int *)(bars + 12);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  auto bbuf = [&](int b) { return sm + L.b + b * L.bbuf; };  // hi, then lo N * Kp * 2 bytes on
+  auto zbuf = [&](int b) { return (float2 *)(sm + L.z + b * L.zbuf); };
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < 11; i++) mbar_init(bars + i, 1);
+    *abort = 0;
+    fence_mbar_init();
+  }
+  if (warp == 0) tmem_alloc(tslot, 2 * N);
+  // zero both buffers: the tails past the last ring are read (against zero weights) and stay 0
+  for (int e = threadIdx.x; e < (int)(2 * L.zbuf / 4); e += blockDim.x) ((float *)zbuf(0))[e] = 0.f;
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+  auto next_item = [&](int w) {
+    do w += gridDim.x;
+    while (w < A.nitems && A.active && !A.active[w / A.items_per_rhs]);
+    return w;
+  };
+  const int first = (A.active && !A.active[blockIdx.x / A.items_per_rhs]) ? next_item(blockIdx.x) : blockIdx.x;
+  auto scale_of = [&](int w) {
+    return pow2_scale(__uint_as_float(A.levmax[(w / A.items_per_rhs) * kMaxLevels + A.lvl_in]));
+  };
+  const int nc = 2 << A.lg_np, npm = (1 << A.lg_np) - 1;
+  const uint32_t ring_bytes = (uint32_t)A.ns_in * 8;
+  // an item's children: two contiguous runs of 2 ppi rings (child rows 2 py, 2 py + 1)
+  auto stage = [&](int w, int b) {
+    if (lane != 0) return;
+    const int rhs = w / A.items_per_rhs, P = (w % A.items_per_rhs) * A.ppi;
+    const int py = P >> A.lg_np, px = P & npm;
+    const float2 *base = A.mul + (size_t)rhs * A.mp + A.off_in;
+    const uint32_t run = 2 * A.ppi * ring_bytes;
+    mbar_expect_tx(zfull + b, 2 * run);
+    for (int qy = 0; qy < 2; qy++)
+      bulk_g2s(zbuf(b) + qy * 2 * A.ppi * zs, base + ((size_t)(2 * py + qy) * nc + 2 * px) * A.ns_in, run, zfull + b);
+  };
+  const int ngroups = A.ppi * kc;  // core-matrix groups of B (8 rows x 8 samples)
+
+  if (warp < kPipeConvWarps) {
+    // ---- converters: B[b] rows 8 parent + 2 q + (re, im) = child q's samples times s ----
+    if (warp == 0) {
+      if (lane == 0) {
+        mbar_expect_tx(abar, 512 * Kp);
+        bulk_g2s(sm + L.a, A.A, 512 * Kp, abar);
+      }
+      __syncwarp();
+      if (first < A.nitems) stage(first, 0);
+      const int second = first < A.nitems ? next_item(first) : A.nitems;
+      if (second < A.nitems) stage(second, 1);
+    }
+    int w = first, w2 = first < A.nitems ? next_item(next_item(first)) : A.nitems;
+    for (int it = 0; w < A.nitems; it++) {
+      const int b = it & 1, ph = (it >> 1) & 1;
+      const bool zok = mbar_wait_or(zfull + b, ph, abort, A.err, kErrM2m);
+      const bool bok = mbar_wait_or(bfree + b, ph ^ 1, abort, A.err, kErrM2m);
+      const float s = scale_of(w);
+      const float2 *zst = zbuf(b);
+      char *bhi = bbuf(b), *blo = bhi + (size_t)N * Kp * 2;
+      if (zok && bok) {
+        for (int ub = threadIdx.x; ub < 4 * ngroups; ub += 2 * kPipeConv) {
+          float4 zv[2][4];
+          int cmk[2], qk[2];
+#pragma unroll
+          for (int k = 0; k < 2; k++) {
+            const int u = min(ub + k * kPipeConv, 4 * ngroups - 1);
+            qk[k] = u & 3;
+            cmk[k] = u >> 2;
+            const int pl = (int)__umulhi((unsigned)cmk[k], A.kc_magic), j8 = cmk[k] - pl * kc;
+            const int slot = (qk[k] >> 1) * 2 * A.ppi + 2 * pl + (qk[k] & 1);
+            const float4 *zp = (const float4 *)(zst + slot * zs + 8 * j8);
+#pragma unroll
+            for (int i = 0; i < 4; i++) zv[k][i] = zp[i];
+          }
+#pragma unroll
+          for (int k = 0; k < 2; k++) {
+            __half2 hr[4], lr[4], hm[4], lm[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+              const float4 z = zv[k][i];
+              split2(z.x * s, z.z * s, hr[i], lr[i]);
+              split2(z.y * s, z.w * s, hm[i], lm[i]);
+            }
+            if (ub + k * kPipeConv < 4 * ngroups) {
+              const size_t o = (size_t)cmk[k] * 128 + qk[k] * 32;
+              *(uint4 *)(bhi + o) = *(uint4 *)hr;
+              *(uint4 *)(bhi + o + 16) = *(uint4 *)hm;
+              *(uint4 *)(blo + o) = *(uint4 *)lr;
+              *(uint4 *)(blo + o + 16) = *(uint4 *)lm;
+            }
+          }
+        }
+      }
+      fence_proxy_async();
+      named_sync(1, kPipeConv);  // every converter is done with zbuf(b) and B[b]
+      if (threadIdx.x == 0) mbar_arrive(bfull + b);
+      if (warp == 0 && w2 < A.nitems) stage(w2, b);
+      w = next_item(w);
+      w2 = w2 < A.nitems ? next_item(w2) : A.nitems;
+    }
+  } else if (warp == kPipeMmaWarp) {
+    // ---- MMA issue ----
+    const uint32_t idesc = idesc_f16_f32(128, N);
+    const uint32_t sbo = (uint32_t)kc * 128, sbase = smem_u32(sm);
+    const uint64_t ah = smem_desc(sbase + (uint32_t)L.a, 128, sbo);
+    const uint64_t al = smem_desc(sbase + (uint32_t)L.a + 256 * Kp, 128, sbo);
+    const bool aok = mbar_wait_or(abar, 0, abort, A.err, kErrM2m);
+    int w = first;
+    for (int it = 0; w < A.nitems; it++) {
+      const int b = it & 1, ph = (it >> 1) & 1;
+      const bool ok = mbar_wait_or(bfull + b, ph, abort, A.err, kErrM2m) &&
+                      mbar_wait_or(tfree + b, ph ^ 1, abort, A.err, kErrM2m) && aok;
+      if (lane == 0) {
+        tc_fence_after();
+        if (ok) {
+          const uint64_t bh = smem_desc(smem_u32(bbuf(b)), 128, sbo);
+          const uint64_t bl = smem_desc(smem_u32(bbuf(b)) + N * Kp * 2, 128, sbo);
+          const uint32_t d = tmem + (uint32_t)(b * N);
+          for (int ks = 0; ks < Kp / 16; ks++) {
+            const uint32_t k = ks * 256;
+            mma_f16(d, desc_add(ah, k), desc_add(bh, k), idesc, ks ? 1 : 0);
+            mma_f16(d, desc_add(ah, k), desc_add(bl, k), idesc, 1);
+            mma_f16(d, desc_add(al, k), desc_add(bh, k), idesc, 1);
+          }
+        }
+        mma_commit(bfree + b);
+        mma_commit(tfull + b);
+      }
+      __syncwarp();
+      w = next_item(w);
+    }
+  } else {
+    // ---- epilogue: lane = parent sample, 16 columns = 2 parents x 4 children x (re, im) ----
+    const int ew = warp - kPipeEpiWarp0, qd = ew & 3, ch0 = ew >> 2;  // lane quarter, column half
+    const int km = 32 * qd + lane;
+    float2 shq[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) shq[q] = km < A.ns_out ? __ldg(A.shm + q * A.ns_out + km) : make_float2(0.f, 0.f);
+    int w = first;
+    for (int it = 0; w < A.nitems; it++) {
+      const int b = it & 1, ph = (it >> 1) & 1;
+      const bool ok = mbar_wait_or(tfull + b, ph, abort, A.err, kErrM2m);
+      tc_fence_after();
+      const int rhs = w / A.items_per_rhs, p0 = (w % A.items_per_rhs) * A.ppi;
+      const float inv = A.inv_a / scale_of(w);
+      float2 *obase = A.mul + (size_t)rhs * A.mp + A.off_out + km;
+      float omx = 0.f;
+      for (int ch = 0; ch < N / 32; ch++) {
+        const int col0 = ch0 * (N / 2) + 16 * ch;
+        float d[16];
+        tmem_ld16(tmem + ((uint32_t)(32 * qd) << 16) + (uint32_t)(b * N + col0), d);
+        if (!ok || km >= A.ns_out) continue;
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+          const int P = p0 + col0 / 8 + u;
+          float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+          for (int q = 0; q < 4; q++)
+            cfma(acc, shq[q], make_float2(d[8 * u + 2 * q] * inv, d[8 * u + 2 * q + 1] * inv));
+          obase[(size_t)P * A.ns_out] = acc;
+          omx = fmaxf(omx, fmaxf(fabsf(acc.x), fabsf(acc.y)));
+        }
+      }
+      tc_fence_before();
+      named_sync(2, kPipeEpi);  // the accumulator is read out
+      if (ew == 0 && lane == 0) mbar_arrive(tfree + b);
+      // the parent level's maximum for the next transition (omx >= 0: bits order as values)
+      const unsigned mbits = __reduce_max_sync(0xffffffffu, __float_as_uint(omx));
+      if (lane == 0 && ok && mbits) atomicMax(&A.levmax[rhs * kMaxLevels + A.lvl_out], mbits);
+      w = next_item(w);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, 2 * N);
+}
+
+struct M2mPlan {
+  uint8_t *A = nullptr;  // device
+  int Kp = 0, ppi = 0;
+  unsigned kc_magic = 0;
+  float inv_a = 1;
+  bool ok = false;
+};
+
 // One L2L transition on the tensor cores (child level `lvl`).
 struct L2lPlan {
   uint8_t *A = nullptr;  // device
@@ -510,10 +759,73 @@ void pack_chunk(std::vector<uint8_t> &buf, size_t at, int k0, double scale, F re
 
 struct BandPlan {
   Transition m2m[kMaxLevels];  // indexed by parent level
+  M2mPlan pm2m[kMaxLevels];    // persistent M2M, indexed by parent level
   L2lPlan l2l[kMaxLevels];     // indexed by child level
   std::vector<void *> allocs;
   int sms = 148;
 };
+
+// Packs a dense [128 x Kp] real matrix as FP16 hi then lo (K-major core
+// matrices) after a power-of-two scale; returns the inverse of the scale.
+static double pack_resident(const std::vector<double> &dense, int Kp, std::vector<uint8_t> &buf) {
+  double mw = 0;
+  for (double v : dense) mw = std::max(mw, std::abs(v));
+  int e2;
+  std::frexp(mw > 0 ? mw : 1.0, &e2);
+  const double sa = std::ldexp(1.0, 14 - e2);
+  buf.assign((size_t)512 * Kp, 0);
+  __half *hi = (__half *)buf.data(), *lo = (__half *)(buf.data() + (size_t)256 * Kp);
+  for (int m = 0; m < 128; m++)
+    for (int k = 0; k < Kp; k++) {
+      const double v = dense[(size_t)m * Kp + k] * sa;
+      const __half h = __double2half(v);
+      const __half l = __double2half(v - (double)__half2float(h));
+      const size_t idx = ((size_t)(m / 8) * (Kp / 8) + k / 8) * 64 + (m % 8) * 8 + (k % 8);
+      hi[idx] = h;
+      lo[idx] = l;
+    }
+  return 1.0 / sa;
+}
+
+// ceil(2^32 / kc), if it divides exactly for every group index below `count`.
+static bool kc_magic(unsigned kc, unsigned count, unsigned *magic) {
+  const unsigned m = (unsigned)((((unsigned long long)1 << 32) + kc - 1) / kc);
+  for (unsigned cm = 0; cm < count; cm++)
+    if ((unsigned)(((unsigned long long)cm * m) >> 32) != cm / kc) return false;
+  *magic = m;
+  return true;
+}
+
+// The persistent M2M into parent level i (ns_i <= 128): the interpolation
+// matrix [parent sample x child sample] resident in shared memory.
+static isg_status build_m2m(isg_ctx *c, int i, size_t smem_cap) {
+  const HostTables &H = c->T;
+  const int ns_out = H.nsamp[i], ns_in = H.nsamp[i + 1], ni = H.ninter;
+  M2mPlan &T = c->band->pm2m[i];
+  if (ns_out > 128) return ISG_OK;
+  const int Kp = (ns_in + 15) / 16 * 16;
+  int ppi = 0;
+  for (int cand : {32, 16})
+    if (M2mSmem(Kp, cand, ns_in).total <= smem_cap && (1 << i) >= cand) {
+      ppi = cand;
+      break;
+    }
+  const int nparents = 1 << (2 * i);
+  if (!ppi || nparents % ppi || !kc_magic(Kp / 8, (unsigned)(ppi * Kp / 8), &T.kc_magic)) return ISG_OK;
+  std::vector<double> dense((size_t)128 * Kp, 0.0);
+  for (int k = 0; k < ns_out; k++)
+    for (int t = 0; t < ni; t++) dense[(size_t)k * Kp + H.intind[i][(size_t)k * ni + t]] += H.interp[i][(size_t)k * ni + t];
+  std::vector<uint8_t> buf;
+  T.inv_a = (float)pack_resident(dense, Kp, buf);
+  isg_status e;
+  if ((e = cuda_check(c, cudaMalloc(&T.A, buf.size()), "m2m alloc")) != ISG_OK) return e;
+  if ((e = cuda_check(c, cudaMemcpy(T.A, buf.data(), buf.size(), cudaMemcpyHostToDevice), "m2m upload")) != ISG_OK)
+    return e;
+  T.Kp = Kp;
+  T.ppi = ppi;
+  T.ok = true;
+  return ISG_OK;
+}
 
 // The [128 x Kp] anterpolation matrix of child level i (rows: child samples,
 // columns: parent samples) as FP16 hi then lo in the K-major core-matrix
@@ -533,41 +845,22 @@ static isg_status build_l2l(isg_ctx *c, int i, size_t smem_cap) {
   const int nparents = 1 << (2 * (i - 1));
   if (!ppi || nparents % ppi) return ISG_OK;
   std::vector<double> dense((size_t)128 * Kp, 0.0);
-  double mw = 0;
   for (int k = 0; k < ns_out; k++)
     for (int t = 0; t < taps; t++) {
       const int j = H.antind[i][(size_t)k * W + t];
       dense[(size_t)k * Kp + j] += H.anterp[i][(size_t)k * W + t];
     }
-  for (double v : dense) mw = std::max(mw, std::abs(v));
-  int e2;
-  std::frexp(mw > 0 ? mw : 1.0, &e2);
-  const double sa = std::ldexp(1.0, 14 - e2);
-  std::vector<uint8_t> buf((size_t)512 * Kp, 0);
-  __half *hi = (__half *)buf.data(), *lo = (__half *)(buf.data() + (size_t)256 * Kp);
-  for (int m = 0; m < 128; m++)
-    for (int k = 0; k < Kp; k++) {
-      const double v = dense[(size_t)m * Kp + k] * sa;
-      const __half h = __double2half(v);
-      const __half l = __double2half(v - (double)__half2float(h));
-      const size_t idx = ((size_t)(m / 8) * (Kp / 8) + k / 8) * 64 + (m % 8) * 8 + (k % 8);
-      hi[idx] = h;
-      lo[idx] = l;
-    }
+  if (!kc_magic(Kp / 8, (unsigned)(ppi * Kp / 8), &T.kc_magic)) return ISG_OK;
+  std::vector<uint8_t> buf;
+  T.inv_a = (float)pack_resident(dense, Kp, buf);
   double smax = 0;
   for (const cd &z : H.shiftloc[i - 1]) smax = std::max(smax, std::abs(z));
   isg_status e;
   if ((e = cuda_check(c, cudaMalloc(&T.A, buf.size()), "l2l alloc")) != ISG_OK) return e;
   if ((e = cuda_check(c, cudaMemcpy(T.A, buf.data(), buf.size(), cudaMemcpyHostToDevice), "l2l upload")) != ISG_OK)
     return e;
-  const unsigned kc = (unsigned)(Kp / 8);
-  const unsigned magic = (unsigned)((((unsigned long long)1 << 32) + kc - 1) / kc);
-  for (unsigned cm = 0; cm < (unsigned)(ppi * Kp / 8); cm++)
-    if ((unsigned)(((unsigned long long)cm * magic) >> 32) != cm / kc) return ISG_OK;  // not exact: SIMT L2L
-  T.kc_magic = magic;
   T.Kp = Kp;
   T.ppi = ppi;
-  T.inv_a = (float)(1.0 / sa);
   T.shl_max = (float)std::max(smax, 1e-30);
   T.ok = true;
   return ISG_OK;
@@ -672,6 +965,11 @@ isg_status band_setup(isg_ctx *c) {
   const size_t cap = (size_t)optin - fa.sharedSizeBytes;
   for (int i = 3; i < L; i++)  // L2L into child level i
     if ((e = build_l2l(c, i, cap)) != ISG_OK) return e;
+  for (int i = 2; i <= L - 2; i++)  // persistent M2M into parent level i
+    if ((e = build_m2m(c, i, cap)) != ISG_OK) return e;
+  if ((e = cuda_check(c, cudaFuncSetAttribute(k_tc_m2m, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap),
+                      "m2m attr")) != ISG_OK)
+    return e;
   if ((e = cuda_check(c, cudaFuncSetAttribute(k_tc_l2l, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap),
                       "l2l attr")) != ISG_OK)
     return e;
@@ -689,6 +987,7 @@ void band_destroy(isg_ctx *c) {
     cudaFree(T->nchunk);
     cudaFree(T->chunk0);
     cudaFree(c->band->l2l[i].A);
+    cudaFree(c->band->pm2m[i].A);
   }
   delete c->band;
   c->band = nullptr;
@@ -723,8 +1022,39 @@ static isg_status band_launch(isg_ctx *c, int lvl, const Transition &T, const fl
 }
 
 bool band_m2m(isg_ctx *c, int lvl, float2 *mul, int nrhs, const int *active, cudaStream_t st, isg_status *e) {
-  if (!c->band || lvl >= kMaxLevels || !c->band->m2m[lvl].ok) return false;
+  if (!c->band || lvl >= kMaxLevels) return false;
   const DevLevel &p = c->P.lv[lvl], &ch = c->P.lv[lvl + 1];
+  if (c->band->pm2m[lvl].ok) {
+    const M2mPlan &T = c->band->pm2m[lvl];
+    M2mArgs A;
+    A.mul = mul;
+    A.mp = c->P.mp;
+    A.off_in = ch.off;
+    A.off_out = p.off;
+    A.lg_np = 0;
+    while ((1 << A.lg_np) < p.n) A.lg_np++;
+    A.ns_in = ch.ns;
+    A.ns_out = p.ns;
+    A.Kp = T.Kp;
+    A.ppi = T.ppi;
+    A.kc_magic = T.kc_magic;
+    A.A = T.A;
+    A.shm = p.shm;
+    A.inv_a = T.inv_a;
+    A.nparents = p.n * p.n;
+    A.items_per_rhs = A.nparents / T.ppi;
+    A.nitems = A.items_per_rhs * nrhs;
+    A.active = active;
+    A.err = c->tc_err_flag();
+    A.levmax = c->levmax;
+    A.lvl_in = lvl + 1;
+    A.lvl_out = lvl;
+    count_launch();
+    k_tc_m2m<<<std::min(A.nitems, c->band->sms), kL2lThreads, M2mSmem(T.Kp, T.ppi, ch.ns).total, st>>>(A);
+    *e = cuda_check(c, cudaGetLastError(), "m2m launch");
+    return true;
+  }
+  if (!c->band->m2m[lvl].ok) return false;
   *e = band_launch(c, lvl, c->band->m2m[lvl], mul + ch.off, mul + p.off, p.n, ch.ns, p.ns, p.shm, nrhs, active,
                    st);
   return true;
