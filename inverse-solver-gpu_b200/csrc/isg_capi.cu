@@ -361,10 +361,11 @@ isg_status isg_setup_gpu(isg_ctx *c) {
   if ((e = dalloc(c, &c->mul, R * P.mp)) || (e = dalloc(c, &c->loc, R * P.mp)) || (e = dalloc(c, &c->wx, R * U)) ||
       (e = dalloc(c, &c->wy, R * U)) || (e = dalloc(c, &c->wg, R * U)) || (e = dalloc(c, &c->vr, R * U)) ||
       (e = dalloc(c, &c->vrt, R * U)) || (e = dalloc(c, &c->vp, R * U)) || (e = dalloc(c, &c->vv, R * U)) ||
-      (e = dalloc(c, &c->vs, R * U)) || (e = dalloc(c, &c->vt, R * U)) || (e = dalloc(c, &c->vgx, R * U)) || (e = dalloc(c, &c->levmax, R * kMaxLevels)) ||
+      (e = dalloc(c, &c->vs, R * U)) || (e = dalloc(c, &c->vt, R * U)) || (e = dalloc(c, &c->vgx, R * U)) || (e = dalloc(c, &c->levmax, 2 * R * kMaxLevels)) ||
       (e = dalloc(c, &c->part, R * (size_t)c->part_blocks * 4 + 64)) || (e = dalloc(c, &c->state, R)) ||
       (e = dalloc(c, &c->active, R)) || (e = dalloc(c, &c->count, 1)))
     return e;
+  c->locmax = c->levmax + R * kMaxLevels;
   if ((e = cuda_check(c, cudaMallocHost(&c->h_count, sizeof(int)), "cudaMallocHost"))) return e;
   if ((e = cuda_check(c, cudaMemset(c->mul, 0, R * P.mp * sizeof(float2)), "memset"))) return e;
   if ((e = cuda_check(c, cudaMemset(c->loc, 0, R * P.mp * sizeof(float2)), "memset"))) return e;
@@ -580,6 +581,7 @@ isg_status isg_time_stages(isg_ctx *c, int nrhs, int engine, int reps, double *m
     cudaEventRecord(ev[0], st);
     if (tc) {
       cudaMemsetAsync(c->levmax, 0, (size_t)nrhs * kMaxLevels * sizeof(unsigned), st);
+      cudaMemsetAsync(c->locmax, 0, (size_t)nrhs * kMaxLevels * sizeof(unsigned), st);
       tc_p2m(c, B, c->mul, st);
     } else {
       launch_p2m(P, B, c->mul, st);
@@ -591,7 +593,7 @@ isg_status isg_time_stages(isg_ctx *c, int nrhs, int engine, int reps, double *m
     cudaEventRecord(ev[2], st);
     for (int i = 2; i < P.L; i++) {
       if (i >= 3 && !(tc && band_l2l(c, i, c->loc, nrhs, nullptr, st, &be))) launch_l2l(P, i, c->loc, nrhs, nullptr, st);
-      launch_m2l(P, i, c->mul, c->loc, nrhs, nullptr, i >= 3, st);
+      launch_m2l(P, i, c->mul, c->loc, nrhs, nullptr, i >= 3, st, tc ? c->locmax : nullptr);
     }
     cudaEventRecord(ev[3], st);
     if (tc) tc_near(c, A, st); else launch_near(P, A, st);

@@ -44,6 +44,7 @@ struct isg_ctx {
   float2 *vr = nullptr, *vrt = nullptr, *vp = nullptr, *vv = nullptr, *vs = nullptr, *vt = nullptr;
   float2 *vgx = nullptr;  // [R][U] g times the next matvec's input, written by the update kernels
   unsigned *levmax = nullptr;  // [R][kMaxLevels] per-level max |re|, |im| of the multipoles (FP32 bits)
+  unsigned *locmax = nullptr;  // [R][kMaxLevels] the same for the locals (written by M2L)
   double *part = nullptr;  // [R][part_blocks][4]
   int part_blocks = 0;
   isg::RhsState *state = nullptr;  // [R]

@@ -149,7 +149,8 @@ void launch_p2m(const DevPlan &P, const BatchArgs &B, float2 *mul, cudaStream_t 
 void launch_m2m(const DevPlan &P, int lvl, float2 *mul, int nrhs, const int *active, cudaStream_t st);
 // M2L into level lvl: written over its local expansions, or added to them.
 void launch_m2l(const DevPlan &P, int lvl, const float2 *mul, float2 *loc, int nrhs, const int *active, bool accumulate,
-                cudaStream_t st);
+                cudaStream_t st,
+                unsigned *locmax = nullptr);
 // L2L from level lvl-1 into level lvl, written over its locals.
 void launch_l2l(const DevPlan &P, int lvl, float2 *loc, int nrhs, const int *active, cudaStream_t st);
 // y = epilogue(L2P(loc_leaf) + near(x)); optional FP64 partials per block.

@@ -105,6 +105,8 @@ struct M2lArgs {
   const float2 *T;
   const int *active;
   const float2 *zeros;  // at least ns zeros
+  unsigned *locmax;     // optional [R][kMaxLevels]: max |re|, |im| of the level's locals (FP32 bits)
+  int lvl;
 };
 
 // One thread's six source columns: base address and bytes per cluster row.
@@ -139,7 +141,7 @@ __device__ __forceinline__ void m2l_old(const float2 *out, size_t row_stride, in
 template <int S, bool ACC>
 __device__ __forceinline__ void m2l_step(const M2lArgs &A, const M2lCols &C, const float2 (&tw)[7][7],
                                          float2 (&w)[8][6], float2 (&ob)[2][2][2], float2 *out, size_t row_stride,
-                                         int b, int a, int a1) {
+                                         int b, int a, int a1, float &mx) {
   if (a + 1 < a1) {
     m2l_row(C, 2 * a + 4, A.n, w[(2 * S + 6) & 7]);
     m2l_row(C, 2 * a + 5, A.n, w[(2 * S + 7) & 7]);
@@ -161,7 +163,10 @@ __device__ __forceinline__ void m2l_step(const M2lArgs &A, const M2lCols &C, con
 #pragma unroll
   for (int oy = 0; oy < 2; oy++)
 #pragma unroll
-    for (int ox = 0; ox < 2; ox++) out[(size_t)(2 * a + oy) * row_stride + (size_t)(2 * b + ox) * A.ns] = acc[oy][ox];
+    for (int ox = 0; ox < 2; ox++) {
+      out[(size_t)(2 * a + oy) * row_stride + (size_t)(2 * b + ox) * A.ns] = acc[oy][ox];
+      mx = fmaxf(mx, fmaxf(fabsf(acc[oy][ox].x), fabsf(acc[oy][ox].y)));
+    }
 }
 
 template <bool ACC>
@@ -195,15 +200,20 @@ __global__ void __launch_bounds__(128, 2) k_m2l(M2lArgs A) {
 #pragma unroll
   for (int i = 0; i < 6; i++) m2l_row(C, 2 * a0 - 2 + i, A.n, w[i]);
   m2l_old<ACC>(out, row_stride, ns, b, a0, ob[0]);
+  float mx = 0.f;
 #pragma unroll 1
   for (int a = a0; a < a1; a += 4) {
-    m2l_step<0, ACC>(A, C, tw, w, ob, out, row_stride, b, a, a1);
+    m2l_step<0, ACC>(A, C, tw, w, ob, out, row_stride, b, a, a1, mx);
     if (a + 1 >= a1) break;
-    m2l_step<1, ACC>(A, C, tw, w, ob, out, row_stride, b, a + 1, a1);
+    m2l_step<1, ACC>(A, C, tw, w, ob, out, row_stride, b, a + 1, a1, mx);
     if (a + 2 >= a1) break;
-    m2l_step<2, ACC>(A, C, tw, w, ob, out, row_stride, b, a + 2, a1);
+    m2l_step<2, ACC>(A, C, tw, w, ob, out, row_stride, b, a + 2, a1, mx);
     if (a + 3 >= a1) break;
-    m2l_step<3, ACC>(A, C, tw, w, ob, out, row_stride, b, a + 3, a1);
+    m2l_step<3, ACC>(A, C, tw, w, ob, out, row_stride, b, a + 3, a1, mx);
+  }
+  if (A.locmax) {  // the level's maximum, for the power-of-two scale of the tensor-core L2L below it
+    const unsigned m = __activemask(), bits = __reduce_max_sync(m, __float_as_uint(mx));
+    if ((threadIdx.x & 31) == __ffs(m) - 1 && bits) atomicMax(&A.locmax[rhs * kMaxLevels + A.lvl], bits);
   }
 }
 
@@ -627,7 +637,8 @@ void launch_m2m(const DevPlan &P, int lvl, float2 *mul, int nrhs, const int *act
 }
 
 void launch_m2l(const DevPlan &P, int lvl, const float2 *mul, float2 *loc, int nrhs, const int *active, bool accumulate,
-                cudaStream_t st) {
+                cudaStream_t st,
+                unsigned *locmax) {
   const DevLevel &c = P.lv[lvl];
   M2lArgs A;
   A.mul = mul;
@@ -639,6 +650,8 @@ void launch_m2l(const DevPlan &P, int lvl, const float2 *mul, float2 *loc, int n
   A.T = c.T;
   A.active = active;
   A.zeros = P.zeros;
+  A.locmax = locmax;
+  A.lvl = lvl;
   const int half = c.n / 2, bx = (half * c.ns + 127) / 128;
   // eight groups per thread when the grid stays large, fewer for small batches
   int ty = std::min(8, half);

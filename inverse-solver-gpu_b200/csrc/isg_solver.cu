@@ -358,6 +358,7 @@ isg_status run_matvec(isg_ctx *c, const float2 *x, const float2 *g, int64_t gs, 
   }
   if (tc) {
     cudaMemsetAsync(c->levmax, 0, (size_t)nrhs * kMaxLevels * sizeof(unsigned), st);
+    cudaMemsetAsync(c->locmax, 0, (size_t)nrhs * kMaxLevels * sizeof(unsigned), st);
     isg_status e = tc_p2m(c, Bg, c->mul, st);
     if (e != ISG_OK) return e;
   } else {
@@ -371,7 +372,7 @@ isg_status run_matvec(isg_ctx *c, const float2 *x, const float2 *g, int64_t gs, 
   // then the level's own far-field translations added (M2L)
   for (int i = 2; i < P.L; i++) {
     if (i >= 3 && !(tc && band_l2l(c, i, c->loc, nrhs, active, st, &be))) launch_l2l(P, i, c->loc, nrhs, active, st);
-    launch_m2l(P, i, c->mul, c->loc, nrhs, active, i >= 3, st);
+    launch_m2l(P, i, c->mul, c->loc, nrhs, active, i >= 3, st, tc ? c->locmax : nullptr);
   }
   if (be != ISG_OK) return be;
   NearArgs A;

@@ -114,7 +114,6 @@ __global__ void __launch_bounds__(256, 2) k_tc_band(BandArgs A) {
   const int mt = blockIdx.y, m0 = mt * 128;
   const int kw0 = A.kw0[mt], nch = A.nchunk[mt];
   const uint8_t *Achunks = A.A + (size_t)A.chunk0[mt] * 2 * kAHalf;
-  const int kwtot = nch * kKC;
 
   // power-of-two scale from the input level's maximum over the CTA's RHS
   // (written by the kernel that produced that level)
@@ -246,23 +245,8 @@ struct L2lArgs {
   int nparents, items_per_rhs, nitems;
   const int *active;
   int *err;
-};
-
-// Shared-memory carve-up (bytes): A hi/lo; B hi/lo (8 rows per parent: 4
-// children x re, im); the item's rings staged as [parent][Kp / 8] groups of 8
-// samples, each group padded to 80 bytes; the shifts as [4][Kp + 2] float2
-// (child-major, padded); barriers and scratch.  The paddings put the groups
-// that one warp reads on distinct banks.
-struct L2lSmem {
-  size_t a, b, z, sh, bar, total;
-  __host__ __device__ L2lSmem(int Kp, int ppi) {
-    a = 0;
-    b = a + (size_t)512 * Kp;
-    z = b + (size_t)32 * ppi * Kp;
-    sh = z + (size_t)10 * ppi * Kp;
-    bar = sh + (size_t)32 * (Kp + 2);
-    total = bar + 128;
-  }
+  const unsigned *locmax;  // [R][kMaxLevels] max |re|, |im| of the locals per level (written by M2L)
+  int lvl_in;
 };
 
 // Splits (a, b), already scaled into the FP16 range, into packed hi and lo halves.
@@ -272,204 +256,242 @@ __device__ __forceinline__ void split2(float a, float b, __half2 &hi, __half2 &l
   lo = __floats2half2_rn(a - h.x, b - h.y);
 }
 
-constexpr int kL2lThreads = 512;
-constexpr int kL2lConvWarps = kL2lThreads / 32 - 1;  // the last warp issues the MMAs
-constexpr int kL2lConv = 32 * kL2lConvWarps;
+// The same split as packed 32-bit words (lo half = first value).
+__device__ __forceinline__ void split2u(float a, float b, uint32_t &hi, uint32_t &lo) {
+  __half2 h, l;
+  split2(a, b, h, l);
+  hi = *(uint32_t *)&h;
+  lo = *(uint32_t *)&l;
+}
+__device__ __forceinline__ void st_shared_v4(void *p, const uint32_t (&v)[4]) {
+  asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};\n" ::"r"(smem_u32(p)), "r"(v[0]), "r"(v[1]), "r"(v[2]),
+               "r"(v[3])
+               : "memory");
+}
 
-// Named barriers 1..15 (0 is __syncthreads): sync waits for `count` threads,
-// arrive only signals.
+constexpr int kL2lThreads = 512;
+
+// Named barrier 1..15 (0 is __syncthreads) over `count` threads.
 __device__ __forceinline__ void named_sync(int id, int count) {
   asm volatile("bar.sync %0, %1;\n" ::"r"(id), "r"(count) : "memory");
 }
-__device__ __forceinline__ void named_arrive(int id, int count) {
-  asm volatile("bar.arrive %0, %1;\n" ::"r"(id), "r"(count) : "memory");
-}
+
+// The persistent tensor-core L2L and M2M kernels run items (groups of
+// consecutive parents of one RHS) through three roles, each item's buffers
+// alternating between two sets: converter warps turn the item's staged rings
+// into the FP16 hi/lo operand B[b] while the MMA warp multiplies the previous
+// item's B[1-b] into TMEM accumulator 1-b and the epilogue warps drain the
+// accumulator of the item before that.  Hand-offs are mbarriers: zfull (the
+// item's rings landed), bfull / bfree (operand written / consumed by the
+// MMAs), tfull / tfree (accumulator written / read out).  Every wait is
+// bounded and gives up once any role has given up.  The weight matrix A
+// (128 output samples x Kp input samples, FP16 hi/lo) stays resident.
+constexpr int kPipeConvWarps = 11;  // warps 0..10
+constexpr int kPipeMmaWarp = 11;    // warp 11
+constexpr int kPipeEpiWarp0 = 12;   // warps 12..15, one per TMEM lane quarter
+constexpr int kPipeConv = 32 * kPipeConvWarps;
+constexpr int kPipeEpi = kL2lThreads - 32 * kPipeEpiWarp0;
+constexpr int kPipeEpiGroups = kPipeEpi / 128;  // column groups of the accumulator
+
+// Barrier slots: A, zfull[2], bfull[2], bfree[2], tfull[2], tfree[2]; then
+// the TMEM base and the abort flag.
+struct PipeBars {
+  uint64_t *abar, *zfull, *bfull, *bfree, *tfull, *tfree;
+  uint32_t *tslot;
+  volatile int *abort;
+  __device__ explicit PipeBars(char *p) {
+    uint64_t *b = (uint64_t *)p;
+    abar = b;
+    zfull = b + 1;
+    bfull = b + 3;
+    bfree = b + 5;
+    tfull = b + 7;
+    tfree = b + 9;
+    tslot = (uint32_t *)(b + 11);
+    abort = (volatile int *)(b + 12);
+  }
+};
+
+// L2L layout: A hi/lo; B[2] hi/lo; the shifts [4][Kp + 2] (child-major,
+// padded against bank conflicts); two staging buffers, each the item's ppi
+// consecutive parent rings (one contiguous run) and Kp zero samples; barriers.
+struct L2lSmem {
+  size_t a, b, bbuf, sh, z, zbuf, bar, total;
+  __host__ __device__ L2lSmem(int Kp, int ppi, int ns) {
+    a = 0;
+    b = a + (size_t)512 * Kp;
+    bbuf = (size_t)32 * ppi * Kp;
+    sh = b + 2 * bbuf;
+    z = sh + (((size_t)32 * (Kp + 2) + 127) & ~(size_t)127);
+    zbuf = ((size_t)(ppi * ns + Kp) * 8 + 127) & ~(size_t)127;
+    bar = z + 2 * zbuf;
+    total = bar + 256;
+  }
+};
 
 __global__ void __launch_bounds__(kL2lThreads, 1) k_tc_l2l(L2lArgs A) {
   extern __shared__ __align__(1024) char sm[];
-  const L2lSmem L(A.Kp, A.ppi);
-  const int N = 8 * A.ppi, Kp = A.Kp, kc = Kp / 8, NH = N / 2;
-  char *bhi = sm + L.b, *blo = bhi + (size_t)N * Kp * 2;
-  float4 *zst = (float4 *)(sm + L.z);  // 5 float4 per group of 8 samples (the fifth is padding)
+  const L2lSmem L(A.Kp, A.ppi, A.ns_in);
+  const int N = 8 * A.ppi, Kp = A.Kp, kc = Kp / 8, zs = A.ns_in;
+  const PipeBars Bq(sm + L.bar);
   float2 *shs = (float2 *)(sm + L.sh);
-  uint64_t *abar = (uint64_t *)(sm + L.bar);
-  uint64_t *done = abar + 1;  // [2]: one per column half
-  uint32_t *tslot = (uint32_t *)(abar + 3);
-  float *fscr = (float *)(abar + 4);  // [kL2lThreads / 32]
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = kL2lThreads / 32;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  auto bbuf = [&](int b) { return sm + L.b + b * L.bbuf; };  // hi, then lo N * Kp * 2 bytes on
+  auto zbuf = [&](int b) { return (float2 *)(sm + L.z + b * L.zbuf); };
   if (threadIdx.x == 0) {
-    mbar_init(abar, 1);
-    mbar_init(done, 1);
-    mbar_init(done + 1, 1);
+    for (int i = 0; i < 11; i++) mbar_init(Bq.abar + i, 1);
+    *Bq.abort = 0;
     fence_mbar_init();
   }
-  if (warp == 0) tmem_alloc(tslot, N);
+  if (warp == 0) tmem_alloc(Bq.tslot, 2 * N);
   for (int e = threadIdx.x; e < 4 * (Kp + 2); e += blockDim.x) {
     const int q = e / (Kp + 2), j = e - q * (Kp + 2);
     shs[e] = j < A.ns_in ? __ldg(A.shl + 4 * j + q) : make_float2(0.f, 0.f);
   }
-  const int ngroups = A.ppi * kc;
-  for (int e = threadIdx.x; e < 5 * ngroups; e += blockDim.x) zst[e] = make_float4(0.f, 0.f, 0.f, 0.f);
+  // zero both staging buffers: the tail past the last ring is read (against zero weights)
+  for (int e = threadIdx.x; e < (int)(2 * L.zbuf / 4); e += blockDim.x) ((float *)zbuf(0))[e] = 0.f;
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  const uint32_t tmem = *tslot;
-  if (threadIdx.x == 0) {
-    mbar_expect_tx(abar, 512 * Kp);
-    bulk_g2s(sm + L.a, A.A, 512 * Kp, abar);
-  }
-  auto active_item = [&](int w) {
-    while (w < A.nitems && A.active && !A.active[w / A.items_per_rhs]) w += gridDim.x;
+  const uint32_t tmem = *Bq.tslot;
+  auto next_item = [&](int w) {
+    do w += gridDim.x;
+    while (w < A.nitems && A.active && !A.active[w / A.items_per_rhs]);
     return w;
   };
-  // an item's parent rings into the staging groups, 16 bytes (2 samples) per copy
-  const int pieces = A.ns_in / 2;
-  auto stage = [&](int w, int t, int nt) {
-    const int rhs = w / A.items_per_rhs, p0 = (w % A.items_per_rhs) * A.ppi;
-    const float2 *base = A.loc + (size_t)rhs * A.mp + A.off_in;
-    for (int pl = t >> 5; pl < A.ppi; pl += nt >> 5) {
-      const int P = p0 + pl;
-      const bool ok = P < A.nparents;
-      const float2 *ring = base + (size_t)(ok ? P : 0) * A.ns_in;
-      for (int c = lane; c < pieces; c += 32) cp_async16z(zst + (pl * kc + (c >> 2)) * 5 + (c & 3), ring + 2 * c, ok);
-    }
+  const int first = (A.active && !A.active[blockIdx.x / A.items_per_rhs]) ? next_item(blockIdx.x) : blockIdx.x;
+  auto scale_of = [&](int w) {
+    return pow2_scale(1.5f * A.shl_max * __uint_as_float(A.locmax[(w / A.items_per_rhs) * kMaxLevels + A.lvl_in]));
   };
-  const uint32_t sbase = smem_u32(sm);
-  const uint32_t idesc = idesc_f16_f32(128, NH);
-  const uint32_t sbo = (uint32_t)kc * 128;
-  const int nc = 2 << A.lg_np, npm = (1 << A.lg_np) - 1;
-  bool ok = mbar_wait(abar, 0, A.err, kErrL2l);
-  int parity = 0;
-  int w = active_item(blockIdx.x);
-  if (w < A.nitems) stage(w, threadIdx.x, kL2lThreads);
-  cp_async_wait_all();
-  __syncthreads();
-  while (w < A.nitems) {
-    // power-of-two scale of this item's shifted rings
-    float mx = 0.f;
-    for (int e = threadIdx.x; e < 5 * ngroups; e += blockDim.x) {
-      const float4 v = zst[e];
-      mx = fmaxf(mx, fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w))));
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    if (lane == 0) fscr[warp] = mx;
-    __syncthreads();
-    float m2 = 0.f;
-    for (int k = 0; k < nwarps; k++) m2 = fmaxf(m2, fscr[k]);
-    const float s = pow2_scale(1.5f * A.shl_max * m2);
-    const int nxt = active_item(w + gridDim.x);
-    if (warp < kL2lConvWarps) {
-      // B rows 8 parent + 2 q + (re, im) = shl[q][j] z[j] s.  A unit is one child q
-      // of one core-matrix group (8 samples of one parent): both rows, hi and lo.
-      // Each thread keeps two units in flight; each finished half is handed to
-      // the MMA warp through a named barrier it only arrives at.
-      const int ct = threadIdx.x;
-      for (int h = 0; h < 2; h++) {
-        const int u0 = h * 2 * ngroups, u1 = u0 + 2 * ngroups;
-        for (int ub = u0 + ct; ub < u1; ub += 2 * kL2lConv) {
-          float4 zv[2][4], sv[2][4];
-          int cmk[2], qk[2];
-#pragma unroll
-          for (int k = 0; k < 2; k++) {
-            const int u = min(ub + k * kL2lConv, u1 - 1);
-            qk[k] = u & 3;
-            cmk[k] = u >> 2;
-            const int j0 = 8 * (cmk[k] - (int)__umulhi((unsigned)cmk[k], A.kc_magic) * kc);
-            const float4 *sp = (const float4 *)(shs + qk[k] * (Kp + 2) + j0);
-#pragma unroll
-            for (int i = 0; i < 4; i++) {
-              zv[k][i] = zst[cmk[k] * 5 + i];
-              sv[k][i] = sp[i];
-            }
-          }
-#pragma unroll
-          for (int k = 0; k < 2; k++) {
-            __half2 hr[4], lr[4], hm[4], lm[4];
-#pragma unroll
-            for (int i = 0; i < 4; i++) {
-              const float4 z = zv[k][i], sh = sv[k][i];
-              const float re0 = fmaf(sh.x, z.x, -sh.y * z.y), im0 = fmaf(sh.x, z.y, sh.y * z.x);
-              const float re1 = fmaf(sh.z, z.z, -sh.w * z.w), im1 = fmaf(sh.z, z.w, sh.w * z.z);
-              split2(re0 * s, re1 * s, hr[i], lr[i]);
-              split2(im0 * s, im1 * s, hm[i], lm[i]);
-            }
-            if (ub + k * kL2lConv < u1) {
-              const size_t o = (size_t)cmk[k] * 128 + qk[k] * 32;
-              *(uint4 *)(bhi + o) = *(uint4 *)hr;
-              *(uint4 *)(bhi + o + 16) = *(uint4 *)hm;
-              *(uint4 *)(blo + o) = *(uint4 *)lr;
-              *(uint4 *)(blo + o + 16) = *(uint4 *)lm;
-            }
-          }
-        }
-        fence_proxy_async();
-        named_arrive(1 + h, kL2lThreads);
-      }
-      // every unit is converted: the staging buffer takes the next item's rings
-      named_sync(3, kL2lConv);
-      if (nxt < A.nitems) stage(nxt, ct, kL2lConv);
-    } else {
-      // the MMA warp: one elected lane issues each half once it is converted
-      for (int h = 0; h < 2; h++) {
-        named_sync(1 + h, kL2lThreads);
-        if (lane == 0) {
-          tc_fence_after();
-          if (ok) {
-            const uint32_t bo = (uint32_t)h * 8 * A.ppi * Kp;  // bytes of one half of B
-            const uint64_t ah = smem_desc(sbase + (uint32_t)L.a, 128, sbo);
-            const uint64_t al = smem_desc(sbase + (uint32_t)L.a + 256 * Kp, 128, sbo);
-            const uint64_t bh = smem_desc(smem_u32(bhi) + bo, 128, sbo);
-            const uint64_t bl = smem_desc(smem_u32(blo) + bo, 128, sbo);
-            const uint32_t d = tmem + (uint32_t)(h * NH);
-            for (int ks = 0; ks < Kp / 16; ks++) {
-              const uint32_t k = ks * 256;
-              mma_f16(d, desc_add(ah, k), desc_add(bh, k), idesc, ks ? 1 : 0);
-              mma_f16(d, desc_add(ah, k), desc_add(bl, k), idesc, 1);
-              mma_f16(d, desc_add(al, k), desc_add(bh, k), idesc, 1);
-            }
-          }
-          mma_commit(done + h);
-        }
-        __syncwarp();
-      }
-    }
+  // an item's ppi consecutive parent rings: one bulk copy
+  const uint32_t run = (uint32_t)A.ppi * A.ns_in * 8;
+  auto stage = [&](int w, int b) {
+    if (lane != 0) return;
     const int rhs = w / A.items_per_rhs, p0 = (w % A.items_per_rhs) * A.ppi;
-    // epilogue per half: lane = child sample, 16 columns = 2 parents x 4 children x (re, im);
-    // warp = (column quarter, lane quarter)
-    const float inv = A.inv_a / s;
-    const int qd = warp & 3, cq = warp >> 2, km = 32 * qd + lane;
-    float2 *obase = A.loc + (size_t)rhs * A.mp + A.off_out + km;
+    mbar_expect_tx(Bq.zfull + b, run);
+    bulk_g2s(zbuf(b), A.loc + (size_t)rhs * A.mp + A.off_in + (size_t)p0 * A.ns_in, run, Bq.zfull + b);
+  };
+  const int ngroups = A.ppi * kc;
+
+  if (warp < kPipeConvWarps) {
+    // ---- converters: B[b] rows 8 parent + 2 q + (re, im) = shl[q][j] z[j] s ----
+    if (warp == 0) {
+      if (lane == 0) {
+        mbar_expect_tx(Bq.abar, 512 * Kp);
+        bulk_g2s(sm + L.a, A.A, 512 * Kp, Bq.abar);
+      }
+      if (first < A.nitems) stage(first, 0);
+      const int second = first < A.nitems ? next_item(first) : A.nitems;
+      if (second < A.nitems) stage(second, 1);
+    }
+    int w = first, w2 = first < A.nitems ? next_item(next_item(first)) : A.nitems;
+    for (int it = 0; w < A.nitems; it++) {
+      const int b = it & 1, ph = (it >> 1) & 1;
+      const bool zok = mbar_wait_or(Bq.zfull + b, ph, Bq.abort, A.err, kErrL2l);
+      const bool bok = mbar_wait_or(Bq.bfree + b, ph ^ 1, Bq.abort, A.err, kErrL2l);
+      const float s = scale_of(w);
+      const float2 *zst = zbuf(b);
+      char *bhi = bbuf(b), *blo = bhi + (size_t)N * Kp * 2;
+      if (zok && bok) {
+        // a unit is one child q of one core-matrix group (8 samples of one parent):
+        // both rows, hi and lo
+#pragma unroll 2
+        for (int u = threadIdx.x; u < 4 * ngroups; u += kPipeConv) {
+          const int q = u & 3, cm = u >> 2;
+          const int pl = (int)__umulhi((unsigned)cm, A.kc_magic), j0 = 8 * (cm - pl * kc);
+          const float4 *zp = (const float4 *)(zst + pl * zs + j0);
+          const float4 *sp = (const float4 *)(shs + q * (Kp + 2) + j0);
+          uint32_t hr[4], lr[4], hm[4], lm[4];
+#pragma unroll
+          for (int i = 0; i < 4; i++) {
+            const float4 z = zp[i], sh = sp[i];
+            const float re0 = fmaf(sh.x, z.x, -sh.y * z.y) * s, im0 = fmaf(sh.x, z.y, sh.y * z.x) * s;
+            const float re1 = fmaf(sh.z, z.z, -sh.w * z.w) * s, im1 = fmaf(sh.z, z.w, sh.w * z.z) * s;
+            split2u(re0, re1, hr[i], lr[i]);
+            split2u(im0, im1, hm[i], lm[i]);
+          }
+          const uint32_t o = (uint32_t)cm * 128 + q * 32;
+          st_shared_v4(bhi + o, hr);
+          st_shared_v4(bhi + o + 16, hm);
+          st_shared_v4(blo + o, lr);
+          st_shared_v4(blo + o + 16, lm);
+        }
+      }
+      fence_proxy_async();
+      named_sync(1, kPipeConv);  // every converter is done with zbuf(b) and B[b]
+      if (threadIdx.x == 0) mbar_arrive(Bq.bfull + b);
+      if (warp == 0 && w2 < A.nitems) stage(w2, b);
+      w = next_item(w);
+      w2 = w2 < A.nitems ? next_item(w2) : A.nitems;
+    }
+  } else if (warp == kPipeMmaWarp) {
+    // ---- MMA issue ----
+    const uint32_t idesc = idesc_f16_f32(128, N);
+    const uint32_t sbo = (uint32_t)kc * 128, sbase = smem_u32(sm);
+    const uint64_t ah = smem_desc(sbase + (uint32_t)L.a, 128, sbo);
+    const uint64_t al = smem_desc(sbase + (uint32_t)L.a + 256 * Kp, 128, sbo);
+    const bool aok = mbar_wait_or(Bq.abar, 0, Bq.abort, A.err, kErrL2l);
+    int w = first;
+    for (int it = 0; w < A.nitems; it++) {
+      const int b = it & 1, ph = (it >> 1) & 1;
+      const bool ok = mbar_wait_or(Bq.bfull + b, ph, Bq.abort, A.err, kErrL2l) &&
+                      mbar_wait_or(Bq.tfree + b, ph ^ 1, Bq.abort, A.err, kErrL2l) && aok;
+      if (lane == 0) {
+        tc_fence_after();
+        if (ok) {
+          const uint64_t bh = smem_desc(smem_u32(bbuf(b)), 128, sbo);
+          const uint64_t bl = smem_desc(smem_u32(bbuf(b)) + N * Kp * 2, 128, sbo);
+          const uint32_t d = tmem + (uint32_t)(b * N);
+          for (int ks = 0; ks < Kp / 16; ks++) {
+            const uint32_t k = ks * 256;
+            mma_f16(d, desc_add(ah, k), desc_add(bh, k), idesc, ks ? 1 : 0);
+            mma_f16(d, desc_add(ah, k), desc_add(bl, k), idesc, 1);
+            mma_f16(d, desc_add(al, k), desc_add(bh, k), idesc, 1);
+          }
+        }
+        mma_commit(Bq.bfree + b);
+        mma_commit(Bq.tfull + b);
+      }
+      __syncwarp();
+      w = next_item(w);
+    }
+  } else {
+    // ---- epilogue: lane = child sample, 16 columns = 2 parents x 4 children x (re, im) ----
+    const int ew = warp - kPipeEpiWarp0, qd = ew & 3, ch0 = ew >> 2;  // lane quarter, column group
+    const int km = 32 * qd + lane;
+    const int nc = 2 << A.lg_np, npm = (1 << A.lg_np) - 1;
     const int so = A.ns_out, qoff[4] = {0, so, nc * so, nc * so + so};
-    for (int h = 0; h < 2; h++) {
-      ok = mbar_wait(done + h, parity, A.err, kErrL2l) && ok;
+    int w = first;
+    for (int it = 0; w < A.nitems; it++) {
+      const int b = it & 1, ph = (it >> 1) & 1;
+      const bool ok = mbar_wait_or(Bq.tfull + b, ph, Bq.abort, A.err, kErrL2l);
       tc_fence_after();
-      for (int ch = 0; ch < NH / 64; ch++) {
-        const int col0 = h * NH + cq * (NH / 4) + 16 * ch;
-        float d[16];
-        tmem_ld16(tmem + ((uint32_t)(32 * qd) << 16) + col0, d);
+      const int rhs = w / A.items_per_rhs, p0 = (w % A.items_per_rhs) * A.ppi;
+      const float inv = A.inv_a / scale_of(w);
+      // the item's parents share a row: parent p0 + pl's first child is 2 pl clusters on
+      float2 *ob = A.loc + (size_t)rhs * A.mp + A.off_out + km +
+                   (size_t)(2 * (p0 >> A.lg_np) * nc + 2 * (p0 & npm)) * so;
+      for (int cg = 0; cg < N / (32 * kPipeEpiGroups); cg++) {  // 32 columns = 4 parents
+        const int col0 = ch0 * (N / kPipeEpiGroups) + 32 * cg;
+        float d[32];
+        tmem_ld32(tmem + ((uint32_t)(32 * qd) << 16) + (uint32_t)(b * N + col0), d);
         if (!ok || km >= A.ns_out) continue;
 #pragma unroll
-        for (int u = 0; u < 2; u++) {
-          const int P = p0 + col0 / 8 + u;
-          if (P >= A.nparents) continue;
-          const int py = P >> A.lg_np, px = P & npm;
-          const int base = (2 * py * nc + 2 * px) * so;
+        for (int u = 0; u < 4; u++) {
+          float2 *o = ob + (size_t)2 * (col0 / 8 + u) * so;
 #pragma unroll
-          for (int q = 0; q < 4; q++)
-            obase[base + qoff[q]] = make_float2(d[8 * u + 2 * q] * inv, d[8 * u + 2 * q + 1] * inv);
+          for (int q = 0; q < 4; q++) o[qoff[q]] = make_float2(d[8 * u + 2 * q] * inv, d[8 * u + 2 * q + 1] * inv);
         }
       }
+      tc_fence_before();
+      named_sync(2, kPipeEpi);  // the accumulator is read out
+      if (ew == 0 && lane == 0) mbar_arrive(Bq.tfree + b);
+      w = next_item(w);
     }
-    parity ^= 1;
-    cp_async_wait_all();
-    tc_fence_before();
-    __syncthreads();  // staging, B and TMEM are reused by the next item
-    w = nxt;
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 0) tmem_dealloc(tmem, N);
+  if (warp == 0) tmem_dealloc(tmem, 2 * N);
 }
 
 // ---- M2M, persistent, for parents of at most 128 samples ----
@@ -497,19 +519,6 @@ struct M2mArgs {
   unsigned *levmax;
   int lvl_in, lvl_out;
 };
-
-// Pipelined over items in three roles, each item's buffers alternating
-// between two sets: converter warps turn staged rings into B[b] while the MMA
-// warp multiplies B[1-b] into TMEM accumulator 1-b and the epilogue warps
-// drain the accumulator of the item before.  Hand-offs are mbarriers:
-// zfull (bulk copies landed), bfull / bfree (operand written / consumed),
-// tfull / tfree (accumulator written / read out).  Every wait is bounded and
-// gives up once any role has given up.
-constexpr int kPipeConvWarps = 7;  // warps 0..6
-constexpr int kPipeMmaWarp = 7;    // warp 7
-constexpr int kPipeEpiWarp0 = 8;   // warps 8..15
-constexpr int kPipeConv = 32 * kPipeConvWarps;
-constexpr int kPipeEpi = kL2lThreads - 32 * kPipeEpiWarp0;
 
 // A hi/lo; B[2] hi/lo; staged child rings [2][2 rows][2 ppi clusters][ns]
 // (the item's parents are consecutive in one row, so each child row is one
@@ -596,37 +605,24 @@ __global__ void __launch_bounds__(kL2lThreads, 1) k_tc_m2m(M2mArgs A) {
       const float2 *zst = zbuf(b);
       char *bhi = bbuf(b), *blo = bhi + (size_t)N * Kp * 2;
       if (zok && bok) {
-        for (int ub = threadIdx.x; ub < 4 * ngroups; ub += 2 * kPipeConv) {
-          float4 zv[2][4];
-          int cmk[2], qk[2];
+#pragma unroll 2
+        for (int u = threadIdx.x; u < 4 * ngroups; u += kPipeConv) {
+          const int q = u & 3, cm = u >> 2;
+          const int pl = (int)__umulhi((unsigned)cm, A.kc_magic), j8 = cm - pl * kc;
+          const int slot = (q >> 1) * 2 * A.ppi + 2 * pl + (q & 1);
+          const float4 *zp = (const float4 *)(zst + slot * zs + 8 * j8);
+          uint32_t hr[4], lr[4], hm[4], lm[4];
 #pragma unroll
-          for (int k = 0; k < 2; k++) {
-            const int u = min(ub + k * kPipeConv, 4 * ngroups - 1);
-            qk[k] = u & 3;
-            cmk[k] = u >> 2;
-            const int pl = (int)__umulhi((unsigned)cmk[k], A.kc_magic), j8 = cmk[k] - pl * kc;
-            const int slot = (qk[k] >> 1) * 2 * A.ppi + 2 * pl + (qk[k] & 1);
-            const float4 *zp = (const float4 *)(zst + slot * zs + 8 * j8);
-#pragma unroll
-            for (int i = 0; i < 4; i++) zv[k][i] = zp[i];
+          for (int i = 0; i < 4; i++) {
+            const float4 z = zp[i];
+            split2u(z.x * s, z.z * s, hr[i], lr[i]);
+            split2u(z.y * s, z.w * s, hm[i], lm[i]);
           }
-#pragma unroll
-          for (int k = 0; k < 2; k++) {
-            __half2 hr[4], lr[4], hm[4], lm[4];
-#pragma unroll
-            for (int i = 0; i < 4; i++) {
-              const float4 z = zv[k][i];
-              split2(z.x * s, z.z * s, hr[i], lr[i]);
-              split2(z.y * s, z.w * s, hm[i], lm[i]);
-            }
-            if (ub + k * kPipeConv < 4 * ngroups) {
-              const size_t o = (size_t)cmk[k] * 128 + qk[k] * 32;
-              *(uint4 *)(bhi + o) = *(uint4 *)hr;
-              *(uint4 *)(bhi + o + 16) = *(uint4 *)hm;
-              *(uint4 *)(blo + o) = *(uint4 *)lr;
-              *(uint4 *)(blo + o + 16) = *(uint4 *)lm;
-            }
-          }
+          const uint32_t o = (uint32_t)cm * 128 + q * 32;
+          st_shared_v4(bhi + o, hr);
+          st_shared_v4(bhi + o + 16, hm);
+          st_shared_v4(blo + o, lr);
+          st_shared_v4(blo + o + 16, lm);
         }
       }
       fence_proxy_async();
@@ -669,7 +665,7 @@ __global__ void __launch_bounds__(kL2lThreads, 1) k_tc_m2m(M2mArgs A) {
     }
   } else {
     // ---- epilogue: lane = parent sample, 16 columns = 2 parents x 4 children x (re, im) ----
-    const int ew = warp - kPipeEpiWarp0, qd = ew & 3, ch0 = ew >> 2;  // lane quarter, column half
+    const int ew = warp - kPipeEpiWarp0, qd = ew & 3, ch0 = ew >> 2;  // lane quarter, column group
     const int km = 32 * qd + lane;
     float2 shq[4];
 #pragma unroll
@@ -683,13 +679,13 @@ __global__ void __launch_bounds__(kL2lThreads, 1) k_tc_m2m(M2mArgs A) {
       const float inv = A.inv_a / scale_of(w);
       float2 *obase = A.mul + (size_t)rhs * A.mp + A.off_out + km;
       float omx = 0.f;
-      for (int ch = 0; ch < N / 32; ch++) {
-        const int col0 = ch0 * (N / 2) + 16 * ch;
-        float d[16];
-        tmem_ld16(tmem + ((uint32_t)(32 * qd) << 16) + (uint32_t)(b * N + col0), d);
+      for (int cg = 0; cg < N / (32 * kPipeEpiGroups); cg++) {  // 32 columns = 4 parents
+        const int col0 = ch0 * (N / kPipeEpiGroups) + 32 * cg;
+        float d[32];
+        tmem_ld32(tmem + ((uint32_t)(32 * qd) << 16) + (uint32_t)(b * N + col0), d);
         if (!ok || km >= A.ns_out) continue;
 #pragma unroll
-        for (int u = 0; u < 2; u++) {
+        for (int u = 0; u < 4; u++) {
           const int P = p0 + col0 / 8 + u;
           float2 acc = make_float2(0.f, 0.f);
 #pragma unroll
@@ -837,13 +833,13 @@ static isg_status build_l2l(isg_ctx *c, int i, size_t smem_cap) {
   if (ns_out > 128) return ISG_OK;
   const int Kp = (ns_in + 15) / 16 * 16;
   int ppi = 0;
-  for (int cand : {32, 16})
-    if (L2lSmem(Kp, cand).total <= smem_cap) {
+  for (int cand : {32, 16, 8})
+    if (L2lSmem(Kp, cand, ns_in).total <= smem_cap) {
       ppi = cand;
       break;
     }
   const int nparents = 1 << (2 * (i - 1));
-  if (!ppi || nparents % ppi) return ISG_OK;
+  if (!ppi || nparents % ppi || (1 << (i - 1)) < ppi) return ISG_OK;  // an item's parents share a row
   std::vector<double> dense((size_t)128 * Kp, 0.0);
   for (int k = 0; k < ns_out; k++)
     for (int t = 0; t < taps; t++) {
@@ -1081,13 +1077,15 @@ bool band_l2l(isg_ctx *c, int lvl, float2 *loc, int nrhs, const int *active, cud
   A.shl = p.shlT;
   A.inv_a = T.inv_a;
   A.shl_max = T.shl_max;
+  A.locmax = c->locmax;
+  A.lvl_in = lvl - 1;
   A.nparents = p.n * p.n;
   A.items_per_rhs = A.nparents / T.ppi;
   A.nitems = A.items_per_rhs * nrhs;
   A.active = active;
   A.err = c->tc_err_flag();
   count_launch();
-  k_tc_l2l<<<std::min(A.nitems, c->band->sms), kL2lThreads, L2lSmem(T.Kp, T.ppi).total, st>>>(A);
+  k_tc_l2l<<<std::min(A.nitems, c->band->sms), kL2lThreads, L2lSmem(T.Kp, T.ppi, p.ns).total, st>>>(A);
   *e = cuda_check(c, cudaGetLastError(), "l2l launch");
   return true;
 }
