@@ -166,5 +166,68 @@ __device__ __forceinline__ float pow2_scale(float maxabs) {
   return ldexpf(1.f, 14 - e);
 }
 
+// Splits (a, b), already scaled into the FP16 range, into packed hi and lo halves.
+__device__ __forceinline__ void split2(float a, float b, __half2 &hi, __half2 &lo) {
+  hi = __floats2half2_rn(a, b);
+  const float2 h = __half22float2(hi);
+  lo = __floats2half2_rn(a - h.x, b - h.y);
+}
+
+// The same split as packed 32-bit words (lo half = first value).
+__device__ __forceinline__ void split2u(float a, float b, uint32_t &hi, uint32_t &lo) {
+  __half2 h, l;
+  split2(a, b, h, l);
+  hi = *(uint32_t *)&h;
+  lo = *(uint32_t *)&l;
+}
+__device__ __forceinline__ void st_shared_v4(void *p, const uint32_t (&v)[4]) {
+  asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};\n" ::"r"(smem_u32(p)), "r"(v[0]), "r"(v[1]), "r"(v[2]),
+               "r"(v[3])
+               : "memory");
+}
+
+constexpr int kPipeThreads = 512;
+
+// Named barrier 1..15 (0 is __syncthreads) over `count` threads.
+__device__ __forceinline__ void named_sync(int id, int count) {
+  asm volatile("bar.sync %0, %1;\n" ::"r"(id), "r"(count) : "memory");
+}
+
+// The persistent pipelined tensor-core kernels (P2M, M2M, L2L) run items (a
+// tile of leaves, or a group of consecutive parents, of one RHS) through three
+// roles, each item's buffers alternating between two sets: converter warps
+// turn the item's input into the FP16 hi/lo data operand [b] while the MMA
+// warp multiplies the previous item's operand [1-b] into TMEM accumulator 1-b
+// and the epilogue warps drain the accumulator of the item before that.
+// Hand-offs are mbarriers: zfull (the item's input landed), bfull / bfree
+// (operand written / consumed by the MMAs), tfull / tfree (accumulator
+// written / read out).  Every wait is bounded and gives up once any role has
+// given up.  The weight operand stays resident in shared memory.
+constexpr int kPipeConvWarps = 11;  // warps 0..10
+constexpr int kPipeMmaWarp = 11;    // warp 11
+constexpr int kPipeEpiWarp0 = 12;   // warps 12..15, one per TMEM lane quarter
+constexpr int kPipeConv = 32 * kPipeConvWarps;
+constexpr int kPipeEpi = kPipeThreads - 32 * kPipeEpiWarp0;
+constexpr int kPipeEpiGroups = kPipeEpi / 128;  // column groups of the accumulator
+
+// Barrier slots: A, zfull[2], bfull[2], bfree[2], tfull[2], tfree[2]; then
+// the TMEM base and the abort flag.
+struct PipeBars {
+  uint64_t *abar, *zfull, *bfull, *bfree, *tfull, *tfree;
+  uint32_t *tslot;
+  volatile int *abort;
+  __device__ explicit PipeBars(char *p) {
+    uint64_t *b = (uint64_t *)p;
+    abar = b;
+    zfull = b + 1;
+    bfull = b + 3;
+    bfree = b + 5;
+    tfull = b + 7;
+    tfree = b + 9;
+    tslot = (uint32_t *)(b + 11);
+    abort = (volatile int *)(b + 12);
+  }
+};
+
 }  // namespace tc
 }  // namespace isg

@@ -249,69 +249,6 @@ struct L2lArgs {
   int lvl_in;
 };
 
-// Splits (a, b), already scaled into the FP16 range, into packed hi and lo halves.
-__device__ __forceinline__ void split2(float a, float b, __half2 &hi, __half2 &lo) {
-  hi = __floats2half2_rn(a, b);
-  const float2 h = __half22float2(hi);
-  lo = __floats2half2_rn(a - h.x, b - h.y);
-}
-
-// The same split as packed 32-bit words (lo half = first value).
-__device__ __forceinline__ void split2u(float a, float b, uint32_t &hi, uint32_t &lo) {
-  __half2 h, l;
-  split2(a, b, h, l);
-  hi = *(uint32_t *)&h;
-  lo = *(uint32_t *)&l;
-}
-__device__ __forceinline__ void st_shared_v4(void *p, const uint32_t (&v)[4]) {
-  asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};\n" ::"r"(smem_u32(p)), "r"(v[0]), "r"(v[1]), "r"(v[2]),
-               "r"(v[3])
-               : "memory");
-}
-
-constexpr int kL2lThreads = 512;
-
-// Named barrier 1..15 (0 is __syncthreads) over `count` threads.
-__device__ __forceinline__ void named_sync(int id, int count) {
-  asm volatile("bar.sync %0, %1;\n" ::"r"(id), "r"(count) : "memory");
-}
-
-// The persistent tensor-core L2L and M2M kernels run items (groups of
-// consecutive parents of one RHS) through three roles, each item's buffers
-// alternating between two sets: converter warps turn the item's staged rings
-// into the FP16 hi/lo operand B[b] while the MMA warp multiplies the previous
-// item's B[1-b] into TMEM accumulator 1-b and the epilogue warps drain the
-// accumulator of the item before that.  Hand-offs are mbarriers: zfull (the
-// item's rings landed), bfull / bfree (operand written / consumed by the
-// MMAs), tfull / tfree (accumulator written / read out).  Every wait is
-// bounded and gives up once any role has given up.  The weight matrix A
-// (128 output samples x Kp input samples, FP16 hi/lo) stays resident.
-constexpr int kPipeConvWarps = 11;  // warps 0..10
-constexpr int kPipeMmaWarp = 11;    // warp 11
-constexpr int kPipeEpiWarp0 = 12;   // warps 12..15, one per TMEM lane quarter
-constexpr int kPipeConv = 32 * kPipeConvWarps;
-constexpr int kPipeEpi = kL2lThreads - 32 * kPipeEpiWarp0;
-constexpr int kPipeEpiGroups = kPipeEpi / 128;  // column groups of the accumulator
-
-// Barrier slots: A, zfull[2], bfull[2], bfree[2], tfull[2], tfree[2]; then
-// the TMEM base and the abort flag.
-struct PipeBars {
-  uint64_t *abar, *zfull, *bfull, *bfree, *tfull, *tfree;
-  uint32_t *tslot;
-  volatile int *abort;
-  __device__ explicit PipeBars(char *p) {
-    uint64_t *b = (uint64_t *)p;
-    abar = b;
-    zfull = b + 1;
-    bfull = b + 3;
-    bfree = b + 5;
-    tfull = b + 7;
-    tfree = b + 9;
-    tslot = (uint32_t *)(b + 11);
-    abort = (volatile int *)(b + 12);
-  }
-};
-
 // L2L layout: A hi/lo; B[2] hi/lo; the shifts [4][Kp + 2] (child-major,
 // padded against bank conflicts); two staging buffers, each the item's ppi
 // consecutive parent rings (one contiguous run) and Kp zero samples; barriers.
@@ -329,7 +266,7 @@ struct L2lSmem {
   }
 };
 
-__global__ void __launch_bounds__(kL2lThreads, 1) k_tc_l2l(L2lArgs A) {
+__global__ void __launch_bounds__(kPipeThreads, 1) k_tc_l2l(L2lArgs A) {
   extern __shared__ __align__(1024) char sm[];
   const L2lSmem L(A.Kp, A.ppi, A.ns_in);
   const int N = 8 * A.ppi, Kp = A.Kp, kc = Kp / 8, zs = A.ns_in;
@@ -536,7 +473,7 @@ struct M2mSmem {
   }
 };
 
-__global__ void __launch_bounds__(kL2lThreads, 1) k_tc_m2m(M2mArgs A) {
+__global__ void __launch_bounds__(kPipeThreads, 1) k_tc_m2m(M2mArgs A) {
   extern __shared__ __align__(1024) char sm[];
   const M2mSmem L(A.Kp, A.ppi, A.ns_in);
   const int N = 8 * A.ppi, Kp = A.Kp, kc = Kp / 8, zs = A.ns_in;
@@ -1046,7 +983,7 @@ bool band_m2m(isg_ctx *c, int lvl, float2 *mul, int nrhs, const int *active, cud
     A.lvl_in = lvl + 1;
     A.lvl_out = lvl;
     count_launch();
-    k_tc_m2m<<<std::min(A.nitems, c->band->sms), kL2lThreads, M2mSmem(T.Kp, T.ppi, ch.ns).total, st>>>(A);
+    k_tc_m2m<<<std::min(A.nitems, c->band->sms), kPipeThreads, M2mSmem(T.Kp, T.ppi, ch.ns).total, st>>>(A);
     *e = cuda_check(c, cudaGetLastError(), "m2m launch");
     return true;
   }
@@ -1085,7 +1022,7 @@ bool band_l2l(isg_ctx *c, int lvl, float2 *loc, int nrhs, const int *active, cud
   A.active = active;
   A.err = c->tc_err_flag();
   count_launch();
-  k_tc_l2l<<<std::min(A.nitems, c->band->sms), kL2lThreads, L2lSmem(T.Kp, T.ppi, p.ns).total, st>>>(A);
+  k_tc_l2l<<<std::min(A.nitems, c->band->sms), kPipeThreads, L2lSmem(T.Kp, T.ppi, p.ns).total, st>>>(A);
   *e = cuda_check(c, cudaGetLastError(), "l2l launch");
   return true;
 }
