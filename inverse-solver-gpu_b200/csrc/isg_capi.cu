@@ -577,6 +577,16 @@ isg_status isg_time_stages(isg_ctx *c, int nrhs, int engine, int reps, double *m
   A.dot_a = c->wx;
   A.part = c->part;
   const bool tc = engine == ISG_ENGINE_TENSOR;
+  if (tc) {
+    // as in a forward tensor-engine solve: the vector updates already formed g x
+    // (wx stands in for it), so P2M and the near field read it plainly and the
+    // epilogue takes x separately
+    B.g = nullptr;
+    B.gstride = 0;
+    B.mode = IN_PLAIN;
+    A.in = B;
+    A.x_epi = c->wx;
+  }
   for (int r = -1; r < reps; r++) {
     cudaEventRecord(ev[0], st);
     if (tc) {

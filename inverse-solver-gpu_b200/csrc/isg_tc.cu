@@ -635,18 +635,22 @@ __global__ void __launch_bounds__(256, 1) k_tc_p2m(TcP2mArgs A) {
 struct P2mPipeSmem {
   __host__ __device__ static size_t a(int b) { return (size_t)b * 2 * kP2mA; }  // hi, then lo kP2mA on
   __host__ __device__ static size_t bst() { return 4 * (size_t)kP2mA; }
-  // per epilogue warp: 32 leaves x 16 complex (+1 pad)
+  // per epilogue warp: 32 leaves x 8 complex (+1 pad)
   __host__ __device__ static size_t epi(int stage_bytes) { return bst() + 4 * (size_t)stage_bytes; }
-  __host__ __device__ static size_t bar(int stage_bytes) { return epi(stage_bytes) + 4 * 32 * 17 * 8; }
+  __host__ __device__ static size_t bar(int stage_bytes) { return epi(stage_bytes) + 8 * 32 * 9 * 8; }
   __host__ __device__ static size_t total(int stage_bytes) { return bar(stage_bytes) + 256; }
 };
-constexpr int kP2mUnits = 128 * 16;                               // (leaf, 4-pixel chunk) per item
-constexpr int kP2mPer = (kP2mUnits + kPipeConv - 1) / kPipeConv;  // units per converter thread
+// Roles: converters warps 0..7, MMA warp 8, epilogue warps 9..16 (two per
+// TMEM lane quarter warp % 4, each taking every other 16-column chunk).
+constexpr int kP2mConvWarps = 8, kP2mMmaWarp = 8, kP2mEpiWarp0 = 9, kP2mThreads = 17 * 32;
+constexpr int kP2mConv = 32 * kP2mConvWarps, kP2mEpi = kP2mThreads - 32 * kP2mEpiWarp0;
+constexpr int kP2mUnits = 128 * 16;                             // (leaf, 4-pixel chunk) per item
+constexpr int kP2mPer = (kP2mUnits + kP2mConv - 1) / kP2mConv;  // units per converter thread
 
-__global__ void __launch_bounds__(kPipeThreads, 1) k_tc_p2m_pipe(TcP2mArgs A) {
+__global__ void __launch_bounds__(kP2mThreads, 1) k_tc_p2m_pipe(TcP2mArgs A) {
   extern __shared__ __align__(1024) char sm[];
   const PipeBars Bq(sm + P2mPipeSmem::bar(A.stage_bytes));
-  float *fscr = (float *)(Bq.abar + 16);  // [kPipeConvWarps] converter maxima
+  float *fscr = (float *)(Bq.abar + 16);  // [kP2mConvWarps] converter maxima
   float *sval = fscr + 16;                // [2] the scale of the item in buffer b
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
@@ -665,43 +669,54 @@ __global__ void __launch_bounds__(kPipeThreads, 1) k_tc_p2m_pipe(TcP2mArgs A) {
     return w;
   };
   const int first = (A.active && !A.active[blockIdx.x / A.tiles]) ? next_item(blockIdx.x) : blockIdx.x;
+  // an item's pixels (its leaves are one contiguous run) into operand buffer b, as FP32
+  auto stage = [&](int w, int b) {
+    const int rhs = w / A.tiles, leaf0 = (w % A.tiles) * 128;
+    const uint32_t bytes = (uint32_t)min(128, A.nleaves - leaf0) * kBB * 8;
+    mbar_expect_tx(Bq.zfull + b, bytes);
+    bulk_g2s(sm + P2mPipeSmem::a(b), A.x + (size_t)rhs * A.U + (size_t)leaf0 * kBB, bytes, Bq.zfull + b);
+  };
 
-  if (warp < kPipeConvWarps) {
+  if (warp < kP2mConvWarps) {
     // ---- converters ----
     if (threadIdx.x == 0) {
       mbar_expect_tx(Bq.abar, 4 * A.stage_bytes);
       for (int c = 0; c < 4; c++)
         bulk_g2s(sm + P2mPipeSmem::bst() + c * A.stage_bytes, A.B + (size_t)c * A.stage_bytes, A.stage_bytes,
                  Bq.abar);
+      if (first < A.nitems) {
+        stage(first, 0);
+        const int second = next_item(first);
+        if (second < A.nitems) stage(second, 1);
+      }
     }
     int w = first;
     for (int it = 0; w < A.nitems; it++) {
       const int b = it & 1, ph = (it >> 1) & 1;
-      // the buffer and its scale slot are free once the epilogue of item it - 2 is done
-      const bool fok = mbar_wait_or(Bq.tfree + b, ph ^ 1, Bq.abort, A.err, kErrP2m);
-      const int rhs = w / A.tiles, leaf0 = (w % A.tiles) * 128;
-      const size_t rbase = (size_t)rhs * A.U;
-      const float2 *gr = A.g ? A.g + rhs * A.gstride : nullptr;
+      // the staged pixels, and the scale slot (free once the epilogue of item it - 2 is done)
+      const bool fok = mbar_wait_or(Bq.zfull + b, ph, Bq.abort, A.err, kErrP2m) &&
+                       mbar_wait_or(Bq.tfree + b, ph ^ 1, Bq.abort, A.err, kErrP2m);
+      const int leaf0 = (w % A.tiles) * 128;
+      const float4 *zst = (const float4 *)(sm + P2mPipeSmem::a(b));  // [leaf][32 float4]
       float2 v[kP2mPer][4];
       float mx = 0.f;
 #pragma unroll
       for (int r = 0; r < kP2mPer; r++) {
-        const int u = threadIdx.x + r * kPipeConv;
-        const int m = ((u >> 7) << 3) | (u & 7), c = (u >> 3) & 15, leaf = leaf0 + m;
+        const int u = threadIdx.x + r * kP2mConv;
+        const int m = ((u >> 7) << 3) | (u & 7), c = (u >> 3) & 15;
 #pragma unroll
         for (int p = 0; p < 4; p++) v[r][p] = make_float2(0.f, 0.f);
-        if (u < kP2mUnits && leaf < A.nleaves) {
-          const size_t i = (size_t)leaf * kBB + 4 * c;
-          const float4 a0 = *(const float4 *)(A.x + rbase + i), a1 = *(const float4 *)(A.x + rbase + i + 2);
-          float4 g0 = make_float4(0.f, 0.f, 0.f, 0.f), g1 = g0;
-          if (A.mode == IN_G) {
-            g0 = *(const float4 *)(gr + i);
-            g1 = *(const float4 *)(gr + i + 2);
-          }
-          v[r][0] = transform(make_float2(a0.x, a0.y), make_float2(g0.x, g0.y), A.mode);
-          v[r][1] = transform(make_float2(a0.z, a0.w), make_float2(g0.z, g0.w), A.mode);
-          v[r][2] = transform(make_float2(a1.x, a1.y), make_float2(g1.x, g1.y), A.mode);
-          v[r][3] = transform(make_float2(a1.z, a1.w), make_float2(g1.z, g1.w), A.mode);
+        if (u < kP2mUnits && leaf0 + m < A.nleaves) {
+          // odd leaves read their two halves in the other order: the 16-byte loads of a
+          // warp then fall on 8 distinct bank groups
+          const int odd = m & 1;
+          const float4 x0 = zst[m * 32 + 2 * c + odd], x1 = zst[m * 32 + 2 * c + 1 - odd];
+          const float4 a0 = odd ? x1 : x0, a1 = odd ? x0 : x1;
+          const float2 g0 = make_float2(0.f, 0.f);
+          v[r][0] = transform(make_float2(a0.x, a0.y), g0, A.mode);
+          v[r][1] = transform(make_float2(a0.z, a0.w), g0, A.mode);
+          v[r][2] = transform(make_float2(a1.x, a1.y), g0, A.mode);
+          v[r][3] = transform(make_float2(a1.z, a1.w), g0, A.mode);
 #pragma unroll
           for (int p = 0; p < 4; p++) mx = fmaxf(mx, cabs1(v[r][p]));
         }
@@ -709,15 +724,15 @@ __global__ void __launch_bounds__(kPipeThreads, 1) k_tc_p2m_pipe(TcP2mArgs A) {
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
       if (lane == 0) fscr[warp] = mx;
-      named_sync(1, kPipeConv);
+      named_sync(1, kP2mConv);  // every staged value is in registers: the buffer is rewritten in place
       float m2 = 0.f;
-      for (int k = 0; k < kPipeConvWarps; k++) m2 = fmaxf(m2, fscr[k]);
+      for (int k = 0; k < kP2mConvWarps; k++) m2 = fmaxf(m2, fscr[k]);
       const float s = pow2_scale(m2);
       char *ahi = sm + P2mPipeSmem::a(b), *alo = ahi + kP2mA;
       if (fok) {
 #pragma unroll
         for (int r = 0; r < kP2mPer; r++) {
-          const int u = threadIdx.x + r * kPipeConv;
+          const int u = threadIdx.x + r * kP2mConv;
           if (u >= kP2mUnits) continue;
           uint32_t h[4], l[4];
 #pragma unroll
@@ -728,11 +743,11 @@ __global__ void __launch_bounds__(kPipeThreads, 1) k_tc_p2m_pipe(TcP2mArgs A) {
       }
       if (threadIdx.x == 0) sval[b] = s;
       fence_proxy_async();
-      named_sync(1, kPipeConv);  // the operand is written; fscr may be reused
+      named_sync(1, kP2mConv);  // the operand is written; fscr may be reused
       if (threadIdx.x == 0) mbar_arrive(Bq.bfull + b);
       w = next_item(w);
     }
-  } else if (warp == kPipeMmaWarp) {
+  } else if (warp == kP2mMmaWarp) {
     // ---- MMA issue: D[128 leaves][npad] = A[b] (hi/lo) x coefficients (hi/lo) ----
     const uint32_t idesc = idesc_f16_f32(128, A.npad), sbase = smem_u32(sm);
     const uint64_t bh0 = smem_desc(sbase + (uint32_t)P2mPipeSmem::bst(), 128, 512);
@@ -763,41 +778,40 @@ __global__ void __launch_bounds__(kPipeThreads, 1) k_tc_p2m_pipe(TcP2mArgs A) {
       w = next_item(w);
     }
   } else {
-    // ---- epilogue: lane = leaf, columns 2k (re), 2k + 1 (im).  Each 32-column chunk
-    // (16 samples of the warp's 32 consecutive leaves) goes through a padded
-    // shared tile so that 16 lanes write one leaf's 128 contiguous bytes ----
-    const int qd = warp - kPipeEpiWarp0;
-    float2 *tile = (float2 *)(sm + P2mPipeSmem::epi(A.stage_bytes)) + qd * 32 * 17;
-    int w = first;
+    // ---- epilogue: lane = leaf, columns 2k (re), 2k + 1 (im).  Each 16-column chunk
+    // (8 samples of the warp's 32 consecutive leaves) goes through a padded
+    // shared tile so that 8 lanes write one leaf's 64 contiguous bytes ----
+    const int ew = warp - kP2mEpiWarp0, qd = warp & 3, eg = ew >> 2;  // lane quarter, chunk parity
+    float2 *tile = (float2 *)(sm + P2mPipeSmem::epi(A.stage_bytes)) + ew * 32 * 9;
+    int w = first, w2 = first < A.nitems ? next_item(next_item(first)) : A.nitems;
     for (int it = 0; w < A.nitems; it++) {
       const int b = it & 1, ph = (it >> 1) & 1;
       // tfull: the accumulator; bfull (already complete): the item's scale is visible
       const bool ok = mbar_wait_or(Bq.tfull + b, ph, Bq.abort, A.err, kErrP2m) &&
                       mbar_wait_or(Bq.bfull + b, ph, Bq.abort, A.err, kErrP2m);
       tc_fence_after();
+      // the MMAs are done with operand buffer b: item it + 2's pixels go there now
+      if (ew == 0 && lane == 0 && w2 < A.nitems) stage(w2, b);
+      w2 = w2 < A.nitems ? next_item(w2) : A.nitems;
       const int rhs = w / A.tiles, leafw = (w % A.tiles) * 128 + 32 * qd;  // the warp's first leaf
       const float inv = A.inv_c / sval[b];
       float2 *outw = A.mul_leaf + (size_t)rhs * A.mp + (size_t)leafw * A.ns;
       float omx = 0.f;
       const uint32_t taddr = tmem + ((uint32_t)(32 * qd) << 16) + (uint32_t)(b * 256);
-      for (int c0 = 0; c0 < A.npad; c0 += 32) {
-        float d[32];
-        if (c0 + 32 <= A.npad) {
-          tmem_ld32(taddr + c0, d);
-        } else {
-          tmem_ld16(taddr + c0, d);
-        }
-        const int k0 = c0 / 2, nk = min(16, A.ns - k0);
+      for (int c0 = 16 * eg; c0 < A.npad; c0 += 32) {
+        float d[16];
+        tmem_ld16(taddr + c0, d);
+        const int k0 = c0 / 2, nk = min(8, A.ns - k0);
 #pragma unroll
-        for (int j = 0; j < 16; j++)
-          if (j < nk) tile[lane * 17 + j] = make_float2(d[2 * j] * inv, d[2 * j + 1] * inv);
+        for (int j = 0; j < 8; j++)
+          if (j < nk) tile[lane * 9 + j] = make_float2(d[2 * j] * inv, d[2 * j + 1] * inv);
         __syncwarp();
         if (ok) {
 #pragma unroll
-          for (int r = 0; r < 16; r++) {  // element r * 32 + lane: leaf e / 16, sample e % 16
-            const int e = r * 32 + lane, lf = e >> 4, j = e & 15;
+          for (int r = 0; r < 8; r++) {  // element r * 32 + lane: leaf e / 8, sample e % 8
+            const int e = r * 32 + lane, lf = e >> 3, j = e & 7;
             if (j < nk && leafw + lf < A.nleaves) {
-              const float2 o = tile[lf * 17 + j];
+              const float2 o = tile[lf * 9 + j];
               outw[(size_t)lf * A.ns + k0 + j] = o;
               omx = fmaxf(omx, fmaxf(fabsf(o.x), fabsf(o.y)));
             }
@@ -806,8 +820,8 @@ __global__ void __launch_bounds__(kPipeThreads, 1) k_tc_p2m_pipe(TcP2mArgs A) {
         __syncwarp();
       }
       tc_fence_before();
-      named_sync(2, kPipeEpi);  // the accumulator is read out
-      if (qd == 0 && lane == 0) mbar_arrive(Bq.tfree + b);
+      named_sync(2, kP2mEpi);  // the accumulator is read out
+      if (ew == 0 && lane == 0) mbar_arrive(Bq.tfree + b);
       const unsigned mbits = __reduce_max_sync(0xffffffffu, __float_as_uint(omx));  // omx >= 0
       if (lane == 0 && ok && mbits) atomicMax(&A.levmax[rhs * kMaxLevels + A.lvl], mbits);
       w = next_item(w);
@@ -1028,7 +1042,10 @@ isg_status tc_p2m(isg_ctx *c, const BatchArgs &B, float2 *mul, cudaStream_t st) 
   count_launch();
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->opts.device);
-  k_tc_p2m_pipe<<<std::min(A.nitems, sms), kPipeThreads, P2mPipeSmem::total(T.p2m_stage), st>>>(A);
+  if (B.mode == IN_G)  // the pipelined kernel stages x alone
+    k_tc_p2m<<<std::min(A.nitems, sms), 256, P2mSmem::total(T.p2m_stage, A.ns), st>>>(A);
+  else
+    k_tc_p2m_pipe<<<std::min(A.nitems, sms), kP2mThreads, P2mPipeSmem::total(T.p2m_stage), st>>>(A);
   return cuda_check(c, cudaGetLastError(), "tc p2m launch");
 }
 
