@@ -203,6 +203,16 @@ __device__ __forceinline__ void named_sync(int id, int count) {
 // (operand written / consumed by the MMAs), tfull / tfree (accumulator
 // written / read out).  Every wait is bounded and gives up once any role has
 // given up.  The weight operand stays resident in shared memory.
+// A role split: CONV converter warps (0 .. CONV-1), one MMA warp (CONV), EPI
+// epilogue warps after it (a multiple of 4; the TMEM lane quarter of warp w is
+// w % 4, and the epilogue warps of one quarter split the columns in EPI / 4
+// groups).
+template <int CONV, int EPI>
+struct PipeRoles {
+  static constexpr int conv_warps = CONV, mma_warp = CONV, epi_warp0 = CONV + 1;
+  static constexpr int threads = 32 * (CONV + 1 + EPI), conv = 32 * CONV, epi = 32 * EPI, epi_groups = EPI / 4;
+};
+
 constexpr int kPipeConvWarps = 11;  // warps 0..10
 constexpr int kPipeMmaWarp = 11;    // warp 11
 constexpr int kPipeEpiWarp0 = 12;   // warps 12..15, one per TMEM lane quarter

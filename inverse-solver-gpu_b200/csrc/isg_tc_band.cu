@@ -249,6 +249,9 @@ struct L2lArgs {
   int lvl_in;
 };
 
+using L2lRoles = PipeRoles<8, 8>;
+using M2mRoles = PipeRoles<11, 4>;
+
 // L2L layout: A hi/lo; B[2] hi/lo; the shifts [4][Kp + 2] (child-major,
 // padded against bank conflicts); two staging buffers, each the item's ppi
 // consecutive parent rings (one contiguous run) and Kp zero samples; barriers.
@@ -266,7 +269,8 @@ struct L2lSmem {
   }
 };
 
-__global__ void __launch_bounds__(kPipeThreads, 1) k_tc_l2l(L2lArgs A) {
+template <class R>
+__global__ void __launch_bounds__(R::threads, 1) k_tc_l2l(L2lArgs A) {
   extern __shared__ __align__(1024) char sm[];
   const L2lSmem L(A.Kp, A.ppi, A.ns_in);
   const int N = 8 * A.ppi, Kp = A.Kp, kc = Kp / 8, zs = A.ns_in;
@@ -310,7 +314,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) k_tc_l2l(L2lArgs A) {
   };
   const int ngroups = A.ppi * kc;
 
-  if (warp < kPipeConvWarps) {
+  if (warp < R::conv_warps) {
     // ---- converters: B[b] rows 8 parent + 2 q + (re, im) = shl[q][j] z[j] s ----
     if (warp == 0) {
       if (lane == 0) {
@@ -333,7 +337,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) k_tc_l2l(L2lArgs A) {
         // a unit is one child q of one core-matrix group (8 samples of one parent):
         // both rows, hi and lo
 #pragma unroll 2
-        for (int u = threadIdx.x; u < 4 * ngroups; u += kPipeConv) {
+        for (int u = threadIdx.x; u < 4 * ngroups; u += R::conv) {
           const int q = u & 3, cm = u >> 2;
           const int pl = (int)__umulhi((unsigned)cm, A.kc_magic), j0 = 8 * (cm - pl * kc);
           const float4 *zp = (const float4 *)(zst + pl * zs + j0);
@@ -355,13 +359,13 @@ __global__ void __launch_bounds__(kPipeThreads, 1) k_tc_l2l(L2lArgs A) {
         }
       }
       fence_proxy_async();
-      named_sync(1, kPipeConv);  // every converter is done with zbuf(b) and B[b]
+      named_sync(1, R::conv);  // every converter is done with zbuf(b) and B[b]
       if (threadIdx.x == 0) mbar_arrive(Bq.bfull + b);
       if (warp == 0 && w2 < A.nitems) stage(w2, b);
       w = next_item(w);
       w2 = w2 < A.nitems ? next_item(w2) : A.nitems;
     }
-  } else if (warp == kPipeMmaWarp) {
+  } else if (warp == R::mma_warp) {
     // ---- MMA issue ----
     const uint32_t idesc = idesc_f16_f32(128, N);
     const uint32_t sbo = (uint32_t)kc * 128, sbase = smem_u32(sm);
@@ -394,7 +398,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) k_tc_l2l(L2lArgs A) {
     }
   } else {
     // ---- epilogue: lane = child sample, 16 columns = 2 parents x 4 children x (re, im) ----
-    const int ew = warp - kPipeEpiWarp0, qd = ew & 3, ch0 = ew >> 2;  // lane quarter, column group
+    const int ew = warp - R::epi_warp0, qd = warp & 3, ch0 = ew >> 2;  // lane quarter, column group
     const int km = 32 * qd + lane;
     const int nc = 2 << A.lg_np, npm = (1 << A.lg_np) - 1;
     const int so = A.ns_out, qoff[4] = {0, so, nc * so, nc * so + so};
@@ -408,8 +412,8 @@ __global__ void __launch_bounds__(kPipeThreads, 1) k_tc_l2l(L2lArgs A) {
       // the item's parents share a row: parent p0 + pl's first child is 2 pl clusters on
       float2 *ob = A.loc + (size_t)rhs * A.mp + A.off_out + km +
                    (size_t)(2 * (p0 >> A.lg_np) * nc + 2 * (p0 & npm)) * so;
-      for (int cg = 0; cg < N / (32 * kPipeEpiGroups); cg++) {  // 32 columns = 4 parents
-        const int col0 = ch0 * (N / kPipeEpiGroups) + 32 * cg;
+      for (int cg = 0; cg < N / (32 * R::epi_groups); cg++) {  // 32 columns = 4 parents
+        const int col0 = ch0 * (N / R::epi_groups) + 32 * cg;
         float d[32];
         tmem_ld32(tmem + ((uint32_t)(32 * qd) << 16) + (uint32_t)(b * N + col0), d);
         if (!ok || km >= A.ns_out) continue;
@@ -421,7 +425,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) k_tc_l2l(L2lArgs A) {
         }
       }
       tc_fence_before();
-      named_sync(2, kPipeEpi);  // the accumulator is read out
+      named_sync(2, R::epi);  // the accumulator is read out
       if (ew == 0 && lane == 0) mbar_arrive(Bq.tfree + b);
       w = next_item(w);
     }
@@ -473,7 +477,8 @@ struct M2mSmem {
   }
 };
 
-__global__ void __launch_bounds__(kPipeThreads, 1) k_tc_m2m(M2mArgs A) {
+template <class R>
+__global__ void __launch_bounds__(R::threads, 1) k_tc_m2m(M2mArgs A) {
   extern __shared__ __align__(1024) char sm[];
   const M2mSmem L(A.Kp, A.ppi, A.ns_in);
   const int N = 8 * A.ppi, Kp = A.Kp, kc = Kp / 8, zs = A.ns_in;
@@ -521,7 +526,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) k_tc_m2m(M2mArgs A) {
   };
   const int ngroups = A.ppi * kc;  // core-matrix groups of B (8 rows x 8 samples)
 
-  if (warp < kPipeConvWarps) {
+  if (warp < R::conv_warps) {
     // ---- converters: B[b] rows 8 parent + 2 q + (re, im) = child q's samples times s ----
     if (warp == 0) {
       if (lane == 0) {
@@ -543,7 +548,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) k_tc_m2m(M2mArgs A) {
       char *bhi = bbuf(b), *blo = bhi + (size_t)N * Kp * 2;
       if (zok && bok) {
 #pragma unroll 2
-        for (int u = threadIdx.x; u < 4 * ngroups; u += kPipeConv) {
+        for (int u = threadIdx.x; u < 4 * ngroups; u += R::conv) {
           const int q = u & 3, cm = u >> 2;
           const int pl = (int)__umulhi((unsigned)cm, A.kc_magic), j8 = cm - pl * kc;
           const int slot = (q >> 1) * 2 * A.ppi + 2 * pl + (q & 1);
@@ -563,13 +568,13 @@ __global__ void __launch_bounds__(kPipeThreads, 1) k_tc_m2m(M2mArgs A) {
         }
       }
       fence_proxy_async();
-      named_sync(1, kPipeConv);  // every converter is done with zbuf(b) and B[b]
+      named_sync(1, R::conv);  // every converter is done with zbuf(b) and B[b]
       if (threadIdx.x == 0) mbar_arrive(bfull + b);
       if (warp == 0 && w2 < A.nitems) stage(w2, b);
       w = next_item(w);
       w2 = w2 < A.nitems ? next_item(w2) : A.nitems;
     }
-  } else if (warp == kPipeMmaWarp) {
+  } else if (warp == R::mma_warp) {
     // ---- MMA issue ----
     const uint32_t idesc = idesc_f16_f32(128, N);
     const uint32_t sbo = (uint32_t)kc * 128, sbase = smem_u32(sm);
@@ -602,7 +607,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) k_tc_m2m(M2mArgs A) {
     }
   } else {
     // ---- epilogue: lane = parent sample, 16 columns = 2 parents x 4 children x (re, im) ----
-    const int ew = warp - kPipeEpiWarp0, qd = ew & 3, ch0 = ew >> 2;  // lane quarter, column group
+    const int ew = warp - R::epi_warp0, qd = warp & 3, ch0 = ew >> 2;  // lane quarter, column group
     const int km = 32 * qd + lane;
     float2 shq[4];
 #pragma unroll
@@ -616,8 +621,8 @@ __global__ void __launch_bounds__(kPipeThreads, 1) k_tc_m2m(M2mArgs A) {
       const float inv = A.inv_a / scale_of(w);
       float2 *obase = A.mul + (size_t)rhs * A.mp + A.off_out + km;
       float omx = 0.f;
-      for (int cg = 0; cg < N / (32 * kPipeEpiGroups); cg++) {  // 32 columns = 4 parents
-        const int col0 = ch0 * (N / kPipeEpiGroups) + 32 * cg;
+      for (int cg = 0; cg < N / (32 * R::epi_groups); cg++) {  // 32 columns = 4 parents
+        const int col0 = ch0 * (N / R::epi_groups) + 32 * cg;
         float d[32];
         tmem_ld32(tmem + ((uint32_t)(32 * qd) << 16) + (uint32_t)(b * N + col0), d);
         if (!ok || km >= A.ns_out) continue;
@@ -633,7 +638,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) k_tc_m2m(M2mArgs A) {
         }
       }
       tc_fence_before();
-      named_sync(2, kPipeEpi);  // the accumulator is read out
+      named_sync(2, R::epi);  // the accumulator is read out
       if (ew == 0 && lane == 0) mbar_arrive(tfree + b);
       // the parent level's maximum for the next transition (omx >= 0: bits order as values)
       const unsigned mbits = __reduce_max_sync(0xffffffffu, __float_as_uint(omx));
@@ -893,17 +898,17 @@ isg_status band_setup(isg_ctx *c) {
           ISG_OK ||
       (e = cuda_check(c, cudaDeviceGetAttribute(&c->band->sms, cudaDevAttrMultiProcessorCount, dev), "attr")) !=
           ISG_OK ||
-      (e = cuda_check(c, cudaFuncGetAttributes(&fa, k_tc_l2l), "l2l attr")) != ISG_OK)
+      (e = cuda_check(c, cudaFuncGetAttributes(&fa, k_tc_l2l<L2lRoles>), "l2l attr")) != ISG_OK)
     return e;
   const size_t cap = (size_t)optin - fa.sharedSizeBytes;
   for (int i = 3; i < L; i++)  // L2L into child level i
     if ((e = build_l2l(c, i, cap)) != ISG_OK) return e;
   for (int i = 2; i <= L - 2; i++)  // persistent M2M into parent level i
     if ((e = build_m2m(c, i, cap)) != ISG_OK) return e;
-  if ((e = cuda_check(c, cudaFuncSetAttribute(k_tc_m2m, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap),
+  if ((e = cuda_check(c, cudaFuncSetAttribute(k_tc_m2m<M2mRoles>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap),
                       "m2m attr")) != ISG_OK)
     return e;
-  if ((e = cuda_check(c, cudaFuncSetAttribute(k_tc_l2l, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap),
+  if ((e = cuda_check(c, cudaFuncSetAttribute(k_tc_l2l<L2lRoles>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap),
                       "l2l attr")) != ISG_OK)
     return e;
   return cuda_check(c, cudaFuncSetAttribute(k_tc_band, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem),
@@ -983,7 +988,7 @@ bool band_m2m(isg_ctx *c, int lvl, float2 *mul, int nrhs, const int *active, cud
     A.lvl_in = lvl + 1;
     A.lvl_out = lvl;
     count_launch();
-    k_tc_m2m<<<std::min(A.nitems, c->band->sms), kPipeThreads, M2mSmem(T.Kp, T.ppi, ch.ns).total, st>>>(A);
+    k_tc_m2m<M2mRoles><<<std::min(A.nitems, c->band->sms), M2mRoles::threads, M2mSmem(T.Kp, T.ppi, ch.ns).total, st>>>(A);
     *e = cuda_check(c, cudaGetLastError(), "m2m launch");
     return true;
   }
@@ -1022,7 +1027,7 @@ bool band_l2l(isg_ctx *c, int lvl, float2 *loc, int nrhs, const int *active, cud
   A.active = active;
   A.err = c->tc_err_flag();
   count_launch();
-  k_tc_l2l<<<std::min(A.nitems, c->band->sms), kPipeThreads, L2lSmem(T.Kp, T.ppi, p.ns).total, st>>>(A);
+  k_tc_l2l<L2lRoles><<<std::min(A.nitems, c->band->sms), L2lRoles::threads, L2lSmem(T.Kp, T.ppi, p.ns).total, st>>>(A);
   *e = cuda_check(c, cudaGetLastError(), "l2l launch");
   return true;
 }
