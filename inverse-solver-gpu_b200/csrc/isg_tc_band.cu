@@ -449,9 +449,9 @@ constexpr int kErrM2m = 123;
 struct M2mArgs {
   float2 *mul;  // every level's multipoles; children at off_in, parents at off_out
   size_t mp, off_in, off_out;
-  int lg_np, ns_in, ns_out, Kp, ppi;
+  int lg_np, ns_in, ns_out, Kp, ppi, mt;  // mt: 128-sample tiles of the parent ring (1 or 2)
   unsigned kc_magic;
-  const uint8_t *A;    // [128 x Kp] FP16 hi then lo
+  const uint8_t *A;    // per tile, [128 x Kp] FP16 hi then lo
   const float2 *shm;   // [4][ns_out] multipole shifts of the parent level
   float inv_a;
   int nparents, items_per_rhs, nitems;
@@ -466,9 +466,9 @@ struct M2mArgs {
 // contiguous run), each buffer followed by Kp zero samples; barriers and flags.
 struct M2mSmem {
   size_t a, b, bbuf, z, zbuf, bar, total;
-  __host__ __device__ M2mSmem(int Kp, int ppi, int ns) {
+  __host__ __device__ M2mSmem(int Kp, int ppi, int ns, int mt) {
     a = 0;
-    b = a + (size_t)512 * Kp;
+    b = a + (size_t)512 * Kp * mt;
     bbuf = (size_t)32 * ppi * Kp;
     z = b + 2 * bbuf;
     zbuf = ((size_t)(4 * ppi * ns + Kp) * 8 + 127) & ~(size_t)127;
@@ -480,7 +480,7 @@ struct M2mSmem {
 template <class R>
 __global__ void __launch_bounds__(R::threads, 1) k_tc_m2m(M2mArgs A) {
   extern __shared__ __align__(1024) char sm[];
-  const M2mSmem L(A.Kp, A.ppi, A.ns_in);
+  const M2mSmem L(A.Kp, A.ppi, A.ns_in, A.mt);
   const int N = 8 * A.ppi, Kp = A.Kp, kc = Kp / 8, zs = A.ns_in;
   uint64_t *bars = (uint64_t *)(sm + L.bar);
   uint64_t *abar = bars, *zfull = bars + 1, *bfull = bars + 3, *bfree = bars + 5, *tfull = bars + 7,
@@ -495,7 +495,7 @@ __global__ void __launch_bounds__(R::threads, 1) k_tc_m2m(M2mArgs A) {
     *abort = 0;
     fence_mbar_init();
   }
-  if (warp == 0) tmem_alloc(tslot, 2 * N);
+  if (warp == 0) tmem_alloc(tslot, 2 * A.mt * N);
   // zero both buffers: the tails past the last ring are read (against zero weights) and stay 0
   for (int e = threadIdx.x; e < (int)(2 * L.zbuf / 4); e += blockDim.x) ((float *)zbuf(0))[e] = 0.f;
   tc_fence_before();
@@ -530,8 +530,8 @@ __global__ void __launch_bounds__(R::threads, 1) k_tc_m2m(M2mArgs A) {
     // ---- converters: B[b] rows 8 parent + 2 q + (re, im) = child q's samples times s ----
     if (warp == 0) {
       if (lane == 0) {
-        mbar_expect_tx(abar, 512 * Kp);
-        bulk_g2s(sm + L.a, A.A, 512 * Kp, abar);
+        mbar_expect_tx(abar, 512 * Kp * A.mt);
+        bulk_g2s(sm + L.a, A.A, 512 * Kp * A.mt, abar);
       }
       __syncwarp();
       if (first < A.nitems) stage(first, 0);
@@ -580,6 +580,7 @@ __global__ void __launch_bounds__(R::threads, 1) k_tc_m2m(M2mArgs A) {
     const uint32_t sbo = (uint32_t)kc * 128, sbase = smem_u32(sm);
     const uint64_t ah = smem_desc(sbase + (uint32_t)L.a, 128, sbo);
     const uint64_t al = smem_desc(sbase + (uint32_t)L.a + 256 * Kp, 128, sbo);
+    const uint32_t tile_bytes = 512 * Kp;  // hi and lo of one 128-sample tile
     const bool aok = mbar_wait_or(abar, 0, abort, A.err, kErrM2m);
     int w = first;
     for (int it = 0; w < A.nitems; it++) {
@@ -591,12 +592,14 @@ __global__ void __launch_bounds__(R::threads, 1) k_tc_m2m(M2mArgs A) {
         if (ok) {
           const uint64_t bh = smem_desc(smem_u32(bbuf(b)), 128, sbo);
           const uint64_t bl = smem_desc(smem_u32(bbuf(b)) + N * Kp * 2, 128, sbo);
-          const uint32_t d = tmem + (uint32_t)(b * N);
-          for (int ks = 0; ks < Kp / 16; ks++) {
-            const uint32_t k = ks * 256;
-            mma_f16(d, desc_add(ah, k), desc_add(bh, k), idesc, ks ? 1 : 0);
-            mma_f16(d, desc_add(ah, k), desc_add(bl, k), idesc, 1);
-            mma_f16(d, desc_add(al, k), desc_add(bh, k), idesc, 1);
+          for (int t = 0; t < A.mt; t++) {
+            const uint32_t d = tmem + (uint32_t)((b * A.mt + t) * N), ta = t * tile_bytes;
+            for (int ks = 0; ks < Kp / 16; ks++) {
+              const uint32_t k = ks * 256;
+              mma_f16(d, desc_add(ah, ta + k), desc_add(bh, k), idesc, ks ? 1 : 0);
+              mma_f16(d, desc_add(ah, ta + k), desc_add(bl, k), idesc, 1);
+              mma_f16(d, desc_add(al, ta + k), desc_add(bh, k), idesc, 1);
+            }
           }
         }
         mma_commit(bfree + b);
@@ -606,12 +609,16 @@ __global__ void __launch_bounds__(R::threads, 1) k_tc_m2m(M2mArgs A) {
       w = next_item(w);
     }
   } else {
-    // ---- epilogue: lane = parent sample, 16 columns = 2 parents x 4 children x (re, im) ----
+    // ---- epilogue: lane = parent sample (of tile t), 32 columns = 4 parents x 4 children x (re, im) ----
     const int ew = warp - R::epi_warp0, qd = warp & 3, ch0 = ew >> 2;  // lane quarter, column group
-    const int km = 32 * qd + lane;
-    float2 shq[4];
+    float2 shq[2][4];
 #pragma unroll
-    for (int q = 0; q < 4; q++) shq[q] = km < A.ns_out ? __ldg(A.shm + q * A.ns_out + km) : make_float2(0.f, 0.f);
+    for (int t = 0; t < 2; t++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int km = 128 * t + 32 * qd + lane;
+        shq[t][q] = t < A.mt && km < A.ns_out ? __ldg(A.shm + q * A.ns_out + km) : make_float2(0.f, 0.f);
+      }
     int w = first;
     for (int it = 0; w < A.nitems; it++) {
       const int b = it & 1, ph = (it >> 1) & 1;
@@ -619,22 +626,27 @@ __global__ void __launch_bounds__(R::threads, 1) k_tc_m2m(M2mArgs A) {
       tc_fence_after();
       const int rhs = w / A.items_per_rhs, p0 = (w % A.items_per_rhs) * A.ppi;
       const float inv = A.inv_a / scale_of(w);
-      float2 *obase = A.mul + (size_t)rhs * A.mp + A.off_out + km;
       float omx = 0.f;
-      for (int cg = 0; cg < N / (32 * R::epi_groups); cg++) {  // 32 columns = 4 parents
-        const int col0 = ch0 * (N / R::epi_groups) + 32 * cg;
-        float d[32];
-        tmem_ld32(tmem + ((uint32_t)(32 * qd) << 16) + (uint32_t)(b * N + col0), d);
-        if (!ok || km >= A.ns_out) continue;
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
-          const int P = p0 + col0 / 8 + u;
-          float2 acc = make_float2(0.f, 0.f);
+      for (int t = 0; t < 2; t++) {
+        if (t >= A.mt) break;
+        const int km = 128 * t + 32 * qd + lane;
+        float2 *obase = A.mul + (size_t)rhs * A.mp + A.off_out + km;
+        for (int cg = 0; cg < N / (32 * R::epi_groups); cg++) {  // 32 columns = 4 parents
+          const int col0 = ch0 * (N / R::epi_groups) + 32 * cg;
+          float d[32];
+          tmem_ld32(tmem + ((uint32_t)(32 * qd) << 16) + (uint32_t)((b * A.mt + t) * N + col0), d);
+          if (!ok || km >= A.ns_out) continue;
 #pragma unroll
-          for (int q = 0; q < 4; q++)
-            cfma(acc, shq[q], make_float2(d[8 * u + 2 * q] * inv, d[8 * u + 2 * q + 1] * inv));
-          obase[(size_t)P * A.ns_out] = acc;
-          omx = fmaxf(omx, fmaxf(fabsf(acc.x), fabsf(acc.y)));
+          for (int u = 0; u < 4; u++) {
+            const int P = p0 + col0 / 8 + u;
+            float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+              cfma(acc, shq[t][q], make_float2(d[8 * u + 2 * q] * inv, d[8 * u + 2 * q + 1] * inv));
+            obase[(size_t)P * A.ns_out] = acc;
+            omx = fmaxf(omx, fmaxf(fabsf(acc.x), fabsf(acc.y)));
+          }
         }
       }
       tc_fence_before();
@@ -648,12 +660,12 @@ __global__ void __launch_bounds__(R::threads, 1) k_tc_m2m(M2mArgs A) {
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 0) tmem_dealloc(tmem, 2 * N);
+  if (warp == 0) tmem_dealloc(tmem, 2 * A.mt * N);
 }
 
 struct M2mPlan {
   uint8_t *A = nullptr;  // device
-  int Kp = 0, ppi = 0;
+  int Kp = 0, ppi = 0, mt = 1;
   unsigned kc_magic = 0;
   float inv_a = 1;
   bool ok = false;
@@ -705,23 +717,25 @@ struct BandPlan {
 
 // Packs a dense [128 x Kp] real matrix as FP16 hi then lo (K-major core
 // matrices) after a power-of-two scale; returns the inverse of the scale.
-static double pack_resident(const std::vector<double> &dense, int Kp, std::vector<uint8_t> &buf) {
+static double pack_resident(const std::vector<double> &dense, int Kp, std::vector<uint8_t> &buf, int tiles = 1) {
   double mw = 0;
   for (double v : dense) mw = std::max(mw, std::abs(v));
   int e2;
   std::frexp(mw > 0 ? mw : 1.0, &e2);
   const double sa = std::ldexp(1.0, 14 - e2);
-  buf.assign((size_t)512 * Kp, 0);
-  __half *hi = (__half *)buf.data(), *lo = (__half *)(buf.data() + (size_t)256 * Kp);
-  for (int m = 0; m < 128; m++)
-    for (int k = 0; k < Kp; k++) {
-      const double v = dense[(size_t)m * Kp + k] * sa;
-      const __half h = __double2half(v);
-      const __half l = __double2half(v - (double)__half2float(h));
-      const size_t idx = ((size_t)(m / 8) * (Kp / 8) + k / 8) * 64 + (m % 8) * 8 + (k % 8);
-      hi[idx] = h;
-      lo[idx] = l;
-    }
+  buf.assign((size_t)512 * Kp * tiles, 0);
+  for (int t = 0; t < tiles; t++) {  // tile t: rows 128 t .. 128 t + 127, hi then lo
+    __half *hi = (__half *)(buf.data() + (size_t)512 * Kp * t), *lo = hi + (size_t)128 * Kp;
+    for (int m = 0; m < 128; m++)
+      for (int k = 0; k < Kp; k++) {
+        const double v = dense[(size_t)(128 * t + m) * Kp + k] * sa;
+        const __half h = __double2half(v);
+        const __half l = __double2half(v - (double)__half2float(h));
+        const size_t idx = ((size_t)(m / 8) * (Kp / 8) + k / 8) * 64 + (m % 8) * 8 + (k % 8);
+        hi[idx] = h;
+        lo[idx] = l;
+      }
+  }
   return 1.0 / sa;
 }
 
@@ -740,27 +754,28 @@ static isg_status build_m2m(isg_ctx *c, int i, size_t smem_cap) {
   const HostTables &H = c->T;
   const int ns_out = H.nsamp[i], ns_in = H.nsamp[i + 1], ni = H.ninter;
   M2mPlan &T = c->band->pm2m[i];
-  if (ns_out > 128) return ISG_OK;
-  const int Kp = (ns_in + 15) / 16 * 16;
+  if (ns_out > 256) return ISG_OK;
+  const int Kp = (ns_in + 15) / 16 * 16, mt = (ns_out + 127) / 128;
   int ppi = 0;
-  for (int cand : {32, 16})
-    if (M2mSmem(Kp, cand, ns_in).total <= smem_cap && (1 << i) >= cand) {
+  for (int cand : {32, 16, 8})
+    if (M2mSmem(Kp, cand, ns_in, mt).total <= smem_cap && (1 << i) >= cand) {
       ppi = cand;
       break;
     }
   const int nparents = 1 << (2 * i);
   if (!ppi || nparents % ppi || !kc_magic(Kp / 8, (unsigned)(ppi * Kp / 8), &T.kc_magic)) return ISG_OK;
-  std::vector<double> dense((size_t)128 * Kp, 0.0);
+  std::vector<double> dense((size_t)128 * mt * Kp, 0.0);
   for (int k = 0; k < ns_out; k++)
     for (int t = 0; t < ni; t++) dense[(size_t)k * Kp + H.intind[i][(size_t)k * ni + t]] += H.interp[i][(size_t)k * ni + t];
   std::vector<uint8_t> buf;
-  T.inv_a = (float)pack_resident(dense, Kp, buf);
+  T.inv_a = (float)pack_resident(dense, Kp, buf, mt);
   isg_status e;
   if ((e = cuda_check(c, cudaMalloc(&T.A, buf.size()), "m2m alloc")) != ISG_OK) return e;
   if ((e = cuda_check(c, cudaMemcpy(T.A, buf.data(), buf.size(), cudaMemcpyHostToDevice), "m2m upload")) != ISG_OK)
     return e;
   T.Kp = Kp;
   T.ppi = ppi;
+  T.mt = mt;
   T.ok = true;
   return ISG_OK;
 }
@@ -975,6 +990,7 @@ bool band_m2m(isg_ctx *c, int lvl, float2 *mul, int nrhs, const int *active, cud
     A.ns_out = p.ns;
     A.Kp = T.Kp;
     A.ppi = T.ppi;
+    A.mt = T.mt;
     A.kc_magic = T.kc_magic;
     A.A = T.A;
     A.shm = p.shm;
@@ -988,7 +1004,7 @@ bool band_m2m(isg_ctx *c, int lvl, float2 *mul, int nrhs, const int *active, cud
     A.lvl_in = lvl + 1;
     A.lvl_out = lvl;
     count_launch();
-    k_tc_m2m<M2mRoles><<<std::min(A.nitems, c->band->sms), M2mRoles::threads, M2mSmem(T.Kp, T.ppi, ch.ns).total, st>>>(A);
+    k_tc_m2m<M2mRoles><<<std::min(A.nitems, c->band->sms), M2mRoles::threads, M2mSmem(T.Kp, T.ppi, ch.ns, T.mt).total, st>>>(A);
     *e = cuda_check(c, cudaGetLastError(), "m2m launch");
     return true;
   }
