@@ -18,7 +18,10 @@
 // async copies.  Warp 1 is the copy producer, thread 0 issues the MMAs, the
 // other warps load and convert operands and all warps run the epilogue.
 #include <cmath>
+#include <cstring>
 #include <vector>
+
+#include <cuda.h>
 
 #include "isg_context.hpp"
 #include "isg_tc.cuh"
@@ -111,16 +114,24 @@ struct TcNearArgs {
   int nleaf, U, tiles_x, tiles;
   int loc_vec;  // leaf locals can be copied in 16-byte chunks (ns % 4 == 0, aligned)
   int pair;     // tiles per CTA: kPair, or 1 when the launch is too small to fill the GPU
+  int tma_x;    // the halo comes by two tensor loads (map tmx)
+  int tma_loc;  // the leaf locals come by tensor loads (map tml)
   int *err;
 };
 
-__global__ void __launch_bounds__(256, 1) k_tc_near(TcNearArgs A) {
+// tmx views the input as [RHS][leaf row][4-pixel chunk][leaf column][8 floats]
+// and tml the leaf locals as [RHS][leaf row][4-sample chunk][leaf column][8
+// floats]: a box of either lands in the staging layout below (first 16 bytes
+// of every chunk in the hi slots, the second 16 in the lo slots).
+__global__ void __launch_bounds__(256, 1) k_tc_near(TcNearArgs A, const __grid_constant__ CUtensorMap tmx,
+                                                    const __grid_constant__ CUtensorMap tml) {
   extern __shared__ __align__(1024) char sm[];
   const int rhs = blockIdx.y;
   if (A.active && !A.active[rhs]) return;
   uint64_t *full = (uint64_t *)(sm + NearSmem::bars);
   uint64_t *empty = full + kNB;
   uint64_t *done = empty + kNB;
+  uint64_t *hbar = done + 1, *lbar = done + 2;  // halo, leaf locals landed
   uint32_t *tslot = (uint32_t *)(sm + NearSmem::misc);
   float *fscr = (float *)(sm + NearSmem::misc + 16);      // [8]
   float *scales = (float *)(sm + NearSmem::misc + 48);    // [2]
@@ -141,6 +152,8 @@ __global__ void __launch_bounds__(256, 1) k_tc_near(TcNearArgs A) {
       mbar_init(&empty[b], 1);
     }
     mbar_init(done, 1);
+    mbar_init(hbar, 1);
+    mbar_init(lbar, 1);
     fence_mbar_init();
   }
   if (warp == 0) tmem_alloc(tslot, 512);
@@ -156,16 +169,26 @@ __global__ void __launch_bounds__(256, 1) k_tc_near(TcNearArgs A) {
   // (halo row, 4-pixel chunk, halo column): consecutive items are consecutive
   // 16-byte slots, free of bank conflicts
   const int kItems = (A.pair * kTY + 2) * kHC * 16;
-  for (int it = threadIdx.x; it < kItems; it += blockDim.x) {
-    const int hc = it % kHC, c = (it / kHC) & 15, hr = it / (kHC * 16);
-    const int ly = ty0 - 1 + hr, lx = tx0 - 1 + hc;
-    const bool in = ly >= 0 && ly < A.nleaf && lx >= 0 && lx < A.nleaf;
-    const size_t i = in ? (size_t)(ly * A.nleaf + lx) * kBB + 4 * c : 0;
-    const int off = hr * kSboA + c * kLboA + hc * 16;
-    cp_async16z(sm + NearSmem::hi + off, A.x + rbase + i, in);
-    cp_async16z(sm + NearSmem::lo + off, A.x + rbase + i + 2, in);
+  if (A.tma_x) {
+    // two tensor loads: pixels 0, 1 of every chunk to the hi slots, 2, 3 to the lo slots
+    if (threadIdx.x == 0) {
+      mbar_expect_tx(hbar, 2 * kItems * 16);
+      tma_load_5d(sm + NearSmem::hi, &tmx, 0, tx0 - 1, 0, ty0 - 1, rhs, hbar);
+      tma_load_5d(sm + NearSmem::lo, &tmx, 4, tx0 - 1, 0, ty0 - 1, rhs, hbar);
+    }
+    mbar_wait(hbar, 0, A.err, kErrNearFull);
+  } else {
+    for (int it = threadIdx.x; it < kItems; it += blockDim.x) {
+      const int hc = it % kHC, c = (it / kHC) & 15, hr = it / (kHC * 16);
+      const int ly = ty0 - 1 + hr, lx = tx0 - 1 + hc;
+      const bool in = ly >= 0 && ly < A.nleaf && lx >= 0 && lx < A.nleaf;
+      const size_t i = in ? (size_t)(ly * A.nleaf + lx) * kBB + 4 * c : 0;
+      const int off = hr * kSboA + c * kLboA + hc * 16;
+      cp_async16z(sm + NearSmem::hi + off, A.x + rbase + i, in);
+      cp_async16z(sm + NearSmem::lo + off, A.x + rbase + i + 2, in);
+    }
+    cp_async_wait_all();
   }
-  cp_async_wait_all();
   __syncthreads();
 
   if (warp == 1) {
@@ -254,8 +277,19 @@ __global__ void __launch_bounds__(256, 1) k_tc_near(TcNearArgs A) {
     const float2 *lr = A.loc_leaf + (size_t)rhs * A.mp;
     const bool near_ok = mbar_wait(done, 0, A.err, kErrNearDone);
     float s2 = 1.f;
+    if (near_ok && A.tma_loc) {
+      // one tensor load per tile and slot: samples 0, 1 of every chunk to hi, 2, 3 to lo
+      if (li == 0) {
+        mbar_expect_tx(lbar, ntile * 2 * kL2pTile);
+        for (int u = 0; u < ntile; u++) {
+          tma_load_5d(sm + NearSmem::hi + u * kL2pTile, &tml, 0, tx0, 0, ty0 + u * kTY, rhs, lbar);
+          tma_load_5d(sm + NearSmem::lo + u * kL2pTile, &tml, 4, tx0, 0, ty0 + u * kTY, rhs, lbar);
+        }
+      }
+      mbar_wait(lbar, 0, A.err, kErrNearFull);
+    }
     if (near_ok) {
-      for (int it = li; it < kL; it += kLoaders) {
+      for (int it = li; it < kL && !A.tma_loc; it += kLoaders) {
         // (tile, row group, chunk, row in group): consecutive 16-byte slots
         const int m7 = it & 7, c = (it >> 3) % kLocChunksMax, mg = (it >> 3) / kLocChunksMax;
         const int u = mg >> 4, m = ((mg & 15) << 3) | m7;
@@ -1011,7 +1045,33 @@ isg_status tc_near(isg_ctx *c, const NearArgs &N, cudaStream_t st) {
   A.pair = (A.tiles * N.in.nrhs >= 2 * kPair * sms) ? kPair : 1;
   if (T.near_pair > 0 && 4 * N.in.nrhs >= P.tuned_nrhs) A.pair = std::min(T.near_pair, kPair);
   const int pairs = A.tiles_x * ((tiles_y + A.pair - 1) / A.pair);
-  k_tc_near<<<dim3(pairs, N.in.nrhs), 256, NearSmem::total, st>>>(A);
+  // tensor maps (see k_tc_near); a map that does not encode keeps its 16-byte copies
+  CUtensorMap tmx, tml;
+  memset(&tmx, 0, sizeof(tmx));
+  memset(&tml, 0, sizeof(tml));
+  const cuuint32_t one[5] = {1, 1, 1, 1, 1};
+  {
+    const cuuint64_t dims[5] = {8, (cuuint64_t)P.nleaf, 16, (cuuint64_t)P.nleaf, (cuuint64_t)N.in.nrhs};
+    const cuuint64_t strides[4] = {(cuuint64_t)kBB * 8, 32, (cuuint64_t)P.nleaf * kBB * 8, (cuuint64_t)P.U * 8};
+    const cuuint32_t box[5] = {4, (cuuint32_t)kHC, 16, (cuuint32_t)(A.pair * kTY + 2), 1};
+    A.tma_x = cuTensorMapEncodeTiled(&tmx, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, (void *)A.x, dims, strides, box, one,
+                                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                     CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  }
+  A.tma_loc = 0;
+  if (A.loc_vec) {
+    const cuuint64_t dims[5] = {8, (cuuint64_t)P.nleaf, (cuuint64_t)(P.ns_leaf / 4), (cuuint64_t)P.nleaf,
+                                (cuuint64_t)N.in.nrhs};
+    const cuuint64_t strides[4] = {(cuuint64_t)P.ns_leaf * 8, 32, (cuuint64_t)P.nleaf * P.ns_leaf * 8,
+                                   (cuuint64_t)P.mp * 8};
+    const cuuint32_t box[5] = {4, (cuuint32_t)kTX, (cuuint32_t)kLocChunksMax, (cuuint32_t)kTY, 1};
+    A.tma_loc = P.ns_leaf / 4 <= kLocChunksMax &&
+                cuTensorMapEncodeTiled(&tml, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, (void *)A.loc_leaf, dims, strides,
+                                       box, one, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                       CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  }
+  k_tc_near<<<dim3(pairs, N.in.nrhs), 256, NearSmem::total, st>>>(A, tmx, tml);
   return cuda_check(c, cudaGetLastError(), "tc near launch");
 }
 
