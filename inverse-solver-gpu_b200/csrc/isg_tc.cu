@@ -54,6 +54,7 @@ struct NearSmem {
   static constexpr int total = misc + 256;
 };
 static_assert(kPair * kL2pTile <= kRegion, "the L2P operands reuse the halo region");
+static_assert(kPair * 128 * 66 * 8 <= 2 * kRegion, "the epilogue tiles reuse the halo region");
 
 __device__ __forceinline__ int loader_id() {
   const int w = threadIdx.x >> 5;
@@ -365,73 +366,74 @@ __global__ void __launch_bounds__(256, 1) k_tc_near(TcNearArgs A, const __grid_c
     }
   }
 
-  // ---- epilogue (all warps), one tile of the pair at a time ----
+  // ---- epilogue (all warps), in two passes per tile: (1) each thread takes its
+  // leaf's 32 pixels out of TMEM (near field and L2P, scaled back) into a padded
+  // shared tile [leaf][66 float2] in the halo region, free once the L2P MMAs are
+  // done; (2) each warp then takes one leaf at a time, so x, the dot vector and
+  // y move as 512 contiguous bytes per warp access ----
+  constexpr int kOutLd = 66;  // float2 per leaf row: 16-byte aligned rows, 2-way bank spread
   const int q = warp & 3, hh = warp >> 2;
   const int m = 32 * q + lane;
   const bool need_x = A.epi == EPI_FWD || A.epi == EPI_ADJ || A.red == RED_TS;
-  bool ok = true;
+  const bool ok = mbar_wait(done, 1, A.err, kErrNearDone);
+  __syncthreads();
+  tc_fence_after();
+  const float inv1 = A.inv_w / scales[0], inv2 = A.inv_b / scales[1];
   for (int u = 0; u < ntile; u++) {
-    const int ly = ty0 + u * kTY + m / kTX, lx = tx0 + m % kTX;
-    const bool in_grid = ly < A.nleaf && lx < A.nleaf;
-    const size_t leafbase = rbase + (size_t)(ly * A.nleaf + lx) * kBB;
-    // this thread's 32 input pixels (for the first tile, fetched while the last MMAs run)
-    float4 xpre[4][4];
-#pragma unroll
-    for (int ch = 0; ch < 4; ch++)
-#pragma unroll
-      for (int pp = 0; pp < 4; pp++)
-        xpre[ch][pp] = (need_x && in_grid) ? *(const float4 *)(A.xe + leafbase + 32 * hh + 8 * ch + 2 * pp)
-                                           : make_float4(0.f, 0.f, 0.f, 0.f);
-    if (u == 0) {
-      ok = mbar_wait(done, 1, A.err, kErrNearDone);
-      __syncthreads();
-      tc_fence_after();
-    }
-    const float inv1 = A.inv_w / scales[0], inv2 = A.inv_b / scales[1];
-    const bool valid = ok && in_grid;
-    double r0 = 0, r1 = 0, r2 = 0;
+    float2 *ot = (float2 *)(sm + NearSmem::hi) + (size_t)u * 128 * kOutLd;
 #pragma unroll
     for (int ch = 0; ch < 4; ch++) {
       const int col = 64 * hh + 16 * ch;
       float d1[16], d2[16];
       tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + 128 * u + col, d1);
       tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + 256 + 128 * u + col, d2);
-      if (!valid) continue;
 #pragma unroll
-      for (int p = 0; p < 8; p += 2) {
-        const int t0 = col / 2 + p;  // complex pixel
-        float2 o[2];
+      for (int p = 0; p < 8; p++)
+        ot[m * kOutLd + col / 2 + p] =
+            make_float2(d1[2 * p] * inv1 + d2[2 * p] * inv2, d1[2 * p + 1] * inv1 + d2[2 * p + 1] * inv2);
+    }
+  }
+  __syncthreads();
+  for (int u = 0; u < ntile; u++) {
+    const float2 *ot = (const float2 *)(sm + NearSmem::hi) + (size_t)u * 128 * kOutLd;
+    double r0 = 0, r1 = 0, r2 = 0;
+#pragma unroll 4
+    for (int r = 0; r < 16; r++) {
+      const int e = threadIdx.x + 256 * r, lm = e >> 5, pp = e & 31;  // leaf, pixel pair
+      const int ly = ty0 + u * kTY + lm / kTX, lx = tx0 + lm % kTX;
+      if (!ok || ly >= A.nleaf || lx >= A.nleaf) continue;
+      const size_t i = rbase + (size_t)(ly * A.nleaf + lx) * kBB + 2 * pp;
+      const float4 ov = *(const float4 *)(ot + lm * kOutLd + 2 * pp);
+      float2 o[2] = {make_float2(ov.x, ov.y), make_float2(ov.z, ov.w)};
+      float2 xin[2] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+      if (need_x) {
+        const float4 xv = *(const float4 *)(A.xe + i);
+        xin[0] = make_float2(xv.x, xv.y);
+        xin[1] = make_float2(xv.z, xv.w);
+      }
+      if (A.epi == EPI_FWD) {
+        o[0] = csub(xin[0], o[0]);
+        o[1] = csub(xin[1], o[1]);
+      } else if (A.epi == EPI_ADJ) {
+        const float4 gv = *(const float4 *)(gr + (i - rbase));
+        o[0] = csub(xin[0], cconj(cmul(make_float2(gv.x, gv.y), o[0])));
+        o[1] = csub(xin[1], cconj(cmul(make_float2(gv.z, gv.w), o[1])));
+      } else if (A.epi == EPI_CONJ) {
+        o[0] = cconj(o[0]);
+        o[1] = cconj(o[1]);
+      }
+      *(float4 *)(A.y + i) = make_float4(o[0].x, o[0].y, o[1].x, o[1].y);
+      if (A.red == RED_DOT) {
+        const float4 av = *(const float4 *)(A.dot_a + i);
+        const float2 a0 = make_float2(av.x, av.y), a1 = make_float2(av.z, av.w);
+        r0 += (double)a0.x * o[0].x + (double)a0.y * o[0].y + (double)a1.x * o[1].x + (double)a1.y * o[1].y;
+        r1 += (double)a0.x * o[0].y - (double)a0.y * o[0].x + (double)a1.x * o[1].y - (double)a1.y * o[1].x;
+      } else if (A.red == RED_TS) {
 #pragma unroll
-        for (int e = 0; e < 2; e++)
-          o[e] = make_float2(d1[2 * (p + e)] * inv1 + d2[2 * (p + e)] * inv2,
-                             d1[2 * (p + e) + 1] * inv1 + d2[2 * (p + e) + 1] * inv2);
-        const size_t i = leafbase + t0;
-        const float4 xv = xpre[ch][p / 2];
-        const float2 xin[2] = {make_float2(xv.x, xv.y), make_float2(xv.z, xv.w)};
-        if (A.epi == EPI_FWD) {
-          o[0] = csub(xin[0], o[0]);
-          o[1] = csub(xin[1], o[1]);
-        } else if (A.epi == EPI_ADJ) {
-          const float4 gv = *(const float4 *)(gr + (i - rbase));
-          o[0] = csub(xin[0], cconj(cmul(make_float2(gv.x, gv.y), o[0])));
-          o[1] = csub(xin[1], cconj(cmul(make_float2(gv.z, gv.w), o[1])));
-        } else if (A.epi == EPI_CONJ) {
-          o[0] = cconj(o[0]);
-          o[1] = cconj(o[1]);
-        }
-        *(float4 *)(A.y + i) = make_float4(o[0].x, o[0].y, o[1].x, o[1].y);
-        if (A.red == RED_DOT) {
-          const float4 av = *(const float4 *)(A.dot_a + i);
-          const float2 a0 = make_float2(av.x, av.y), a1 = make_float2(av.z, av.w);
-          r0 += (double)a0.x * o[0].x + (double)a0.y * o[0].y + (double)a1.x * o[1].x + (double)a1.y * o[1].y;
-          r1 += (double)a0.x * o[0].y - (double)a0.y * o[0].x + (double)a1.x * o[1].y - (double)a1.y * o[1].x;
-        } else if (A.red == RED_TS) {
-#pragma unroll
-          for (int e = 0; e < 2; e++) {
-            r0 += (double)o[e].x * xin[e].x + (double)o[e].y * xin[e].y;
-            r1 += (double)o[e].x * xin[e].y - (double)o[e].y * xin[e].x;
-            r2 += (double)o[e].x * o[e].x + (double)o[e].y * o[e].y;
-          }
+        for (int e2 = 0; e2 < 2; e2++) {
+          r0 += (double)o[e2].x * xin[e2].x + (double)o[e2].y * xin[e2].y;
+          r1 += (double)o[e2].x * xin[e2].y - (double)o[e2].y * xin[e2].x;
+          r2 += (double)o[e2].x * o[e2].x + (double)o[e2].y * o[e2].y;
         }
       }
     }
