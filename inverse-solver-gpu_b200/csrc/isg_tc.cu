@@ -170,6 +170,17 @@ __global__ void __launch_bounds__(256, 1) k_tc_near(TcNearArgs A, const __grid_c
   // (halo row, 4-pixel chunk, halo column): consecutive items are consecutive
   // 16-byte slots, free of bank conflicts
   const int kItems = (A.pair * kTY + 2) * kHC * 16;
+  if (threadIdx.x == 32) {
+    // the epilogue's x and dot vector rows of the pair, into L2 while the MMAs run
+    const uint32_t run = (uint32_t)min(kTX, A.nleaf - tx0) * kBB * 8;
+    for (int r = 0; r < ntile * kTY; r++) {
+      const int ly = ty0 + r;
+      if (ly >= A.nleaf) break;
+      const size_t at = rbase + (size_t)(ly * A.nleaf + tx0) * kBB;
+      if (A.epi == EPI_FWD || A.epi == EPI_ADJ || A.red == RED_TS) bulk_prefetch_l2(A.xe + at, run);
+      if (A.red == RED_DOT) bulk_prefetch_l2(A.dot_a + at, run);
+    }
+  }
   if (A.tma_x) {
     // two tensor loads: pixels 0, 1 of every chunk to the hi slots, 2, 3 to the lo slots
     if (threadIdx.x == 0) {
@@ -397,20 +408,27 @@ __global__ void __launch_bounds__(256, 1) k_tc_near(TcNearArgs A, const __grid_c
   for (int u = 0; u < ntile; u++) {
     const float2 *ot = (const float2 *)(sm + NearSmem::hi) + (size_t)u * 128 * kOutLd;
     double r0 = 0, r1 = 0, r2 = 0;
-#pragma unroll 4
+    // every load of the tile first (one round trip), then the arithmetic and stores
+    float4 xv[16], av[16];
+    size_t idx[16];
+    bool live[16];
+#pragma unroll
     for (int r = 0; r < 16; r++) {
       const int e = threadIdx.x + 256 * r, lm = e >> 5, pp = e & 31;  // leaf, pixel pair
       const int ly = ty0 + u * kTY + lm / kTX, lx = tx0 + lm % kTX;
-      if (!ok || ly >= A.nleaf || lx >= A.nleaf) continue;
-      const size_t i = rbase + (size_t)(ly * A.nleaf + lx) * kBB + 2 * pp;
+      live[r] = ok && ly < A.nleaf && lx < A.nleaf;
+      idx[r] = live[r] ? rbase + (size_t)(ly * A.nleaf + lx) * kBB + 2 * pp : rbase;
+      xv[r] = (need_x && live[r]) ? *(const float4 *)(A.xe + idx[r]) : make_float4(0.f, 0.f, 0.f, 0.f);
+      av[r] = (A.red == RED_DOT && live[r]) ? *(const float4 *)(A.dot_a + idx[r]) : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+#pragma unroll
+    for (int r = 0; r < 16; r++) {
+      if (!live[r]) continue;
+      const int e = threadIdx.x + 256 * r, lm = e >> 5, pp = e & 31;
+      const size_t i = idx[r];
       const float4 ov = *(const float4 *)(ot + lm * kOutLd + 2 * pp);
       float2 o[2] = {make_float2(ov.x, ov.y), make_float2(ov.z, ov.w)};
-      float2 xin[2] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
-      if (need_x) {
-        const float4 xv = *(const float4 *)(A.xe + i);
-        xin[0] = make_float2(xv.x, xv.y);
-        xin[1] = make_float2(xv.z, xv.w);
-      }
+      const float2 xin[2] = {make_float2(xv[r].x, xv[r].y), make_float2(xv[r].z, xv[r].w)};
       if (A.epi == EPI_FWD) {
         o[0] = csub(xin[0], o[0]);
         o[1] = csub(xin[1], o[1]);
@@ -424,8 +442,7 @@ __global__ void __launch_bounds__(256, 1) k_tc_near(TcNearArgs A, const __grid_c
       }
       *(float4 *)(A.y + i) = make_float4(o[0].x, o[0].y, o[1].x, o[1].y);
       if (A.red == RED_DOT) {
-        const float4 av = *(const float4 *)(A.dot_a + i);
-        const float2 a0 = make_float2(av.x, av.y), a1 = make_float2(av.z, av.w);
+        const float2 a0 = make_float2(av[r].x, av[r].y), a1 = make_float2(av[r].z, av[r].w);
         r0 += (double)a0.x * o[0].x + (double)a0.y * o[0].y + (double)a1.x * o[1].x + (double)a1.y * o[1].y;
         r1 += (double)a0.x * o[0].y - (double)a0.y * o[0].x + (double)a1.x * o[1].y - (double)a1.y * o[1].x;
       } else if (A.red == RED_TS) {
