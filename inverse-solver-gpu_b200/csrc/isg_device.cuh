@@ -163,6 +163,7 @@ struct NearArgs {
   const float2 *dot_a = nullptr;  // RED_DOT: partial of sum conj(a) * y
   double *part = nullptr;         // [R][nblocks][4]
   const float2 *x_epi = nullptr;  // x of the `x - ...` epilogue when in.x already holds g x (else in.x)
+  const unsigned *locmax = nullptr;  // tensor engine: per-RHS level maxima of the locals, written by M2L
 };
 int near_blocks_per_rhs(const DevPlan &P);
 void launch_near(const DevPlan &P, const NearArgs &A, cudaStream_t st);

@@ -115,6 +115,8 @@ struct TcNearArgs {
   int nleaf, U, tiles_x, tiles;
   int loc_vec;  // leaf locals can be copied in 16-byte chunks (ns % 4 == 0, aligned)
   int pair;     // tiles per CTA: kPair, or 1 when the launch is too small to fill the GPU
+  const unsigned *locmax;  // when set: [R][kMaxLevels] maxima of the locals (written by M2L), the L2P scale
+  int lvl_leaf;
   int tma_x;    // the halo comes by two tensor loads (map tmx)
   int tma_loc;  // the leaf locals come by tensor loads (map tml)
   int *err;
@@ -322,17 +324,22 @@ __global__ void __launch_bounds__(256, 1) k_tc_near(TcNearArgs A, const __grid_c
       }
       cp_async_wait_all();
       loaders_bar();
-      float mx2 = 0.f;
-      for (int it = li; it < kL; it += kLoaders) {
-        // (tile, row group, chunk, row in group): consecutive 16-byte slots
-        const int m7 = it & 7, c = (it >> 3) % kLocChunksMax, mg = (it >> 3) / kLocChunksMax;
-        const int u = mg >> 4, m = ((mg & 15) << 3) | m7;
-        const int off = u * kL2pTile + (m >> 3) * kSboL + c * 128 + (m & 7) * 16;
-        const float4 q0 = *(const float4 *)(sm + NearSmem::hi + off), q1 = *(const float4 *)(sm + NearSmem::lo + off);
-        mx2 = fmaxf(mx2, fmaxf(fmaxf(fabsf(q0.x), fabsf(q0.y)), fmaxf(fabsf(q0.z), fabsf(q0.w))));
-        mx2 = fmaxf(mx2, fmaxf(fmaxf(fabsf(q1.x), fabsf(q1.y)), fmaxf(fabsf(q1.z), fabsf(q1.w))));
+      if (A.locmax) {  // the leaf level's maximum per RHS, from M2L
+        s2 = pow2_scale(__uint_as_float(A.locmax[rhs * kMaxLevels + A.lvl_leaf]));
+      } else {
+        float mx2 = 0.f;
+        for (int it = li; it < kL; it += kLoaders) {
+          // (tile, row group, chunk, row in group): consecutive 16-byte slots
+          const int m7 = it & 7, c = (it >> 3) % kLocChunksMax, mg = (it >> 3) / kLocChunksMax;
+          const int u = mg >> 4, m = ((mg & 15) << 3) | m7;
+          const int off = u * kL2pTile + (m >> 3) * kSboL + c * 128 + (m & 7) * 16;
+          const float4 q0 = *(const float4 *)(sm + NearSmem::hi + off),
+                       q1 = *(const float4 *)(sm + NearSmem::lo + off);
+          mx2 = fmaxf(mx2, fmaxf(fmaxf(fabsf(q0.x), fabsf(q0.y)), fmaxf(fabsf(q0.z), fabsf(q0.w))));
+          mx2 = fmaxf(mx2, fmaxf(fmaxf(fabsf(q1.x), fabsf(q1.y)), fmaxf(fabsf(q1.z), fabsf(q1.w))));
+        }
+        s2 = pow2_scale(loaders_max(mx2, fscr));
       }
-      s2 = pow2_scale(loaders_max(mx2, fscr));
       for (int it = li; it < kL; it += kLoaders) {
         // (tile, row group, chunk, row in group): consecutive 16-byte slots
         const int m7 = it & 7, c = (it >> 3) % kLocChunksMax, mg = (it >> 3) / kLocChunksMax;
@@ -345,7 +352,7 @@ __global__ void __launch_bounds__(256, 1) k_tc_near(TcNearArgs A, const __grid_c
       }
     } else {
       loaders_bar();  // keeps the named-barrier count of the loaders the same on this path
-      (void)loaders_max(0.f, fscr);
+      if (!A.locmax) (void)loaders_max(0.f, fscr);
     }
     if (li == 0) scales[1] = s2;
     fence_proxy_async();
@@ -1058,6 +1065,8 @@ isg_status tc_near(isg_ctx *c, const NearArgs &N, cudaStream_t st) {
   A.tiles = A.tiles_x * tiles_y;
   A.loc_vec = (P.ns_leaf % 4 == 0) && aligned16(A.loc_leaf) && (P.mp % 2 == 0);
   A.err = T.err;
+  A.locmax = N.locmax;
+  A.lvl_leaf = P.L - 1;
   count_launch();
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->opts.device);
