@@ -22,6 +22,7 @@
 #include <vector>
 
 #include <cuda.h>
+#include <cudaTypedefs.h>
 
 #include "isg_context.hpp"
 #include "isg_tc.cuh"
@@ -1032,6 +1033,24 @@ int tc_error(isg_ctx *c) {
 
 static bool aligned16(const void *p) { return ((uintptr_t)p & 15) == 0; }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry-point query, so
+// that the library does not link the driver library (it still loads where
+// there is no driver, for the checks that need none); null when unavailable.
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  }
+  return fn;
+}
+
 isg_status tc_near(isg_ctx *c, const NearArgs &N, cudaStream_t st) {
   const DevPlan &P = c->P;
   const TcPlan &T = *c->tc;
@@ -1078,24 +1097,26 @@ isg_status tc_near(isg_ctx *c, const NearArgs &N, cudaStream_t st) {
   memset(&tmx, 0, sizeof(tmx));
   memset(&tml, 0, sizeof(tml));
   const cuuint32_t one[5] = {1, 1, 1, 1, 1};
-  {
+  const PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+  A.tma_x = 0;
+  if (encode) {
     const cuuint64_t dims[5] = {8, (cuuint64_t)P.nleaf, 16, (cuuint64_t)P.nleaf, (cuuint64_t)N.in.nrhs};
     const cuuint64_t strides[4] = {(cuuint64_t)kBB * 8, 32, (cuuint64_t)P.nleaf * kBB * 8, (cuuint64_t)P.U * 8};
     const cuuint32_t box[5] = {4, (cuuint32_t)kHC, 16, (cuuint32_t)(A.pair * kTY + 2), 1};
-    A.tma_x = cuTensorMapEncodeTiled(&tmx, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, (void *)A.x, dims, strides, box, one,
+    A.tma_x = encode(&tmx, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, (void *)A.x, dims, strides, box, one,
                                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                                      CU_TENSOR_MAP_L2_PROMOTION_NONE,
                                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
   }
   A.tma_loc = 0;
-  if (A.loc_vec) {
+  if (A.loc_vec && encode) {
     const cuuint64_t dims[5] = {8, (cuuint64_t)P.nleaf, (cuuint64_t)(P.ns_leaf / 4), (cuuint64_t)P.nleaf,
                                 (cuuint64_t)N.in.nrhs};
     const cuuint64_t strides[4] = {(cuuint64_t)P.ns_leaf * 8, 32, (cuuint64_t)P.nleaf * P.ns_leaf * 8,
                                    (cuuint64_t)P.mp * 8};
     const cuuint32_t box[5] = {4, (cuuint32_t)kTX, (cuuint32_t)kLocChunksMax, (cuuint32_t)kTY, 1};
     A.tma_loc = P.ns_leaf / 4 <= kLocChunksMax &&
-                cuTensorMapEncodeTiled(&tml, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, (void *)A.loc_leaf, dims, strides,
+                encode(&tml, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, (void *)A.loc_leaf, dims, strides,
                                        box, one, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                                        CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
   }
