@@ -158,13 +158,19 @@ isg_status isg_aggregateh(isg_ctx *ctx, void *x, const void *rx, int nrhs, int o
  * callers that must not allocate at that point, e.g. a driver whose HBM is
  * fully committed to solve workspaces, or a loop that cannot afford an
  * allocator's device-wide synchronisation.  No counterpart in the reference.
- *  - isg_setup_gpu(ctx) must have run (ISG_BAD_ARG otherwise).
+ *  - isg_setup_gpu(ctx) must have run (ISG_BAD_ARG otherwise).  Set-up looks
+ *    the array's device address up (cudaGetSymbolAddress) and loads the
+ *    kernels this call launches; with CUDA's lazy module loading that is when
+ *    the array's ISG_STATIC_SCRATCH_BYTES of device memory are taken, so
+ *    every device with a set-up context holds them until the process exits,
+ *    and the calls themselves need no free device memory.
  *  - Works in a fixed array of ISG_STATIC_SCRATCH_BYTES inside libisg.so:
  *    nrhs * (multipole samples per RHS, plus numunk unless order is
  *    ISG_ORDER_BLOCKED) * 8 bytes must fit, else ISG_BAD_ARG with the limit in
- *    isg_last_error (level 8: 2 RHS in tree/raster order, 4 in blocked order).
- *  - The first call on each device looks the array's address up
- *    (cudaGetSymbolAddress); make that first call before any stream capture.
+ *    isg_last_error (level 8: 2 RHS in tree/raster order, 4 in blocked order);
+ *    nrhs is also capped at 65535 (one grid row per RHS).
+ *  - The address belongs to the context's CUDA context: after a device reset
+ *    the isg context (like all its workspaces) is invalid; create a new one.
  *  - One array per device per process: calls that overlap in time on the same
  *    device (other streams, threads or contexts) race on it. */
 isg_status isg_aggregate_noalloc(isg_ctx *ctx, const void *x, void *rx, int nrhs, int order, isg_stream stream);

@@ -69,7 +69,7 @@ def build(force: bool = False, jobs: int = 8, verbose_ptxas: bool = False) -> st
     with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
         objs = list(ex.map(lambda s: compile_one(s, force, extra), sources()))
     if force or stale(OUT, objs):
-        cmd = [nvcc(), *ARCH, "-shared", "-o", OUT, *objs, "-lcudart", "-lcuda"]
+        cmd = [nvcc(), *ARCH, "-shared", "-o", OUT, *objs, "-lcudart"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

@@ -245,7 +245,7 @@ const char *isg_last_error(const isg_ctx *c) { return c ? c->err.c_str() : "null
 isg_status isg_create(const isg_opts *opts, isg_ctx **out) {
   if (!opts || !out) return ISG_BAD_ARG;
   *out = nullptr;
-  if (opts->max_rhs < 1) return ISG_BAD_ARG;
+  if (opts->max_rhs < 1 || opts->max_rhs > kMaxGridY) return ISG_BAD_ARG;
   isg_ctx *c = new isg_ctx();
   c->opts = *opts;
   std::string err = build_tables(opts->level, opts->box, opts->res, opts->k0, opts->beta, opts->ninter, opts->numrx, c->T);
@@ -379,6 +379,7 @@ isg_status isg_setup_gpu(isg_ctx *c) {
   if ((e = cuda_check(c, kernels_setup(), "kernel attributes")) != ISG_OK) return e;
   if ((e = tc_setup(c)) != ISG_OK) return e;
   if ((e = band_setup(c)) != ISG_OK) return e;
+  if ((e = noalloc_prepare(c)) != ISG_OK) return e;
   c->gpu_ready = true;
   return cuda_check(c, cudaDeviceSynchronize(), "setup sync");
 }

@@ -55,6 +55,8 @@ struct isg_ctx {
   isg::TcPlan *tc = nullptr;
   isg::BandPlan *band = nullptr;
   isg::FnoModel *fno = nullptr;
+  // device address of isg_aggregate_noalloc's static array, resolved by isg_setup_gpu
+  float2 *static_scratch = nullptr;
   // BiCGSTAB iteration block captured as a CUDA graph, and what it was captured for
   void *graph_exec = nullptr;
   int64_t graph_launches = 0;
@@ -105,6 +107,9 @@ bool band_m2m(isg_ctx *c, int lvl, float2 *mul, int nrhs, const int *active, cud
 // L2L into child level lvl on the tensor cores (overwrites its locals); false
 // when the level is not covered (its rings have more than 128 samples).
 bool band_l2l(isg_ctx *c, int lvl, float2 *loc, int nrhs, const int *active, cudaStream_t st, isg_status *e);
+// Static scratch of isg_aggregate_noalloc (isg_noalloc.cu): resolves its
+// address and loads its kernels; called by isg_setup_gpu.
+isg_status noalloc_prepare(isg_ctx *c);
 // Learned warm start (isg_fno.cu).
 isg_status fno_create(isg_ctx *c, const isg_fno_opts *o);
 void fno_destroy(isg_ctx *c);

@@ -1,6 +1,6 @@
 // The inversion loop of the reference driver (mom.cpp:222-399, with the
 // measurement synthesis of setup_born.cpp:139-168 and the metrics of
-// write_error, setup_born.cpp:593-664), device-resident and batched over
+// write_error, setup_born.cpp:171-242), device-resident and batched over
 // transmitters.  The contrast, gradient and search direction are complex128;
 // the per-transmitter fields are complex64; every reduction is FP64.  The
 // small receiver-side arrays (numrx per transmitter) are reduced on the host.
@@ -82,7 +82,7 @@ __global__ void k_born(const float2 *__restrict__ tot, const double2 *__restrict
   }
 }
 
-// Y = Y + g X (mom.cpp:301), or Y = g X when overwrite (mom.cpp:331, setup_born.cpp:569)
+// Y = Y + g X (mom.cpp:301), or Y = g X when overwrite (mom.cpp:331, setup_born.cpp:146)
 __global__ void k_gx(float2 *__restrict__ Y, const float2 *__restrict__ g, const float2 *__restrict__ X, int U,
                      int overwrite) {
   const size_t r = blockIdx.y;

@@ -11,6 +11,8 @@ namespace isg {
 constexpr int kMaxLevels = 12;
 constexpr int kBox = 8;
 constexpr int kBB = 64;  // pixels per leaf
+// Kernels put one RHS per grid row (gridDim.y or .z), so no batch may exceed this.
+constexpr int kMaxGridY = 65535;
 
 // A banded resampling (interpolation or anterpolation) cut into tiles of `out`
 // consecutive output samples (a multiple of kTileOut, the outputs one thread
@@ -143,6 +145,9 @@ int64_t launch_count();
 void capture_launches(int64_t *sink);
 // Per-device kernel attributes (isg_kernels.cu), called by isg_setup_gpu.
 cudaError_t kernels_setup();
+// Loads the kernels of the receiver projection (permute, P2M, M2M, receiver
+// interpolation) into the current device's context now, not at their first launch.
+cudaError_t aggregate_kernels_load();
 
 // ---- launchers (isg_kernels.cu) ----
 void launch_p2m(const DevPlan &P, const BatchArgs &B, float2 *mul, cudaStream_t st);

@@ -732,4 +732,13 @@ cudaError_t kernels_setup() {
   if (e == cudaSuccess) e = allow_max_smem(k_near, optin);
   return e;
 }
+
+cudaError_t aggregate_kernels_load() {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, k_permute);
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_p2m);
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_m2m_tile);
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_rx_interp);
+  return e;
+}
 }  // namespace isg

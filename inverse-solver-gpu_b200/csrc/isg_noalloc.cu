@@ -8,8 +8,13 @@
 // Every element the kernels read was written earlier in the same call (P2M
 // writes every leaf sample, each M2M every parent sample), so nothing has to
 // be cleared between calls.
-#include <mutex>
-
+//
+// The array lives in this file's own device module.  CUDA loads modules
+// lazily (the default since CUDA 12.2), and loading this one is what
+// allocates the array's 64 MiB, so isg_setup_gpu calls noalloc_prepare: the
+// address lookup below loads the module there, together with the kernels the
+// entry point launches, and the entry point itself only reads the address the
+// context keeps.
 #include "isg_context.hpp"
 
 namespace isg {
@@ -18,30 +23,21 @@ namespace {
 constexpr size_t kScratchElems = (size_t)ISG_STATIC_SCRATCH_BYTES / sizeof(float2);
 static __device__ __align__(256) float2 g_scratch[kScratchElems];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_scratch_mu;
-float2 *g_scratch_ptr[kMaxDevices] = {};
+}  // namespace
 
-// Device address of g_scratch on the current device (ctx->opts.device), looked
-// up once per device.
-isg_status scratch_address(isg_ctx *c, float2 **out) {
-  const int dev = c->opts.device;
-  if (dev < 0 || dev >= kMaxDevices) {
-    c->err = "device ordinal out of range for the static scratch";
-    return ISG_BAD_ARG;
-  }
-  std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (!g_scratch_ptr[dev]) {
-    void *p = nullptr;
-    isg_status e = cuda_check(c, cudaGetSymbolAddress(&p, g_scratch), "cudaGetSymbolAddress(static scratch)");
-    if (e != ISG_OK) return e;
-    g_scratch_ptr[dev] = (float2 *)p;
-  }
-  *out = g_scratch_ptr[dev];
+// Called by isg_setup_gpu with the context's device current: the device
+// address of g_scratch (host code cannot use the symbol itself as a device
+// pointer), and the kernels of the entry point loaded now rather than on its
+// first call.
+isg_status noalloc_prepare(isg_ctx *c) {
+  void *p = nullptr;
+  isg_status e = cuda_check(c, cudaGetSymbolAddress(&p, g_scratch), "cudaGetSymbolAddress(static scratch)");
+  if (e != ISG_OK) return e;
+  if ((e = cuda_check(c, aggregate_kernels_load(), "loading the receiver-projection kernels")) != ISG_OK) return e;
+  c->static_scratch = (float2 *)p;
   return ISG_OK;
 }
 
-}  // namespace
 }  // namespace isg
 
 using namespace isg;
@@ -49,12 +45,17 @@ using namespace isg;
 extern "C" isg_status isg_aggregate_noalloc(isg_ctx *c, const void *x, void *rx, int nrhs, int order,
                                             isg_stream stream) {
   if (!c) return ISG_BAD_ARG;
-  if (!c->gpu_ready) {
+  if (!c->gpu_ready || !c->static_scratch) {
     c->err = "isg_aggregate_noalloc needs isg_setup_gpu first (it allocates nothing itself)";
     return ISG_BAD_ARG;
   }
   if (!x || !rx || order < ISG_ORDER_TREE || order > ISG_ORDER_BLOCKED || nrhs < 1) {
     c->err = "isg_aggregate_noalloc: null pointer, bad order or nrhs < 1";
+    return ISG_BAD_ARG;
+  }
+  if (nrhs > kMaxGridY) {
+    c->err = "isg_aggregate_noalloc: nrhs=" + std::to_string(nrhs) + " exceeds " + std::to_string(kMaxGridY) +
+             " RHS per call (one grid row per RHS)";
     return ISG_BAD_ARG;
   }
   const size_t per_rhs = c->P.mp + (order == ISG_ORDER_BLOCKED ? 0 : (size_t)c->P.U);
@@ -67,13 +68,11 @@ extern "C" isg_status isg_aggregate_noalloc(isg_ctx *c, const void *x, void *rx,
   }
   isg_status e = cuda_check(c, cudaSetDevice(c->opts.device), "cudaSetDevice");
   if (e != ISG_OK) return e;
-  float2 *scratch = nullptr;
-  if ((e = scratch_address(c, &scratch)) != ISG_OK) return e;
   cudaStream_t st = (cudaStream_t)stream;
-  float2 *mul = scratch;
+  float2 *mul = c->static_scratch;
   const float2 *xb = (const float2 *)x;
   if (order != ISG_ORDER_BLOCKED) {
-    float2 *wx = scratch + (size_t)nrhs * c->P.mp;
+    float2 *wx = c->static_scratch + (size_t)nrhs * c->P.mp;
     launch_permute(order_perm(c, order), (const float2 *)x, wx, c->P.U, nrhs, true, st);
     xb = wx;
   }

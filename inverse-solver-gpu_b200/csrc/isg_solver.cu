@@ -209,7 +209,7 @@ __global__ void __launch_bounds__(256) k_update_s(const RhsState *st, const int 
 }
 
 // omega = <t, s> / ||t||^2 (bicgs.cpp:153); zero when t vanishes, which only
-// happens when s itself is zero (bicgs_gpu.cu:376 guards the same case).
+// happens when s itself is zero (bicgs_gpu.cu:197 guards the same case).
 __global__ void __launch_bounds__(256) k_fin_omega(RhsState *st, const int *active, const double *part, int nb) {
   const int rhs = blockIdx.x;
   if (!active[rhs]) return;

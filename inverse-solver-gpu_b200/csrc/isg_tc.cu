@@ -1036,18 +1036,18 @@ static bool aligned16(const void *p) { return ((uintptr_t)p & 15) == 0; }
 // cuTensorMapEncodeTiled through the runtime's driver entry-point query, so
 // that the library does not link the driver library (it still loads where
 // there is no driver, for the checks that need none); null when unavailable.
+// The lookup runs once per process; C++11 makes the static's initialisation
+// thread-safe, so contexts on several host threads may race to it.
 static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  static bool tried = false;
-  if (!tried) {
-    tried = true;
+  static const PFN_cuTensorMapEncodeTiled_v12000 fn = []() -> PFN_cuTensorMapEncodeTiled_v12000 {
     void *p = nullptr;
     cudaDriverEntryPointQueryResult q;
     if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
             cudaSuccess &&
         q == cudaDriverEntryPointSuccess)
-      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
-  }
+      return (PFN_cuTensorMapEncodeTiled_v12000)p;
+    return nullptr;
+  }();
   return fn;
 }
 

@@ -711,7 +711,7 @@ void orc_aggregateh(orc_ctx *c, double complex *x, const double complex *rx) {
   l2p(c, x);
 }
 
-/* One write_error record (setup_born.cpp:593-664). */
+/* One write_error record (setup_born.cpp:171-242). */
 static void dbim_record(const orc_ctx *c, int ntx, const double complex *mesd, const double complex *od,
                         const double complex *o, const double complex *otrue, double regular, double mesnorm,
                         double objnorm, double *rec) {

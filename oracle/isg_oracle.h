@@ -14,6 +14,7 @@
 #define ISG_ORACLE_H
 
 #include <complex.h>
+#include <stdint.h>
 
 #ifdef __cplusplus
 extern "C" {
@@ -64,6 +65,16 @@ void orc_aggregateh(orc_ctx *c, double complex *x, const double complex *rx);
 int orc_dbim(orc_ctx *c, int ntx, const double complex *inc, const double complex *chi_true, int iterations,
              double regular, double tol, int maxit, double complex *chi, double *hist, double *alpha,
              double complex *beta);
+
+/* Seeded inputs (isg_inputs.c): the library's random-ellipse contrast
+ * chi = eps_r - 1 in raster order, and plane waves exp(i k0 d.r) of
+ * transmitters first..first+count-1 of ntx, written in tree order through
+ * unkmap (raster order when unkmap is NULL); bit-identical to
+ * isg_make_phantom (kind 0) and isg_make_plane_waves. */
+void orc_in_ellipses(int side, double res, int count, double axis_min, double axis_max, double eps_min,
+                     double eps_max, double tand_max, uint64_t seed, double complex *chi);
+void orc_in_plane_waves(int side, double res, double k0, int ntx, int first, int count, const int *unkmap,
+                        double complex *inc);
 
 #ifdef __cplusplus
 }

@@ -1,5 +1,6 @@
-"""ctypes access to the checkers: the restated oracle (oracle/liboracle.so) and
-the reference's own compiled CPU path (oracle/_ref/libisgref.so).
+"""ctypes access to the checkers: the restated oracle (oracle/liboracle.so), its
+seeded input generators, and the reference's own compiled CPU path
+(oracle/_ref/libisgref.so).
 
 Test infrastructure only.  Both libraries are built by oracle/Makefile; the
 reference one needs the reference tree at build time and is then used prebuilt.
@@ -21,8 +22,9 @@ _P, _I, _D = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
 
 
 def build_oracle() -> None:
-    if not os.path.exists(ORACLE_LIB) or os.path.getmtime(ORACLE_LIB) < os.path.getmtime(
-            os.path.join(ORACLE_DIR, "isg_oracle.c")):
+    srcs = [os.path.join(ORACLE_DIR, f) for f in ("isg_oracle.c", "isg_inputs.c", "isg_oracle.h")]
+    if not os.path.exists(ORACLE_LIB) or any(os.path.getmtime(ORACLE_LIB) < os.path.getmtime(p)
+                                             for p in srcs if os.path.exists(p)):
         subprocess.run(["make", "-C", ORACLE_DIR, "liboracle.so"], check=True, capture_output=True)
 
 
@@ -128,6 +130,32 @@ class Oracle:
 
     def pos(self):
         return self.table("pos", 0, self.U, "c")
+
+
+def _oracle_lib():
+    L = Oracle.lib()
+    L.orc_in_ellipses.argtypes = [_I, _D, _I, _D, _D, _D, _D, _D, ctypes.c_uint64, _P]
+    L.orc_in_plane_waves.argtypes = [_I, _D, _D, _I, _I, _I, _P, _P]
+    return L
+
+
+def seeded_ellipses(side: int, seed: int, count: int, axis=(1.0, 3.0), eps=(1.1, 1.5), tand_max: float = 0.0,
+                    res: float = 0.1) -> np.ndarray:
+    """Contrast chi = eps_r - 1 (complex128, raster order) from the oracle's
+    restatement of the library's ellipse generator (bit-identical)."""
+    chi = np.zeros(side * side, np.complex128)
+    _oracle_lib().orc_in_ellipses(side, res, count, axis[0], axis[1], eps[0], eps[1], tand_max, seed, _arr(chi))
+    return chi
+
+
+def seeded_plane_waves(side: int, ntx: int, first: int, count: int, unkmap: np.ndarray | None,
+                       k0: float = 2 * np.pi, res: float = 0.1) -> np.ndarray:
+    """Plane waves of transmitters first..first+count-1 of ntx (complex128),
+    in tree order through unkmap (raster order when None)."""
+    out = np.zeros((count, side * side), np.complex128)
+    um = None if unkmap is None else np.ascontiguousarray(unkmap, np.int32)
+    _oracle_lib().orc_in_plane_waves(side, res, k0, ntx, first, count, None if um is None else _arr(um), _arr(out))
+    return out
 
 
 class Reference:

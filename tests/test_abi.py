@@ -82,3 +82,25 @@ def test_refapi_library_exports_the_reference_names():
     undefined = {ln.split()[-1] for ln in out.splitlines() if " U " in ln}
     for g in ("res", "box", "level", "k0", "numunk", "numrx", "toli", "iti", "pos", "unkmap"):
         assert g in undefined, g
+
+
+def test_library_does_not_need_the_driver_library():
+    """libisg.so records only the CUDA runtime: the driver entry points it uses
+    (tensor-map encoding) are looked up at run time, so the library loads on a
+    machine without a driver and fails there with ISG_NO_DEVICE instead."""
+    import subprocess
+    out = subprocess.run(["readelf", "-d", isg.LIBPATH], capture_output=True, text=True, check=True).stdout
+    needed = re.findall(r"\(NEEDED\)\s+Shared library: \[([^\]]+)\]", out)
+    assert any(n.startswith("libcudart") for n in needed), needed
+    assert not [n for n in needed if n.startswith("libcuda.")], needed
+
+
+def test_create_rejects_batches_wider_than_a_grid_row_limit():
+    o = isg.Opts()
+    isg.lib().isg_default_opts(ctypes.byref(o))
+    h = ctypes.c_void_p()
+    o.level, o.max_rhs = 4, 65536
+    assert isg.lib().isg_create(ctypes.byref(o), ctypes.byref(h)) == 5
+    o.max_rhs = 65535
+    assert isg.lib().isg_create(ctypes.byref(o), ctypes.byref(h)) == 0
+    isg.lib().isg_destroy(h)

@@ -62,3 +62,54 @@ def test_noalloc_needs_setup_gpu():
     buf = ctypes.create_string_buffer(16)
     assert isg.lib().isg_aggregate_noalloc(s._h, ctypes.addressof(buf), ctypes.addressof(buf), 1, 0, None) == 5
     assert "isg_setup_gpu" in isg.lib().isg_last_error(s._h).decode()
+
+
+FULL_HBM_SCRIPT = r"""
+import sys
+import numpy as np
+import torch
+sys.path.insert(0, sys.argv[1])
+import isg
+
+s = isg.Solver(6, numrx=64, max_rhs=2, device=0)
+s.setup_gpu()
+x = torch.randn((2, s.numunk), dtype=torch.complex64, device="cuda")
+got = torch.zeros((2, s.numrx), dtype=torch.complex64, device="cuda")
+want = torch.zeros_like(got)
+torch.cuda.synchronize()
+# Leave less free device memory than the static array's size, so that a
+# first call which still had to load it would fail.
+margin = 24 << 20
+hold = []
+for _ in range(64):
+    free, _ = torch.cuda.mem_get_info()
+    if free <= margin + (8 << 20):
+        break
+    hold.append(torch.empty(free - margin, dtype=torch.uint8, device="cuda"))
+free, _ = torch.cuda.mem_get_info()
+assert free < (64 << 20), free
+st = torch.cuda.current_stream().cuda_stream or None
+rc = isg.lib().isg_aggregate_noalloc(s._h, x.data_ptr(), got.data_ptr(), 2, isg.ORDER_TREE, st)
+assert rc == 0, (rc, isg.lib().isg_last_error(s._h).decode())
+assert isg.lib().isg_aggregate(s._h, x.data_ptr(), want.data_ptr(), 2, isg.ORDER_TREE, st) == 0
+torch.cuda.synchronize()
+free_after, _ = torch.cuda.mem_get_info()
+del hold
+g, w = got.cpu().numpy(), want.cpu().numpy()
+err = float(np.linalg.norm(g - w) / np.linalg.norm(w))
+print("free before", free, "after", free_after, "rel", err)
+assert err < 1e-6, err
+"""
+
+
+def test_first_call_succeeds_with_device_memory_full():
+    """The array is resolved by isg_setup_gpu, so the process's first call
+    needs no device memory: after set-up the test fills the device to within
+    24 MiB of full and only then makes that first call (a fresh process, so
+    no earlier call loaded anything)."""
+    import os
+    import subprocess
+    import sys
+    pkg = os.path.dirname(os.path.dirname(isg.__file__))
+    r = subprocess.run([sys.executable, "-c", FULL_HBM_SCRIPT, pkg], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
