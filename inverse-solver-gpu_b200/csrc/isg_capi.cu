@@ -588,6 +588,7 @@ isg_status isg_time_stages(isg_ctx *c, int nrhs, int engine, int reps, double *m
     A.in = B;
     A.x_epi = c->wx;
     A.locmax = c->locmax;
+    A.inmax = c->levmax;
   }
   for (int r = -1; r < reps; r++) {
     cudaEventRecord(ev[0], st);

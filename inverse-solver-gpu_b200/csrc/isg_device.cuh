@@ -169,6 +169,8 @@ struct NearArgs {
   double *part = nullptr;         // [R][nblocks][4]
   const float2 *x_epi = nullptr;  // x of the `x - ...` epilogue when in.x already holds g x (else in.x)
   const unsigned *locmax = nullptr;  // tensor engine: per-RHS level maxima of the locals, written by M2L
+  const unsigned *inmax = nullptr;   // tensor engine: [R][kMaxLevels] whose last slot holds the input's
+                                     // maximum per RHS, written by the tensor-core P2M of the same matvec
 };
 int near_blocks_per_rhs(const DevPlan &P);
 void launch_near(const DevPlan &P, const NearArgs &A, cudaStream_t st);

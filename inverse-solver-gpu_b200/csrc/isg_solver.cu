@@ -379,6 +379,7 @@ isg_status run_matvec(isg_ctx *c, const float2 *x, const float2 *g, int64_t gs, 
   A.in = pre ? Bg : B;
   A.x_epi = pre ? x : nullptr;
   A.locmax = tc ? c->locmax : nullptr;  // M2L of the leaves wrote it above
+  A.inmax = tc ? c->levmax : nullptr;   // and P2M the input's maximum
   A.loc = c->loc;
   A.y = y;
   A.epi = (kind == OP_FWD) ? EPI_FWD : (kind == OP_ADJ ? EPI_ADJ : (kind == OP_GCONJ ? EPI_CONJ : EPI_G));

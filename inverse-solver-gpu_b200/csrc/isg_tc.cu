@@ -497,6 +497,409 @@ __global__ void __launch_bounds__(256, 1) k_tc_near(TcNearArgs A, const __grid_c
   if (warp == 0) tmem_dealloc(tmem, 512);
 }
 
+// ---- near field + L2P, persistent and pipelined ----
+// Items are pairs of vertically adjacent 16 x 8-leaf tiles of one RHS; a
+// persistent CTA walks them in steps of gridDim.x.  An item's K dimension (9
+// neighbour slots x 128 source reals of the halo, then 2 ns reals of the leaf
+// locals for L2P) is staged in shared memory one A-stage at a time: a halo
+// K-group (32 source reals of every leaf of the pair's 34 x 10-leaf halo,
+// 43.5 KB as FP16 hi/lo) feeds the nine weight stages of its K range; an L2P
+// stage (32 reals of the locals of the pair's 256 leaves) feeds one.  Stage
+// order: H0 H1 H2 H3 L0 .. L4; the weights are packed in the same order.  The
+// whole halo is never resident, so four A-stage buffers and a three-deep
+// weight ring fit in shared memory and the roles overlap:
+//   warp 0      tensor loads of the A-stages (5-D maps, no multicast)
+//   warp 1      bulk copies of the weight stages
+//   warp 2      MMA issue (one thread)
+//   warps 3..6  A-stage conversion to FP16 hi/lo, in place
+//   warps 7..14 epilogue, two per TMEM lane quarter (columns 0..63, 64..127)
+// Near field and L2P accumulate into one TMEM accumulator per tile: the input
+// is scaled by the power of two that P2M's per-RHS maximum gives and the
+// locals by M2L's, each lowered until both products carry the same power of
+// two.  Two accumulator sets (two tiles x 128 columns each) alternate between
+// items, so an item's epilogue runs under the next item's MMAs.
+constexpr int kNpKC = 4;                                       // 8-real K-chunks per A-stage
+constexpr int kNpHaloSplit = kHR * kNpKC * kHC * 16;           // 21760: one split of a halo K-group
+constexpr int kNpL2pSplit = kPair * kTY * kNpKC * kTX * 16;    // 16384: one split of an L2P stage
+constexpr int kNpABuf = 2 * kNpHaloSplit;                      // 43520
+constexpr int kNpNA = 4, kNpNB = 3;                            // A-stage buffers, weight ring depth
+constexpr int kNpConvWarp0 = 3, kNpConvWarps = 4, kNpEpiWarp0 = 7, kNpEpiWarps = 8;
+constexpr int kNpThreads = 32 * (kNpEpiWarp0 + kNpEpiWarps);  // 480
+constexpr int kNpConv = 32 * kNpConvWarps, kNpEpi = 32 * kNpEpiWarps;
+constexpr int kInMaxSlot = kMaxLevels - 1;                     // levmax slot of P2M's input maximum
+constexpr int kErrNp = 121;
+struct NpSmem {
+  static constexpr int a = 0;                                  // kNpNA A-stage buffers
+  static constexpr int b = kNpNA * kNpABuf;                    // kNpNB weight stages
+  static constexpr int bars = b + kNpNB * kStageBytes;         // 22 mbarriers
+  static constexpr int misc = bars + 24 * 8;                   // TMEM base, abort flag
+  static constexpr int dscr = misc + 16;                       // [2][kNpEpiWarps][3] double
+  static constexpr int total = dscr + 2 * kNpEpiWarps * 3 * 8;
+};
+static_assert(NpSmem::a % 128 == 0 && kNpABuf % 128 == 0 && kNpHaloSplit % 128 == 0 && kNpL2pSplit % 128 == 0,
+              "tensor-load destinations are 128-byte aligned");
+static_assert(2 * kNpL2pSplit <= kNpABuf, "an L2P stage fits an A-stage buffer");
+static_assert(NpSmem::total <= 227 * 1024, "shared memory of one CTA");
+
+// A-stage a of an item: returns 0 (halo K-group a, a < 4) or 1 (L2P stage
+// a - 4) and its index.  The L2P stages come last: tensor-core accumulation
+// rounds each step against the running sum, and interleaving the L2P terms
+// into the near-field sum measured 2x the operator error (5.5e-6 against
+// 2.5e-6 relative to FP64 on random inputs).
+__host__ __device__ inline int np_stage(int a, int nl2p, int &idx) {
+  (void)nl2p;
+  if (a < 4) {
+    idx = a;
+    return 0;
+  }
+  idx = a - 4;
+  return 1;
+}
+
+struct TcNearPipeArgs {
+  const float2 *x, *g;  // operator input (transformed by mode)
+  const float2 *xe;     // x of the `x - ...` epilogue
+  int64_t gstride;
+  int mode;
+  const int *active;
+  const uint8_t *B;  // weight stages in A-stage order
+  int nl2p;
+  float sw, sb;      // power-of-two scales of the near-field weights and the L2P basis
+  const unsigned *levmax, *locmax;  // [R][kMaxLevels]: P2M's input maximum (slot kInMaxSlot), M2L's locals
+  int lvl_leaf;
+  float2 *y;
+  int epi, red;
+  const float2 *dot_a;
+  double *part;
+  int nleaf, U, tiles_x, tiles_y, tiles, ppr, nitems;
+  int *err;
+};
+
+// The item's operand scales: input s1 and locals s2 lowered to a common product scale p = s1 sw = s2 sb.
+// A zero maximum (an all-zero input or locals) leaves the other operand's scale alone.
+__device__ __forceinline__ void np_scales(const TcNearPipeArgs &A, int rhs, float &s1, float &s2, float &p) {
+  const float mx = __uint_as_float(A.levmax[rhs * kMaxLevels + kInMaxSlot]);
+  const float ml = __uint_as_float(A.locmax[rhs * kMaxLevels + A.lvl_leaf]);
+  const float a = mx > 0.f ? pow2_scale(mx) * A.sw : INFINITY;
+  const float b = ml > 0.f ? pow2_scale(ml) * A.sb : INFINITY;
+  p = fminf(a, b);
+  if (!(p < INFINITY)) p = A.sw;
+  s1 = p / A.sw;
+  s2 = p / A.sb;
+}
+
+__global__ void __launch_bounds__(kNpThreads, 1) k_tc_near_pipe(TcNearPipeArgs A, const __grid_constant__ CUtensorMap tmh,
+                                                                const __grid_constant__ CUtensorMap tml) {
+  extern __shared__ __align__(1024) char sm[];
+  uint64_t *afull = (uint64_t *)(sm + NpSmem::bars);
+  uint64_t *aconv = afull + kNpNA, *afree = aconv + kNpNA;
+  uint64_t *bfull = afree + kNpNA, *bempty = bfull + kNpNB;
+  uint64_t *tfull = bempty + kNpNB, *tfree = tfull + 2, *mdone = tfree + 2;
+  uint32_t *tslot = (uint32_t *)(sm + NpSmem::misc);
+  volatile int *abort = (volatile int *)(sm + NpSmem::misc + 4);
+  double *dscr = (double *)(sm + NpSmem::dscr);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < 3 * kNpNA + 2 * kNpNB + 5; i++) mbar_init(afull + i, 1);
+    *abort = 0;
+    fence_mbar_init();
+  }
+  if (warp == 0) tmem_alloc(tslot, 512);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;  // set s, tile u: columns [256 s + 128 u, +128)
+  const int na = 4 + A.nl2p;     // A-stages per item
+  const int nb = 36 + A.nl2p;    // weight stages per item
+  auto next_item = [&](int w) {
+    do w += gridDim.x;
+    while (w < A.nitems && A.active && !A.active[w / A.ppr]);
+    return w;
+  };
+  const int first = (A.active && blockIdx.x < A.nitems && !A.active[blockIdx.x / A.ppr]) ? next_item(blockIdx.x)
+                                                                                           : blockIdx.x;
+  auto geom = [&](int w, int &rhs, int &ty0, int &tx0, int &ntile) {
+    rhs = w / A.ppr;
+    const int pr = w % A.ppr, pty = pr / A.tiles_x, ptx = pr % A.tiles_x;
+    ty0 = pty * kPair * kTY;
+    tx0 = ptx * kTX;
+    ntile = min(kPair, A.tiles_y - pty * kPair);
+  };
+
+  if (warp == 0) {
+    // ---- A-stage tensor loads: two boxes per stage (pixels / samples 0, 1 of every
+    // 4-element chunk into the hi slots, 2, 3 into the lo slots) ----
+    if (lane == 0) {
+      int ka = 0;
+      for (int w = first; w < A.nitems && !*abort; w = next_item(w)) {
+        int rhs, ty0, tx0, ntile;
+        geom(w, rhs, ty0, tx0, ntile);
+        for (int a = 0; a < na; a++, ka++) {
+          const int i = ka % kNpNA;
+          if (!mbar_wait_or(afree + i, ((ka / kNpNA) & 1) ^ 1, abort, A.err, kErrNp)) break;
+          char *dst = sm + NpSmem::a + i * kNpABuf;
+          int idx;
+          if (np_stage(a, A.nl2p, idx) == 0) {
+            mbar_expect_tx(afull + i, 2 * kNpHaloSplit);
+            tma_load_5d(dst, &tmh, 0, tx0 - 1, kNpKC * idx, ty0 - 1, rhs, afull + i);
+            tma_load_5d(dst + kNpHaloSplit, &tmh, 4, tx0 - 1, kNpKC * idx, ty0 - 1, rhs, afull + i);
+          } else {
+            mbar_expect_tx(afull + i, 2 * kNpL2pSplit);
+            tma_load_5d(dst, &tml, 0, tx0, kNpKC * idx, ty0, rhs, afull + i);
+            tma_load_5d(dst + kNpL2pSplit, &tml, 4, tx0, kNpKC * idx, ty0, rhs, afull + i);
+          }
+        }
+      }
+      // every load issued has landed before the CTA exits (bounded waits)
+      for (int j = 1; j <= kNpNA && j <= ka; j++) {
+        const int kk = ka - j;
+        mbar_wait(afull + kk % kNpNA, (kk / kNpNA) & 1, A.err, kErrNp);
+      }
+    }
+  } else if (warp == 1) {
+    // ---- weight stages through the ring, in A-stage order ----
+    if (lane == 0) {
+      int kb = 0;
+      for (int w = first; w < A.nitems && !*abort; w = next_item(w)) {
+        for (int t = 0; t < nb; t++, kb++) {
+          const int b = kb % kNpNB;
+          if (!mbar_wait_or(bempty + b, ((kb / kNpNB) & 1) ^ 1, abort, A.err, kErrNp)) break;
+          mbar_expect_tx(bfull + b, kStageBytes);
+          bulk_g2s(sm + NpSmem::b + b * kStageBytes, A.B + (size_t)t * kStageBytes, kStageBytes, bfull + b);
+        }
+      }
+      for (int j = 1; j <= kNpNB && j <= kb; j++) {
+        const int kk = kb - j;
+        mbar_wait(bfull + kk % kNpNB, (kk / kNpNB) & 1, A.err, kErrNp);
+      }
+    }
+  } else if (warp == 2) {
+    // ---- MMA issue (one thread): per weight stage, both tiles x 2 K-steps x 3 split products ----
+    if (lane == 0) {
+      const uint32_t idesc = idesc_f16_f32(128, 128), sbase = smem_u32(sm);
+      int ka = 0, kb = 0, it = 0;
+      bool ok = true;
+      for (int w = first; w < A.nitems && ok; w = next_item(w), it++) {
+        int rhs, ty0, tx0, ntile;
+        geom(w, rhs, ty0, tx0, ntile);
+        const int set = it & 1;
+        ok = mbar_wait_or(tfree + set, ((it >> 1) & 1) ^ 1, abort, A.err, kErrNp);
+        for (int a = 0; a < na && ok; a++, ka++) {
+          const int i = ka % kNpNA;
+          ok = mbar_wait_or(aconv + i, (ka / kNpNA) & 1, abort, A.err, kErrNp);
+          int idx;
+          const int kind = np_stage(a, A.nl2p, idx);
+          const uint32_t abase = sbase + NpSmem::a + i * kNpABuf;
+          const uint64_t ah0 = kind == 0 ? smem_desc(abase, kHC * 16, kNpKC * kHC * 16)
+                                         : smem_desc(abase, kTX * 16, kNpKC * kTX * 16);
+          const uint64_t al0 = kind == 0 ? smem_desc(abase + kNpHaloSplit, kHC * 16, kNpKC * kHC * 16)
+                                         : smem_desc(abase + kNpL2pSplit, kTX * 16, kNpKC * kTX * 16);
+          const int nq = kind == 0 ? 9 : 1;
+          for (int q = 0; q < nq && ok; q++, kb++) {
+            const int b = kb % kNpNB;
+            ok = mbar_wait_or(bfull + b, (kb / kNpNB) & 1, abort, A.err, kErrNp);
+            tc_fence_after();
+            if (!ok) break;
+            const uint32_t bb = sbase + NpSmem::b + b * kStageBytes;
+            const uint64_t bh0 = smem_desc(bb, 128, 512), bl0 = smem_desc(bb + kStageHalf, 128, 512);
+            const int dr = q / 3 - 1, dc = q % 3 - 1;
+#pragma unroll
+            for (int ks = 0; ks < 2; ks++) {
+              for (int u = 0; u < ntile; u++) {
+                const uint32_t aoff =
+                    kind == 0 ? (uint32_t)((u * kTY + 1 + dr) * (kNpKC * kHC * 16) + (1 + dc) * 16 + ks * 2 * (kHC * 16))
+                              : (uint32_t)(u * kTY * (kNpKC * kTX * 16) + ks * 2 * (kTX * 16));
+                const uint32_t d = tmem + (uint32_t)(set * 256 + u * 128);
+                const int acc = (a | q | ks) ? 1 : 0;
+                mma_f16(d, desc_add(ah0, aoff), desc_add(bh0, ks * 256), idesc, acc);
+                mma_f16(d, desc_add(ah0, aoff), desc_add(bl0, ks * 256), idesc, 1);
+                mma_f16(d, desc_add(al0, aoff), desc_add(bh0, ks * 256), idesc, 1);
+              }
+            }
+            mma_commit(bempty + b);
+          }
+          if (ok) mma_commit(afree + i);
+        }
+        if (ok) mma_commit(tfull + set);
+      }
+      // every MMA issued is complete before the CTA frees TMEM (bounded wait)
+      mma_commit(mdone);
+      mbar_wait(mdone, 0, A.err, kErrNp);
+    }
+  } else if (warp < kNpEpiWarp0) {
+    // ---- converters: the landed FP32 A-stage becomes FP16 hi/lo in place ----
+    const int ct = threadIdx.x - 32 * kNpConvWarp0;
+    int ka = 0;
+    for (int w = first; w < A.nitems; w = next_item(w)) {
+      int rhs, ty0, tx0, ntile;
+      geom(w, rhs, ty0, tx0, ntile);
+      float s1, s2, p;
+      np_scales(A, rhs, s1, s2, p);
+      const float2 *gr = A.g ? A.g + rhs * A.gstride : nullptr;
+      bool ok = true;
+      for (int a = 0; a < na; a++, ka++) {
+        const int i = ka % kNpNA;
+        ok = mbar_wait_or(afull + i, (ka / kNpNA) & 1, abort, A.err, kErrNp);
+        char *hi = sm + NpSmem::a + i * kNpABuf;
+        int idx;
+        if (np_stage(a, A.nl2p, idx) == 0) {
+          char *lo = hi + kNpHaloSplit;
+          // (halo row, chunk, halo column): off = ((hr * 4 + c) * 10 + hc) * 16
+          for (int e = ct; e < kHR * kNpKC * kHC && ok; e += kNpConv) {
+            const int hc = e % kHC, c = (e / kHC) % kNpKC, hr = e / (kHC * kNpKC);
+            float4 *ph = (float4 *)(hi + e * 16), *pl = (float4 *)(lo + e * 16);
+            const float4 a0 = *ph, a1 = *pl;
+            float4 g0 = make_float4(0.f, 0.f, 0.f, 0.f), g1 = g0;
+            if (A.mode == IN_G) {
+              const int ly = ty0 - 1 + hr, lx = tx0 - 1 + hc;
+              if (ly >= 0 && ly < A.nleaf && lx >= 0 && lx < A.nleaf) {
+                const size_t gi = (size_t)(ly * A.nleaf + lx) * kBB + 4 * (kNpKC * idx + c);
+                g0 = *(const float4 *)(gr + gi);
+                g1 = *(const float4 *)(gr + gi + 2);
+              }
+            }
+            const float2 v0 = transform(make_float2(a0.x, a0.y), make_float2(g0.x, g0.y), A.mode);
+            const float2 v1 = transform(make_float2(a0.z, a0.w), make_float2(g0.z, g0.w), A.mode);
+            const float2 v2 = transform(make_float2(a1.x, a1.y), make_float2(g1.x, g1.y), A.mode);
+            const float2 v3 = transform(make_float2(a1.z, a1.w), make_float2(g1.z, g1.w), A.mode);
+            uint32_t h[4], l[4];
+            split2u(v0.x * s1, v0.y * s1, h[0], l[0]);
+            split2u(v1.x * s1, v1.y * s1, h[1], l[1]);
+            split2u(v2.x * s1, v2.y * s1, h[2], l[2]);
+            split2u(v3.x * s1, v3.y * s1, h[3], l[3]);
+            st_shared_v4(ph, h);
+            st_shared_v4(pl, l);
+          }
+        } else {
+          char *lo = hi + kNpL2pSplit;
+          for (int e = ct; e < kPair * kTY * kNpKC * kTX && ok; e += kNpConv) {
+            float4 *ph = (float4 *)(hi + e * 16), *pl = (float4 *)(lo + e * 16);
+            const float4 a0 = *ph, a1 = *pl;
+            uint32_t h[4], l[4];
+            split2u(a0.x * s2, a0.y * s2, h[0], l[0]);
+            split2u(a0.z * s2, a0.w * s2, h[1], l[1]);
+            split2u(a1.x * s2, a1.y * s2, h[2], l[2]);
+            split2u(a1.z * s2, a1.w * s2, h[3], l[3]);
+            st_shared_v4(ph, h);
+            st_shared_v4(pl, l);
+          }
+        }
+        fence_proxy_async();
+        named_sync(1, kNpConv);
+        if (ct == 0) mbar_arrive(aconv + i);
+      }
+    }
+  } else {
+    // ---- epilogue: lane = leaf, 16-column chunks (8 pixels) straight to y ----
+    const int ew = warp - kNpEpiWarp0, qd = warp & 3, hh = ew >> 2;
+    const bool need_x = A.epi == EPI_FWD || A.epi == EPI_ADJ || A.red == RED_TS;
+    int it = 0;
+    for (int w = first; w < A.nitems; w = next_item(w), it++) {
+      int rhs, ty0, tx0, ntile;
+      geom(w, rhs, ty0, tx0, ntile);
+      const int set = it & 1;
+      float s1, s2, p;
+      np_scales(A, rhs, s1, s2, p);
+      const float inv = 1.f / p;
+      const bool ok = mbar_wait_or(tfull + set, (it >> 1) & 1, abort, A.err, kErrNp);
+      tc_fence_after();
+      const size_t rbase = (size_t)rhs * A.U;
+      const float2 *gr = A.g ? A.g + rhs * A.gstride : nullptr;
+      double r0 = 0, r1 = 0, r2 = 0;
+      const int m = 32 * qd + lane;
+      for (int u = 0; u < ntile; u++) {
+        const int ly = ty0 + u * kTY + m / kTX, lx = tx0 + m % kTX;
+        const bool live = ok && ly < A.nleaf && lx < A.nleaf;
+        const size_t lb = rbase + (size_t)(ly * A.nleaf + lx) * kBB;
+#pragma unroll 1
+        for (int ch = 0; ch < 4; ch++) {
+          const int col = 64 * hh + 16 * ch;
+          float d[16];
+          tmem_ld16(tmem + ((uint32_t)(32 * qd) << 16) + (uint32_t)(set * 256 + u * 128 + col), d);
+          if (!live) continue;
+          const size_t i0 = lb + col / 2;
+          float4 xv[4], av[4], gv[4];
+#pragma unroll
+          for (int k = 0; k < 4; k++) {
+            xv[k] = need_x ? *(const float4 *)(A.xe + i0 + 2 * k) : make_float4(0.f, 0.f, 0.f, 0.f);
+            av[k] = A.red == RED_DOT ? *(const float4 *)(A.dot_a + i0 + 2 * k) : make_float4(0.f, 0.f, 0.f, 0.f);
+            gv[k] = A.epi == EPI_ADJ ? *(const float4 *)(gr + (i0 - rbase) + 2 * k) : make_float4(0.f, 0.f, 0.f, 0.f);
+          }
+#pragma unroll
+          for (int k = 0; k < 4; k++) {
+            float2 o[2] = {make_float2(d[4 * k] * inv, d[4 * k + 1] * inv),
+                           make_float2(d[4 * k + 2] * inv, d[4 * k + 3] * inv)};
+            const float2 xin[2] = {make_float2(xv[k].x, xv[k].y), make_float2(xv[k].z, xv[k].w)};
+            if (A.epi == EPI_FWD) {
+              o[0] = csub(xin[0], o[0]);
+              o[1] = csub(xin[1], o[1]);
+            } else if (A.epi == EPI_ADJ) {
+              o[0] = csub(xin[0], cconj(cmul(make_float2(gv[k].x, gv[k].y), o[0])));
+              o[1] = csub(xin[1], cconj(cmul(make_float2(gv[k].z, gv[k].w), o[1])));
+            } else if (A.epi == EPI_CONJ) {
+              o[0] = cconj(o[0]);
+              o[1] = cconj(o[1]);
+            }
+            *(float4 *)(A.y + i0 + 2 * k) = make_float4(o[0].x, o[0].y, o[1].x, o[1].y);
+            if (A.red == RED_DOT) {
+              const float2 a0 = make_float2(av[k].x, av[k].y), a1 = make_float2(av[k].z, av[k].w);
+              r0 += (double)a0.x * o[0].x + (double)a0.y * o[0].y + (double)a1.x * o[1].x + (double)a1.y * o[1].y;
+              r1 += (double)a0.x * o[0].y - (double)a0.y * o[0].x + (double)a1.x * o[1].y - (double)a1.y * o[1].x;
+            } else if (A.red == RED_TS) {
+#pragma unroll
+              for (int e2 = 0; e2 < 2; e2++) {
+                r0 += (double)o[e2].x * xin[e2].x + (double)o[e2].y * xin[e2].y;
+                r1 += (double)o[e2].x * xin[e2].y - (double)o[e2].y * xin[e2].x;
+                r2 += (double)o[e2].x * o[e2].x + (double)o[e2].y * o[e2].y;
+              }
+            }
+          }
+        }
+      }
+      if (A.red != RED_NONE) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          r0 += __shfl_xor_sync(0xffffffffu, r0, o);
+          r1 += __shfl_xor_sync(0xffffffffu, r1, o);
+          r2 += __shfl_xor_sync(0xffffffffu, r2, o);
+        }
+        if (lane == 0) {
+          double *ds = dscr + (set * kNpEpiWarps + ew) * 3;
+          ds[0] = r0;
+          ds[1] = r1;
+          ds[2] = r2;
+        }
+      }
+      tc_fence_before();
+      named_sync(2, kNpEpi);  // the accumulator set is read out, the warps' sums are in dscr
+      if (ew == 0 && lane == 0) {
+        mbar_arrive(tfree + set);
+        if (A.red != RED_NONE && ok) {
+          double s0 = 0, s1v = 0, s2v = 0;
+          for (int k = 0; k < kNpEpiWarps; k++) {
+            const double *ds = dscr + (set * kNpEpiWarps + k) * 3;
+            s0 += ds[0];
+            s1v += ds[1];
+            s2v += ds[2];
+          }
+          // the pair's sum goes to its first tile's slot, zero to the second's
+          const int pr = w % A.ppr, pty = pr / A.tiles_x, ptx = pr % A.tiles_x;
+          for (int u = 0; u < ntile; u++) {
+            double *pp = A.part + ((size_t)rhs * A.tiles + (pty * kPair + u) * A.tiles_x + ptx) * 4;
+            pp[0] = u ? 0.0 : s0;
+            pp[1] = u ? 0.0 : s1v;
+            pp[2] = u ? 0.0 : s2v;
+            pp[3] = 0.0;
+          }
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, 512);
+}
+
 // ---- P2M: persistent CTAs over (RHS, 128-leaf tile) items, N = 2 ns padded to 16 ----
 // The coefficient matrix is loaded once per CTA; each item's input is loaded
 // into registers while the previous item's outputs are written, converted to
@@ -606,6 +1009,9 @@ __global__ void __launch_bounds__(256, 1) k_tc_p2m(TcP2mArgs A) {
     float m2 = 0.f;
     for (int k = 0; k < 8; k++) m2 = fmaxf(m2, fscr[k]);
     const float s = pow2_scale(m2);
+    // the input's maximum per RHS: the near-field kernel's scale for the same input
+    if (threadIdx.x == 0 && m2 > 0.f && A.lvl < kInMaxSlot)
+      atomicMax(&A.levmax[(w / A.tiles) * kMaxLevels + kInMaxSlot], __float_as_uint(m2));
 #pragma unroll
     for (int r = 0; r < kPer; r++) {
       const int it = threadIdx.x + r * 256;
@@ -789,6 +1195,9 @@ __global__ void __launch_bounds__(kP2mThreads, 1) k_tc_p2m_pipe(TcP2mArgs A) {
       float m2 = 0.f;
       for (int k = 0; k < kP2mConvWarps; k++) m2 = fmaxf(m2, fscr[k]);
       const float s = pow2_scale(m2);
+      // the input's maximum per RHS: the near-field kernel's scale for the same input
+      if (threadIdx.x == 0 && fok && m2 > 0.f && A.lvl < kInMaxSlot)
+        atomicMax(&A.levmax[(w / A.tiles) * kMaxLevels + kInMaxSlot], __float_as_uint(m2));
       char *ahi = sm + P2mPipeSmem::a(b), *alo = ahi + kP2mA;
       if (fok) {
 #pragma unroll
@@ -923,8 +1332,10 @@ void pack_stage(std::vector<uint8_t> &buf, size_t at, int nrows, int k0, double 
 
 struct TcPlan {
   uint8_t *nearB = nullptr;
+  uint8_t *nearNp = nullptr;  // the same stages in the pipelined kernel's A-stage order
   int nl2p = 0;
   float inv_w = 1, inv_b = 1;
+  float sw = 1, sb = 1;
   uint8_t *p2mB = nullptr;
   int npad = 0, p2m_stage = 0;
   float inv_c = 1;
@@ -981,6 +1392,22 @@ isg_status tc_setup(isg_ctx *c) {
     pack_stage(nb, (size_t)(kNearStages + c2) * kStageBytes, 128, c2 * 32, sb, breal);
   P.inv_w = (float)(1.0 / sw);
   P.inv_b = (float)(1.0 / sb);
+  P.sw = (float)sw;
+  P.sb = (float)sb;
+  // pipelined kernel: per A-stage, a halo K-group's nine slots or one L2P stage
+  std::vector<uint8_t> np((size_t)(kNearStages + P.nl2p) * kStageBytes, 0);
+  {
+    size_t t = 0;
+    for (int a = 0; a < 4 + P.nl2p; a++) {
+      int idx;
+      if (np_stage(a, P.nl2p, idx) == 0) {
+        for (int q = 0; q < 9; q++, t++)
+          pack_stage(np, t * kStageBytes, 128, idx * 32, sw, [&](int n, int k) { return wreal(q, n, k); });
+      } else {
+        pack_stage(np, (t++) * kStageBytes, 128, idx * 32, sb, breal);
+      }
+    }
+  }
   // P2M: row n = 2k + d over samples (padded to a multiple of 16), K = 2 pixel + e
   P.npad = ((2 * ns + 15) / 16) * 16;
   P.p2m_stage = P.npad * 32 * 2 * 2;
@@ -995,12 +1422,15 @@ isg_status tc_setup(isg_ctx *c) {
   P.inv_c = (float)(1.0 / sc);
   isg_status e;
   if ((e = cuda_check(c, cudaMalloc(&P.nearB, nb.size()), "tc alloc")) != ISG_OK) return e;
+  if ((e = cuda_check(c, cudaMalloc(&P.nearNp, np.size()), "tc alloc")) != ISG_OK) return e;
   if ((e = cuda_check(c, cudaMalloc(&P.p2mB, pb.size()), "tc alloc")) != ISG_OK) return e;
   if ((e = cuda_check(c, cudaMalloc(&P.err, sizeof(int)), "tc alloc")) != ISG_OK) return e;
   cudaMemcpy(P.nearB, nb.data(), nb.size(), cudaMemcpyHostToDevice);
+  cudaMemcpy(P.nearNp, np.data(), np.size(), cudaMemcpyHostToDevice);
   cudaMemcpy(P.p2mB, pb.data(), pb.size(), cudaMemcpyHostToDevice);
   cudaMemset(P.err, 0, sizeof(int));
   cudaFuncSetAttribute(k_tc_near, cudaFuncAttributeMaxDynamicSharedMemorySize, NearSmem::total);
+  cudaFuncSetAttribute(k_tc_near_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize, NpSmem::total);
   cudaFuncSetAttribute(k_tc_p2m, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)P2mSmem::total(P.p2m_stage, ns));
   cudaFuncSetAttribute(k_tc_p2m_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1013,6 +1443,7 @@ isg_status tc_setup(isg_ctx *c) {
 void tc_destroy(isg_ctx *c) {
   if (!c->tc) return;
   cudaFree(c->tc->nearB);
+  cudaFree(c->tc->nearNp);
   cudaFree(c->tc->p2mB);
   cudaFree(c->tc->err);
   delete c->tc;
@@ -1051,6 +1482,75 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   return fn;
 }
 
+// The pipelined near-field kernel; returns false (launching nothing) when the
+// call does not meet its conditions: P2M's input maximum known (N.inmax), leaf
+// rings of a multiple of 4 samples (<= 80), 16-byte aligned vectors and both
+// tensor maps encoded.
+static bool tc_near_pipe(isg_ctx *c, const NearArgs &N, cudaStream_t st, isg_status *e) {
+  const DevPlan &P = c->P;
+  const TcPlan &T = *c->tc;
+  const float2 *loc_leaf = N.loc + P.lv[P.L - 1].off;
+  if (!N.inmax || !N.locmax || !T.nearNp || P.ns_leaf % 4 || P.ns_leaf > 4 * kLocChunksMax || P.mp % 2 ||
+      !aligned16(loc_leaf) || P.L - 1 >= kInMaxSlot)
+    return false;
+  const PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+  if (!encode) return false;
+  TcNearPipeArgs A;
+  A.x = N.in.x;
+  A.xe = N.x_epi ? N.x_epi : N.in.x;
+  A.g = N.in.g;
+  A.gstride = N.in.gstride;
+  A.mode = N.in.mode;
+  A.active = N.in.active;
+  A.B = T.nearNp;
+  A.nl2p = T.nl2p;
+  A.sw = T.sw;
+  A.sb = T.sb;
+  A.levmax = N.inmax;
+  A.locmax = N.locmax;
+  A.lvl_leaf = P.L - 1;
+  A.y = N.y;
+  A.epi = N.epi;
+  A.red = N.red;
+  A.dot_a = N.dot_a;
+  A.part = N.part;
+  A.nleaf = P.nleaf;
+  A.U = P.U;
+  A.tiles_x = (P.nleaf + kTX - 1) / kTX;
+  A.tiles_y = (P.nleaf + kTY - 1) / kTY;
+  A.tiles = A.tiles_x * A.tiles_y;
+  A.ppr = A.tiles_x * ((A.tiles_y + kPair - 1) / kPair);
+  A.nitems = A.ppr * N.in.nrhs;
+  A.err = T.err;
+  // tmh: the input as [RHS][leaf row][4-pixel chunk][leaf column][8 floats], a box is
+  // one halo K-group (4 chunks) of the pair's 34 x 10 halo; tml: the leaf locals as
+  // [RHS][leaf row][4-sample chunk][leaf column][8 floats], a box is one L2P stage
+  CUtensorMap tmh, tml;
+  memset(&tmh, 0, sizeof(tmh));
+  memset(&tml, 0, sizeof(tml));
+  const cuuint32_t one[5] = {1, 1, 1, 1, 1};
+  const cuuint64_t hd[5] = {8, (cuuint64_t)P.nleaf, 16, (cuuint64_t)P.nleaf, (cuuint64_t)N.in.nrhs};
+  const cuuint64_t hs[4] = {(cuuint64_t)kBB * 8, 32, (cuuint64_t)P.nleaf * kBB * 8, (cuuint64_t)P.U * 8};
+  const cuuint32_t hb[5] = {4, (cuuint32_t)kHC, (cuuint32_t)kNpKC, (cuuint32_t)kHR, 1};
+  const cuuint64_t ld[5] = {8, (cuuint64_t)P.nleaf, (cuuint64_t)(P.ns_leaf / 4), (cuuint64_t)P.nleaf,
+                            (cuuint64_t)N.in.nrhs};
+  const cuuint64_t ls[4] = {(cuuint64_t)P.ns_leaf * 8, 32, (cuuint64_t)P.nleaf * P.ns_leaf * 8, (cuuint64_t)P.mp * 8};
+  const cuuint32_t lb[5] = {4, (cuuint32_t)kTX, (cuuint32_t)kNpKC, (cuuint32_t)(kPair * kTY), 1};
+  if (encode(&tmh, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, (void *)A.x, hd, hs, hb, one, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS ||
+      encode(&tml, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, (void *)loc_leaf, ld, ls, lb, one,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return false;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->opts.device);
+  count_launch();
+  k_tc_near_pipe<<<std::min(A.nitems, sms), kNpThreads, NpSmem::total, st>>>(A, tmh, tml);
+  *e = cuda_check(c, cudaGetLastError(), "tc near launch");
+  return true;
+}
+
 isg_status tc_near(isg_ctx *c, const NearArgs &N, cudaStream_t st) {
   const DevPlan &P = c->P;
   const TcPlan &T = *c->tc;
@@ -1058,6 +1558,8 @@ isg_status tc_near(isg_ctx *c, const NearArgs &N, cudaStream_t st) {
       (N.dot_a && !aligned16(N.dot_a)) ||
       (N.in.gstride % 2) || N.epi == EPI_L2P_ONLY)
     return ISG_UNSUPPORTED;
+  isg_status pe = ISG_OK;
+  if (tc_near_pipe(c, N, st, &pe)) return pe;
   TcNearArgs A;
   A.x = N.in.x;
   A.xe = N.x_epi ? N.x_epi : N.in.x;
