@@ -248,7 +248,10 @@ isg_status isg_create(const isg_opts *opts, isg_ctx **out) {
   if (opts->max_rhs < 1 || opts->max_rhs > kMaxGridY) return ISG_BAD_ARG;
   isg_ctx *c = new isg_ctx();
   c->opts = *opts;
-  std::string err = build_tables(opts->level, opts->box, opts->res, opts->k0, opts->beta, opts->ninter, opts->numrx, c->T);
+  // the near-field blocks and translation operators wait for the device (set-up)
+  // or for a table query, whichever comes first
+  std::string err =
+      build_tables(opts->level, opts->box, opts->res, opts->k0, opts->beta, opts->ninter, opts->numrx, c->T, false);
   if (!err.empty()) {
     delete c;
     return ISG_BAD_ARG;
@@ -269,6 +272,7 @@ isg_status isg_setup_gpu(isg_ctx *c) {
   isg_status e;
   if ((e = cuda_check(c, cudaSetDevice(c->opts.device), "cudaSetDevice")) != ISG_OK) return e;
   if ((e = cuda_check(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream")) != ISG_OK) return e;
+  if (!c->T.green_ready && (e = green_tables_gpu(c)) != ISG_OK) return e;
   const HostTables &T = c->T;
   DevPlan &P = c->P;
   const int L = T.L, ns = T.nsamp[L - 1], ni = T.ninter, W = 2 * ni;
@@ -415,6 +419,7 @@ isg_status isg_host_table(const isg_ctx *c, const char *name, int lvl, const voi
     return ISG_OK;
   };
   const bool lv_ok = lvl >= 0 && lvl < T.L;
+  if ((n == "near" || n == "trans") && !T.green_ready) build_green_tables(const_cast<HostTables &>(T));
   if (n == "numsamp") return put(T.nsamp);
   if (n == "numterm") return put(T.nterm);
   if (n == "clusize") return put(T.csize);

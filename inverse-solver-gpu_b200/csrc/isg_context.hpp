@@ -107,6 +107,9 @@ bool band_m2m(isg_ctx *c, int lvl, float2 *mul, int nrhs, const int *active, cud
 // L2L into child level lvl on the tensor cores (overwrites its locals); false
 // when the level is not covered (its rings have more than 128 samples).
 bool band_l2l(isg_ctx *c, int lvl, float2 *loc, int nrhs, const int *active, cudaStream_t st, isg_status *e);
+// The near-field blocks and translation operators computed on the device into
+// the host tables (isg_tables_gpu.cu); called by isg_setup_gpu.
+isg_status green_tables_gpu(isg_ctx *c);
 // Static scratch of isg_aggregate_noalloc (isg_noalloc.cu): resolves its
 // address and loads its kernels; called by isg_setup_gpu.
 isg_status noalloc_prepare(isg_ctx *c);

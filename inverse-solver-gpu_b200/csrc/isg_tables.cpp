@@ -96,7 +96,53 @@ static std::string transpose_interp(const std::vector<double> &w, const std::vec
   return "";
 }
 
-std::string build_tables(int level, int box, double res, double k0, int beta, int ninter, int numrx, HostTables &t) {
+void build_green_tables(HostTables &t) {
+  const int L = t.L, box = t.box, bb = t.bb;
+  const double res = t.res, k0 = t.k0;
+  // Near-field blocks (setup_mlfma.cpp:492-505): testing pixel t of a leaf,
+  // basis pixel b of the neighbour leaf in slot s; translation-invariant.
+  t.near.assign((size_t)9 * bb * bb, cd(0, 0));
+  for (int s = 0; s < 9; s++) {
+    const int dr = s / 3 - 1, dc = s % 3 - 1;
+    for (int ti = 0; ti < bb; ti++)
+      for (int bi = 0; bi < bb; bi++) {
+        const int ty = ti / box, tx = ti % box, by = bi / box, bx = bi % box;
+        const double dx = (dc * box + bx - tx) * res;
+        const double dy = -(dr * box + by - ty) * res;
+        t.near[((size_t)s * bb + ti) * bb + bi] = green_entry(k0, res, dx, dy);
+      }
+  }
+
+  // Diagonal translation operators for the 7x7 offsets (setup_mlfma.cpp:506-543).
+  t.trans.assign(L, {});
+  {
+    std::vector<cd> hank, ipow;
+    for (int p = 0; p < t.nterm[0]; p++) ipow.push_back(std::exp(cd(0, (p + 1) * kPi / 2)));
+    for (int i = 2; i < L; i++) {
+      const int ns = t.nsamp[i], P = t.nterm[i];
+      const double a = t.csize[i];
+      t.trans[i].assign((size_t)49 * ns, cd(0, 0));
+      hank.assign(P + 1, cd(0, 0));
+      for (int cm = 0; cm < 7; cm++)
+        for (int cn = 0; cn < 7; cn++) {
+          const cd r = -cd(-3 * a + cn * a, 3 * a - cm * a);  // observation minus source centre
+          if (!(std::abs(r) > a * std::sqrt(3.0))) continue;
+          const double kr = k0 * std::abs(r), phi = std::arg(r);
+          for (int p = 0; p <= P; p++) hank[p] = cd(jn(p, kr), yn(p, kr));
+          for (int k = 0; k < ns; k++) {
+            cd sum = hank[0];
+            for (int p = 1; p <= P; p++) sum = sum + 2 * std::cos(p * (2 * kPi * k / ns - phi)) * hank[p] * ipow[p - 1];
+            t.trans[i][(size_t)(cm * 7 + cn) * ns + k] = sum;
+          }
+        }
+    }
+  }
+
+  t.green_ready = true;
+}
+
+std::string build_tables(int level, int box, double res, double k0, int beta, int ninter, int numrx, HostTables &t,
+                         bool with_green) {
   if (level < 3 || level > 12) return "level must be in [3, 12]";
   if (box != 8) return "only 8x8-pixel leaves are supported";
   if (ninter < 2 || ninter % 2) return "ninter must be even and >= 2";
@@ -130,20 +176,6 @@ std::string build_tables(int level, int box, double res, double k0, int beta, in
   }
   const int nsl = t.nsamp[L - 1];
 
-  // Near-field blocks (setup_mlfma.cpp:492-505): testing pixel t of a leaf,
-  // basis pixel b of the neighbour leaf in slot s; translation-invariant.
-  t.near.assign((size_t)9 * bb * bb, cd(0, 0));
-  for (int s = 0; s < 9; s++) {
-    const int dr = s / 3 - 1, dc = s % 3 - 1;
-    for (int ti = 0; ti < bb; ti++)
-      for (int bi = 0; bi < bb; bi++) {
-        const int ty = ti / box, tx = ti % box, by = bi / box, bx = bi % box;
-        const double dx = (dc * box + bx - tx) * res;
-        const double dy = -(dr * box + by - ty) * res;
-        t.near[((size_t)s * bb + ti) * bb + bi] = green_entry(k0, res, dx, dy);
-      }
-  }
-
   // Plane-wave P2M coefficients and L2P basis about the leaf centre
   // (setup_mlfma.cpp:544-553, integrate.cpp:43-69).
   t.coeff.resize((size_t)nsl * bb);
@@ -161,30 +193,7 @@ std::string build_tables(int level, int box, double res, double k0, int beta, in
     }
   }
 
-  // Diagonal translation operators for the 7x7 offsets (setup_mlfma.cpp:506-543).
-  t.trans.assign(L, {});
-  {
-    std::vector<cd> hank, ipow;
-    for (int p = 0; p < t.nterm[0]; p++) ipow.push_back(std::exp(cd(0, (p + 1) * kPi / 2)));
-    for (int i = 2; i < L; i++) {
-      const int ns = t.nsamp[i], P = t.nterm[i];
-      const double a = t.csize[i];
-      t.trans[i].assign((size_t)49 * ns, cd(0, 0));
-      hank.assign(P + 1, cd(0, 0));
-      for (int cm = 0; cm < 7; cm++)
-        for (int cn = 0; cn < 7; cn++) {
-          const cd r = -cd(-3 * a + cn * a, 3 * a - cm * a);  // observation minus source centre
-          if (!(std::abs(r) > a * std::sqrt(3.0))) continue;
-          const double kr = k0 * std::abs(r), phi = std::arg(r);
-          for (int p = 0; p <= P; p++) hank[p] = cd(jn(p, kr), yn(p, kr));
-          for (int k = 0; k < ns; k++) {
-            cd sum = hank[0];
-            for (int p = 1; p <= P; p++) sum = sum + 2 * std::cos(p * (2 * kPi * k / ns - phi)) * hank[p] * ipow[p - 1];
-            t.trans[i][(size_t)(cm * 7 + cn) * ns + k] = sum;
-          }
-        }
-    }
-  }
+  if (with_green) build_green_tables(t);
 
   // Shift phases to the four children (setup_mlfma.cpp:554-570); child
   // q = row*2 + col, rho = parent centre - child centre.

@@ -57,10 +57,21 @@ struct HostTables {
   std::vector<int> tree_of_blocked;    // blocked index -> tree index
   std::vector<int> raster_of_blocked;  // blocked index -> raster index
   std::vector<cd> pos_raster;   // pixel centres in raster order
+
+  // near and trans (the Green's-function tables) are filled: by the host
+  // (build_green_tables) or by the device at set-up (isg_tables_gpu.cu)
+  bool green_ready = false;
 };
 
-// Builds every table; returns an empty string or an error message.
-std::string build_tables(int level, int box, double res, double k0, int beta, int ninter, int numrx, HostTables &t);
+// Builds every table; returns an empty string or an error message.  With
+// with_green false the near-field blocks and translation operators (the
+// tables that evaluate Bessel functions) are left for build_green_tables or
+// the device.
+std::string build_tables(int level, int box, double res, double k0, int beta, int ninter, int numrx, HostTables &t,
+                         bool with_green = true);
+// The near-field blocks and translation operators on the host (glibc jn, yn,
+// j0, y0), as the reference computes them.
+void build_green_tables(HostTables &t);
 
 // integrate.cpp:15-41 for the displacement (posb - post) = (dx, dy).
 cd green_entry(double k0, double res, double dx, double dy);

@@ -502,16 +502,19 @@ __global__ void __launch_bounds__(256, 1) k_tc_near(TcNearArgs A, const __grid_c
 // persistent CTA walks them in steps of gridDim.x.  An item's K dimension (9
 // neighbour slots x 128 source reals of the halo, then 2 ns reals of the leaf
 // locals for L2P) is staged in shared memory one A-stage at a time: a halo
-// K-group (32 source reals of every leaf of the pair's 34 x 10-leaf halo,
-// 43.5 KB as FP16 hi/lo) feeds the nine weight stages of its K range; an L2P
-// stage (32 reals of the locals of the pair's 256 leaves) feeds one.  Stage
-// order: H0 H1 H2 H3 L0 .. L4; the weights are packed in the same order.  The
-// whole halo is never resident, so four A-stage buffers and a three-deep
+// K-group (32 source reals of every leaf of the pair's 34 x 10-leaf halo)
+// feeds the nine weight stages of its K range; an L2P stage (32 reals of the
+// locals of the pair's 256 leaves) feeds one.  Stage order: H0 H1 H2 H3 L0 ..
+// L4; the weights are packed in the same order.  An A-stage arrives as FP32 by
+// one tensor load whose rows are a leaf's 32 reals (128 contiguous bytes) into
+// a staging buffer, and the converters write it as FP16 hi/lo in the MMA's
+// core-matrix layout into an operand buffer.  The whole halo is never
+// resident, so two staging buffers, two operand buffers and a three-deep
 // weight ring fit in shared memory and the roles overlap:
-//   warp 0      tensor loads of the A-stages (5-D maps, no multicast)
+//   warp 0      tensor loads of the A-stages (4-D maps, no multicast)
 //   warp 1      bulk copies of the weight stages
 //   warp 2      MMA issue (one thread)
-//   warps 3..6  A-stage conversion to FP16 hi/lo, in place
+//   warps 3..6  A-stage conversion to FP16 hi/lo
 //   warps 7..14 epilogue, two per TMEM lane quarter (columns 0..63, 64..127)
 // Near field and L2P accumulate into one TMEM accumulator per tile: the input
 // is scaled by the power of two that P2M's per-RHS maximum gives and the
@@ -519,26 +522,28 @@ __global__ void __launch_bounds__(256, 1) k_tc_near(TcNearArgs A, const __grid_c
 // two.  Two accumulator sets (two tiles x 128 columns each) alternate between
 // items, so an item's epilogue runs under the next item's MMAs.
 constexpr int kNpKC = 4;                                       // 8-real K-chunks per A-stage
-constexpr int kNpHaloSplit = kHR * kNpKC * kHC * 16;           // 21760: one split of a halo K-group
-constexpr int kNpL2pSplit = kPair * kTY * kNpKC * kTX * 16;    // 16384: one split of an L2P stage
-constexpr int kNpABuf = 2 * kNpHaloSplit;                      // 43520
-constexpr int kNpNA = 4, kNpNB = 3;                            // A-stage buffers, weight ring depth
+constexpr int kNpHaloSplit = kHR * kNpKC * kHC * 16;           // 21760: one FP16 split of a halo K-group
+constexpr int kNpL2pSplit = kPair * kTY * kNpKC * kTX * 16;    // 16384: one FP16 split of an L2P stage
+constexpr int kNpBuf = 2 * kNpHaloSplit;                       // 43520: an operand (hi, lo) or a staged A-stage
+constexpr int kNpHaloBytes = kHR * kHC * 32 * 4;               // 43520: a halo K-group as FP32
+constexpr int kNpL2pBytes = kPair * kTY * kTX * 32 * 4;        // 32768: an L2P stage as FP32
+constexpr int kNpNS = 2, kNpNO = 2, kNpNB = 3;                 // staging, operand buffers, weight ring depth
 constexpr int kNpConvWarp0 = 3, kNpConvWarps = 4, kNpEpiWarp0 = 7, kNpEpiWarps = 8;
 constexpr int kNpThreads = 32 * (kNpEpiWarp0 + kNpEpiWarps);  // 480
 constexpr int kNpConv = 32 * kNpConvWarps, kNpEpi = 32 * kNpEpiWarps;
 constexpr int kInMaxSlot = kMaxLevels - 1;                     // levmax slot of P2M's input maximum
 constexpr int kErrNp = 121;
 struct NpSmem {
-  static constexpr int a = 0;                                  // kNpNA A-stage buffers
-  static constexpr int b = kNpNA * kNpABuf;                    // kNpNB weight stages
-  static constexpr int bars = b + kNpNB * kStageBytes;         // 22 mbarriers
+  static constexpr int s = 0;                                  // kNpNS FP32 staging buffers
+  static constexpr int o = kNpNS * kNpBuf;                     // kNpNO FP16 hi/lo operand buffers
+  static constexpr int b = o + kNpNO * kNpBuf;                 // kNpNB weight stages
+  static constexpr int bars = b + kNpNB * kStageBytes;         // 19 mbarriers
   static constexpr int misc = bars + 24 * 8;                   // TMEM base, abort flag
   static constexpr int dscr = misc + 16;                       // [2][kNpEpiWarps][3] double
   static constexpr int total = dscr + 2 * kNpEpiWarps * 3 * 8;
 };
-static_assert(NpSmem::a % 128 == 0 && kNpABuf % 128 == 0 && kNpHaloSplit % 128 == 0 && kNpL2pSplit % 128 == 0,
-              "tensor-load destinations are 128-byte aligned");
-static_assert(2 * kNpL2pSplit <= kNpABuf, "an L2P stage fits an A-stage buffer");
+static_assert(kNpBuf % 128 == 0 && NpSmem::o % 128 == 0, "tensor-load destinations are 128-byte aligned");
+static_assert(kNpHaloBytes <= kNpBuf && kNpL2pBytes <= kNpBuf && 2 * kNpL2pSplit <= kNpBuf, "buffer sizes");
 static_assert(NpSmem::total <= 227 * 1024, "shared memory of one CTA");
 
 // A-stage a of an item: returns 0 (halo K-group a, a < 4) or 1 (L2P stage
@@ -591,16 +596,17 @@ __device__ __forceinline__ void np_scales(const TcNearPipeArgs &A, int rhs, floa
 __global__ void __launch_bounds__(kNpThreads, 1) k_tc_near_pipe(TcNearPipeArgs A, const __grid_constant__ CUtensorMap tmh,
                                                                 const __grid_constant__ CUtensorMap tml) {
   extern __shared__ __align__(1024) char sm[];
-  uint64_t *afull = (uint64_t *)(sm + NpSmem::bars);
-  uint64_t *aconv = afull + kNpNA, *afree = aconv + kNpNA;
-  uint64_t *bfull = afree + kNpNA, *bempty = bfull + kNpNB;
+  uint64_t *sfull = (uint64_t *)(sm + NpSmem::bars);  // staging landed / read out
+  uint64_t *sfree = sfull + kNpNS;
+  uint64_t *ofull = sfree + kNpNS, *ofree = ofull + kNpNO;  // operand converted / consumed by the MMAs
+  uint64_t *bfull = ofree + kNpNO, *bempty = bfull + kNpNB;
   uint64_t *tfull = bempty + kNpNB, *tfree = tfull + 2, *mdone = tfree + 2;
   uint32_t *tslot = (uint32_t *)(sm + NpSmem::misc);
   volatile int *abort = (volatile int *)(sm + NpSmem::misc + 4);
   double *dscr = (double *)(sm + NpSmem::dscr);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
-    for (int i = 0; i < 3 * kNpNA + 2 * kNpNB + 5; i++) mbar_init(afull + i, 1);
+    for (int i = 0; i < 2 * kNpNS + 2 * kNpNO + 2 * kNpNB + 5; i++) mbar_init(sfull + i, 1);
     *abort = 0;
     fence_mbar_init();
   }
@@ -627,33 +633,30 @@ __global__ void __launch_bounds__(kNpThreads, 1) k_tc_near_pipe(TcNearPipeArgs A
   };
 
   if (warp == 0) {
-    // ---- A-stage tensor loads: two boxes per stage (pixels / samples 0, 1 of every
-    // 4-element chunk into the hi slots, 2, 3 into the lo slots) ----
+    // ---- A-stage tensor loads into the staging buffers: rows of 32 reals ----
     if (lane == 0) {
       int ka = 0;
       for (int w = first; w < A.nitems && !*abort; w = next_item(w)) {
         int rhs, ty0, tx0, ntile;
         geom(w, rhs, ty0, tx0, ntile);
         for (int a = 0; a < na; a++, ka++) {
-          const int i = ka % kNpNA;
-          if (!mbar_wait_or(afree + i, ((ka / kNpNA) & 1) ^ 1, abort, A.err, kErrNp)) break;
-          char *dst = sm + NpSmem::a + i * kNpABuf;
+          const int i = ka % kNpNS;
+          if (!mbar_wait_or(sfree + i, ((ka / kNpNS) & 1) ^ 1, abort, A.err, kErrNp)) break;
+          char *dst = sm + NpSmem::s + i * kNpBuf;
           int idx;
           if (np_stage(a, A.nl2p, idx) == 0) {
-            mbar_expect_tx(afull + i, 2 * kNpHaloSplit);
-            tma_load_5d(dst, &tmh, 0, tx0 - 1, kNpKC * idx, ty0 - 1, rhs, afull + i);
-            tma_load_5d(dst + kNpHaloSplit, &tmh, 4, tx0 - 1, kNpKC * idx, ty0 - 1, rhs, afull + i);
+            mbar_expect_tx(sfull + i, kNpHaloBytes);
+            tma_load_4d(dst, &tmh, 32 * idx, tx0 - 1, ty0 - 1, rhs, sfull + i);
           } else {
-            mbar_expect_tx(afull + i, 2 * kNpL2pSplit);
-            tma_load_5d(dst, &tml, 0, tx0, kNpKC * idx, ty0, rhs, afull + i);
-            tma_load_5d(dst + kNpL2pSplit, &tml, 4, tx0, kNpKC * idx, ty0, rhs, afull + i);
+            mbar_expect_tx(sfull + i, kNpL2pBytes);
+            tma_load_4d(dst, &tml, 32 * idx, tx0, ty0, rhs, sfull + i);
           }
         }
       }
       // every load issued has landed before the CTA exits (bounded waits)
-      for (int j = 1; j <= kNpNA && j <= ka; j++) {
+      for (int j = 1; j <= kNpNS && j <= ka; j++) {
         const int kk = ka - j;
-        mbar_wait(afull + kk % kNpNA, (kk / kNpNA) & 1, A.err, kErrNp);
+        mbar_wait(sfull + kk % kNpNS, (kk / kNpNS) & 1, A.err, kErrNp);
       }
     }
   } else if (warp == 1) {
@@ -674,26 +677,26 @@ __global__ void __launch_bounds__(kNpThreads, 1) k_tc_near_pipe(TcNearPipeArgs A
       }
     }
   } else if (warp == 2) {
-    // ---- MMA issue (one thread): per weight stage, both tiles x 2 K-steps x 3 split products ----
+    // ---- MMA issue (one thread): D[128 target reals][256 leaves of the pair] +=
+    // weights (A, M = 128) x data (B, N = 256): both tiles in one instruction, so
+    // each weight stage is 2 K-steps x 3 split products ----
     if (lane == 0) {
-      const uint32_t idesc = idesc_f16_f32(128, 128), sbase = smem_u32(sm);
+      const uint32_t idesc = idesc_f16_f32(128, 2 * 128), sbase = smem_u32(sm);
       int ka = 0, kb = 0, it = 0;
       bool ok = true;
       for (int w = first; w < A.nitems && ok; w = next_item(w), it++) {
-        int rhs, ty0, tx0, ntile;
-        geom(w, rhs, ty0, tx0, ntile);
         const int set = it & 1;
+        const uint32_t d = tmem + (uint32_t)(set * 256);
         ok = mbar_wait_or(tfree + set, ((it >> 1) & 1) ^ 1, abort, A.err, kErrNp);
         for (int a = 0; a < na && ok; a++, ka++) {
-          const int i = ka % kNpNA;
-          ok = mbar_wait_or(aconv + i, (ka / kNpNA) & 1, abort, A.err, kErrNp);
+          const int i = ka % kNpNO;
+          ok = mbar_wait_or(ofull + i, (ka / kNpNO) & 1, abort, A.err, kErrNp);
           int idx;
           const int kind = np_stage(a, A.nl2p, idx);
-          const uint32_t abase = sbase + NpSmem::a + i * kNpABuf;
-          const uint64_t ah0 = kind == 0 ? smem_desc(abase, kHC * 16, kNpKC * kHC * 16)
-                                         : smem_desc(abase, kTX * 16, kNpKC * kTX * 16);
-          const uint64_t al0 = kind == 0 ? smem_desc(abase + kNpHaloSplit, kHC * 16, kNpKC * kHC * 16)
-                                         : smem_desc(abase + kNpL2pSplit, kTX * 16, kNpKC * kTX * 16);
+          const uint32_t obase = sbase + NpSmem::o + i * kNpBuf;
+          const uint32_t lbo = kind == 0 ? kHC * 16 : kTX * 16;  // K-adjacent core matrices
+          const uint64_t dh0 = smem_desc(obase, lbo, kNpKC * lbo);
+          const uint64_t dl0 = smem_desc(obase + (kind == 0 ? kNpHaloSplit : kNpL2pSplit), lbo, kNpKC * lbo);
           const int nq = kind == 0 ? 9 : 1;
           for (int q = 0; q < nq && ok; q++, kb++) {
             const int b = kb % kNpNB;
@@ -701,24 +704,20 @@ __global__ void __launch_bounds__(kNpThreads, 1) k_tc_near_pipe(TcNearPipeArgs A
             tc_fence_after();
             if (!ok) break;
             const uint32_t bb = sbase + NpSmem::b + b * kStageBytes;
-            const uint64_t bh0 = smem_desc(bb, 128, 512), bl0 = smem_desc(bb + kStageHalf, 128, 512);
-            const int dr = q / 3 - 1, dc = q % 3 - 1;
+            const uint64_t wh0 = smem_desc(bb, 128, 512), wl0 = smem_desc(bb + kStageHalf, 128, 512);
+            // neighbour slot q: the pair's 32 leaf rows start at halo row 1 + dr, column 1 + dc
+            const uint32_t doff0 = kind == 0 ? (uint32_t)((q / 3) * (kNpKC * kHC * 16) + (q % 3) * 16) : 0u;
 #pragma unroll
             for (int ks = 0; ks < 2; ks++) {
-              for (int u = 0; u < ntile; u++) {
-                const uint32_t aoff =
-                    kind == 0 ? (uint32_t)((u * kTY + 1 + dr) * (kNpKC * kHC * 16) + (1 + dc) * 16 + ks * 2 * (kHC * 16))
-                              : (uint32_t)(u * kTY * (kNpKC * kTX * 16) + ks * 2 * (kTX * 16));
-                const uint32_t d = tmem + (uint32_t)(set * 256 + u * 128);
-                const int acc = (a | q | ks) ? 1 : 0;
-                mma_f16(d, desc_add(ah0, aoff), desc_add(bh0, ks * 256), idesc, acc);
-                mma_f16(d, desc_add(ah0, aoff), desc_add(bl0, ks * 256), idesc, 1);
-                mma_f16(d, desc_add(al0, aoff), desc_add(bh0, ks * 256), idesc, 1);
-              }
+              const uint32_t doff = doff0 + (uint32_t)ks * 2 * lbo;
+              const int acc = (a | q | ks) ? 1 : 0;
+              mma_f16(d, desc_add(wh0, ks * 256), desc_add(dh0, doff), idesc, acc);
+              mma_f16(d, desc_add(wh0, ks * 256), desc_add(dl0, doff), idesc, 1);
+              mma_f16(d, desc_add(wl0, ks * 256), desc_add(dh0, doff), idesc, 1);
             }
             mma_commit(bempty + b);
           }
-          if (ok) mma_commit(afree + i);
+          if (ok) mma_commit(ofree + i);
         }
         if (ok) mma_commit(tfull + set);
       }
@@ -727,7 +726,9 @@ __global__ void __launch_bounds__(kNpThreads, 1) k_tc_near_pipe(TcNearPipeArgs A
       mbar_wait(mdone, 0, A.err, kErrNp);
     }
   } else if (warp < kNpEpiWarp0) {
-    // ---- converters: the landed FP32 A-stage becomes FP16 hi/lo in place ----
+    // ---- converters: a staged FP32 A-stage becomes the FP16 hi/lo operand.  One
+    // unit is a 4-complex chunk (32 bytes) of one leaf: staging [row][col][32 reals]
+    // to operand [row][chunk][col][16 bytes], hi then lo ----
     const int ct = threadIdx.x - 32 * kNpConvWarp0;
     int ka = 0;
     for (int w = first; w < A.nitems; w = next_item(w)) {
@@ -736,24 +737,23 @@ __global__ void __launch_bounds__(kNpThreads, 1) k_tc_near_pipe(TcNearPipeArgs A
       float s1, s2, p;
       np_scales(A, rhs, s1, s2, p);
       const float2 *gr = A.g ? A.g + rhs * A.gstride : nullptr;
-      bool ok = true;
       for (int a = 0; a < na; a++, ka++) {
-        const int i = ka % kNpNA;
-        ok = mbar_wait_or(afull + i, (ka / kNpNA) & 1, abort, A.err, kErrNp);
-        char *hi = sm + NpSmem::a + i * kNpABuf;
+        const int i = ka % kNpNS, o = ka % kNpNO;
+        const bool ok = mbar_wait_or(sfull + i, (ka / kNpNS) & 1, abort, A.err, kErrNp) &&
+                        mbar_wait_or(ofree + o, ((ka / kNpNO) & 1) ^ 1, abort, A.err, kErrNp);
+        const float4 *st = (const float4 *)(sm + NpSmem::s + i * kNpBuf);
+        char *hi = sm + NpSmem::o + o * kNpBuf;
         int idx;
         if (np_stage(a, A.nl2p, idx) == 0) {
           char *lo = hi + kNpHaloSplit;
-          // (halo row, chunk, halo column): off = ((hr * 4 + c) * 10 + hc) * 16
-          for (int e = ct; e < kHR * kNpKC * kHC && ok; e += kNpConv) {
-            const int hc = e % kHC, c = (e / kHC) % kNpKC, hr = e / (kHC * kNpKC);
-            float4 *ph = (float4 *)(hi + e * 16), *pl = (float4 *)(lo + e * 16);
-            const float4 a0 = *ph, a1 = *pl;
+          for (int e = ct; e < kHR * kHC * kNpKC && ok; e += kNpConv) {
+            const int c = e & 3, hc = (e >> 2) % kHC, hr = (e >> 2) / kHC;
+            const float4 a0 = st[2 * e], a1 = st[2 * e + 1];  // staging offset ((hr * 10 + hc) * 32 + 8 c) reals
             float4 g0 = make_float4(0.f, 0.f, 0.f, 0.f), g1 = g0;
             if (A.mode == IN_G) {
               const int ly = ty0 - 1 + hr, lx = tx0 - 1 + hc;
               if (ly >= 0 && ly < A.nleaf && lx >= 0 && lx < A.nleaf) {
-                const size_t gi = (size_t)(ly * A.nleaf + lx) * kBB + 4 * (kNpKC * idx + c);
+                const size_t gi = (size_t)(ly * A.nleaf + lx) * kBB + 16 * idx + 4 * c;
                 g0 = *(const float4 *)(gr + gi);
                 g1 = *(const float4 *)(gr + gi + 2);
               }
@@ -767,32 +767,43 @@ __global__ void __launch_bounds__(kNpThreads, 1) k_tc_near_pipe(TcNearPipeArgs A
             split2u(v1.x * s1, v1.y * s1, h[1], l[1]);
             split2u(v2.x * s1, v2.y * s1, h[2], l[2]);
             split2u(v3.x * s1, v3.y * s1, h[3], l[3]);
-            st_shared_v4(ph, h);
-            st_shared_v4(pl, l);
+            const int off = ((hr * kNpKC + c) * kHC + hc) * 16;
+            st_shared_v4(hi + off, h);
+            st_shared_v4(lo + off, l);
           }
         } else {
           char *lo = hi + kNpL2pSplit;
-          for (int e = ct; e < kPair * kTY * kNpKC * kTX && ok; e += kNpConv) {
-            float4 *ph = (float4 *)(hi + e * 16), *pl = (float4 *)(lo + e * 16);
-            const float4 a0 = *ph, a1 = *pl;
+          for (int e = ct; e < kPair * kTY * kTX * kNpKC && ok; e += kNpConv) {
+            const int c = e & 3, col = (e >> 2) & (kTX - 1), row = e >> 5;
+            const float4 a0 = st[2 * e], a1 = st[2 * e + 1];  // staging offset ((row * 8 + col) * 32 + 8 c) reals
             uint32_t h[4], l[4];
             split2u(a0.x * s2, a0.y * s2, h[0], l[0]);
             split2u(a0.z * s2, a0.w * s2, h[1], l[1]);
             split2u(a1.x * s2, a1.y * s2, h[2], l[2]);
             split2u(a1.z * s2, a1.w * s2, h[3], l[3]);
-            st_shared_v4(ph, h);
-            st_shared_v4(pl, l);
+            const int off = ((row * kNpKC + c) * kTX + col) * 16;
+            st_shared_v4(hi + off, h);
+            st_shared_v4(lo + off, l);
           }
         }
         fence_proxy_async();
         named_sync(1, kNpConv);
-        if (ct == 0) mbar_arrive(aconv + i);
+        if (ct == 0) {
+          mbar_arrive(sfree + i);
+          mbar_arrive(ofull + o);
+        }
       }
     }
   } else {
-    // ---- epilogue: lane = leaf, 16-column chunks (8 pixels) straight to y ----
+    // ---- epilogue: TMEM lane = target real (pixel 16 qd + lane / 2, real part on
+    // even lanes), column = leaf of the pair; the warp's 32 lanes are 128 contiguous
+    // bytes of one leaf's output, so every load and store is one coalesced row.
+    // Warps 7..10 take the pair's first tile (columns 0..127), 11..14 the second ----
     const int ew = warp - kNpEpiWarp0, qd = warp & 3, hh = ew >> 2;
+    const bool odd = lane & 1;
     const bool need_x = A.epi == EPI_FWD || A.epi == EPI_ADJ || A.red == RED_TS;
+    const float *xf = (const float *)A.xe, *af = (const float *)A.dot_a;
+    float *yf = (float *)A.y;
     int it = 0;
     for (int w = first; w < A.nitems; w = next_item(w), it++) {
       int rhs, ty0, tx0, ntile;
@@ -804,54 +815,49 @@ __global__ void __launch_bounds__(kNpThreads, 1) k_tc_near_pipe(TcNearPipeArgs A
       const bool ok = mbar_wait_or(tfull + set, (it >> 1) & 1, abort, A.err, kErrNp);
       tc_fence_after();
       const size_t rbase = (size_t)rhs * A.U;
-      const float2 *gr = A.g ? A.g + rhs * A.gstride : nullptr;
+      const float *gf = A.g ? (const float *)(A.g + rhs * A.gstride) : nullptr;
+      const float *xr = xf + 2 * rbase, *ar = af + 2 * rbase;
+      float *yr = yf + 2 * rbase;
       double r0 = 0, r1 = 0, r2 = 0;
-      const int m = 32 * qd + lane;
-      for (int u = 0; u < ntile; u++) {
-        const int ly = ty0 + u * kTY + m / kTX, lx = tx0 + m % kTX;
-        const bool live = ok && ly < A.nleaf && lx < A.nleaf;
-        const size_t lb = rbase + (size_t)(ly * A.nleaf + lx) * kBB;
+      if (hh < ntile) {  // warp-uniform
 #pragma unroll 1
-        for (int ch = 0; ch < 4; ch++) {
-          const int col = 64 * hh + 16 * ch;
-          float d[16];
-          tmem_ld16(tmem + ((uint32_t)(32 * qd) << 16) + (uint32_t)(set * 256 + u * 128 + col), d);
-          if (!live) continue;
-          const size_t i0 = lb + col / 2;
-          float4 xv[4], av[4], gv[4];
+        for (int ch = 0; ch < 8; ch++) {
+          float d[16], xv[16], av[16], gv[16];
+          tmem_ld16(tmem + ((uint32_t)(32 * qd) << 16) + (uint32_t)(set * 256 + 128 * hh + 16 * ch), d);
+          int fi[16];  // float offset within the RHS: 2 (leaf * 64 + pixel) + component
+          bool live[16];
 #pragma unroll
-          for (int k = 0; k < 4; k++) {
-            xv[k] = need_x ? *(const float4 *)(A.xe + i0 + 2 * k) : make_float4(0.f, 0.f, 0.f, 0.f);
-            av[k] = A.red == RED_DOT ? *(const float4 *)(A.dot_a + i0 + 2 * k) : make_float4(0.f, 0.f, 0.f, 0.f);
-            gv[k] = A.epi == EPI_ADJ ? *(const float4 *)(gr + (i0 - rbase) + 2 * k) : make_float4(0.f, 0.f, 0.f, 0.f);
+          for (int j = 0; j < 16; j++) {  // loads first: one round trip per chunk
+            const int n = 16 * ch + j, ly = ty0 + hh * kTY + n / kTX, lx = tx0 + n % kTX;
+            live[j] = ok && ly < A.nleaf && lx < A.nleaf;
+            fi[j] = 2 * (ly * A.nleaf + lx) * kBB + 32 * qd + lane;
+            xv[j] = (need_x && live[j]) ? xr[fi[j]] : 0.f;
+            av[j] = (A.red == RED_DOT && live[j]) ? ar[fi[j]] : 0.f;
+            gv[j] = (A.epi == EPI_ADJ && live[j]) ? gf[fi[j]] : 0.f;
           }
 #pragma unroll
-          for (int k = 0; k < 4; k++) {
-            float2 o[2] = {make_float2(d[4 * k] * inv, d[4 * k + 1] * inv),
-                           make_float2(d[4 * k + 2] * inv, d[4 * k + 3] * inv)};
-            const float2 xin[2] = {make_float2(xv[k].x, xv[k].y), make_float2(xv[k].z, xv[k].w)};
+          for (int j = 0; j < 16; j++) {
+            if (!live[j]) continue;  // warp-uniform
+            const float o = d[j] * inv;
+            float v = o;
             if (A.epi == EPI_FWD) {
-              o[0] = csub(xin[0], o[0]);
-              o[1] = csub(xin[1], o[1]);
-            } else if (A.epi == EPI_ADJ) {
-              o[0] = csub(xin[0], cconj(cmul(make_float2(gv[k].x, gv[k].y), o[0])));
-              o[1] = csub(xin[1], cconj(cmul(make_float2(gv[k].z, gv[k].w), o[1])));
+              v = xv[j] - o;
+            } else if (A.epi == EPI_ADJ) {  // x - conj(g o)
+              const float op = __shfl_xor_sync(0xffffffffu, o, 1), gp = __shfl_xor_sync(0xffffffffu, gv[j], 1);
+              v = odd ? xv[j] + (gp * o + gv[j] * op) : xv[j] - (gv[j] * o - gp * op);
             } else if (A.epi == EPI_CONJ) {
-              o[0] = cconj(o[0]);
-              o[1] = cconj(o[1]);
+              v = odd ? -o : o;
             }
-            *(float4 *)(A.y + i0 + 2 * k) = make_float4(o[0].x, o[0].y, o[1].x, o[1].y);
-            if (A.red == RED_DOT) {
-              const float2 a0 = make_float2(av[k].x, av[k].y), a1 = make_float2(av[k].z, av[k].w);
-              r0 += (double)a0.x * o[0].x + (double)a0.y * o[0].y + (double)a1.x * o[1].x + (double)a1.y * o[1].y;
-              r1 += (double)a0.x * o[0].y - (double)a0.y * o[0].x + (double)a1.x * o[1].y - (double)a1.y * o[1].x;
-            } else if (A.red == RED_TS) {
-#pragma unroll
-              for (int e2 = 0; e2 < 2; e2++) {
-                r0 += (double)o[e2].x * xin[e2].x + (double)o[e2].y * xin[e2].y;
-                r1 += (double)o[e2].x * xin[e2].y - (double)o[e2].y * xin[e2].x;
-                r2 += (double)o[e2].x * o[e2].x + (double)o[e2].y * o[e2].y;
-              }
+            yr[fi[j]] = v;
+            if (A.red == RED_DOT) {  // conj(a) y
+              const float vp = __shfl_xor_sync(0xffffffffu, v, 1);
+              r0 += (double)av[j] * v;
+              r1 += (odd ? -1.0 : 1.0) * (double)av[j] * vp;
+            } else if (A.red == RED_TS) {  // conj(y) x and |y|^2
+              const float xp = __shfl_xor_sync(0xffffffffu, xv[j], 1);
+              r0 += (double)v * xv[j];
+              r1 += (odd ? -1.0 : 1.0) * (double)v * xp;
+              r2 += (double)v * v;
             }
           }
         }
@@ -1522,24 +1528,24 @@ static bool tc_near_pipe(isg_ctx *c, const NearArgs &N, cudaStream_t st, isg_sta
   A.ppr = A.tiles_x * ((A.tiles_y + kPair - 1) / kPair);
   A.nitems = A.ppr * N.in.nrhs;
   A.err = T.err;
-  // tmh: the input as [RHS][leaf row][4-pixel chunk][leaf column][8 floats], a box is
-  // one halo K-group (4 chunks) of the pair's 34 x 10 halo; tml: the leaf locals as
-  // [RHS][leaf row][4-sample chunk][leaf column][8 floats], a box is one L2P stage
+  // tmh: the input as [RHS][leaf row][leaf column][128 reals], a box is one halo
+  // K-group (32 reals) of the pair's 34 x 10 halo; tml: the leaf locals as
+  // [RHS][leaf row][leaf column][2 ns reals], a box is one L2P stage of the pair
   CUtensorMap tmh, tml;
   memset(&tmh, 0, sizeof(tmh));
   memset(&tml, 0, sizeof(tml));
-  const cuuint32_t one[5] = {1, 1, 1, 1, 1};
-  const cuuint64_t hd[5] = {8, (cuuint64_t)P.nleaf, 16, (cuuint64_t)P.nleaf, (cuuint64_t)N.in.nrhs};
-  const cuuint64_t hs[4] = {(cuuint64_t)kBB * 8, 32, (cuuint64_t)P.nleaf * kBB * 8, (cuuint64_t)P.U * 8};
-  const cuuint32_t hb[5] = {4, (cuuint32_t)kHC, (cuuint32_t)kNpKC, (cuuint32_t)kHR, 1};
-  const cuuint64_t ld[5] = {8, (cuuint64_t)P.nleaf, (cuuint64_t)(P.ns_leaf / 4), (cuuint64_t)P.nleaf,
+  const cuuint32_t one[4] = {1, 1, 1, 1};
+  const cuuint64_t hd[4] = {2 * kBB, (cuuint64_t)P.nleaf, (cuuint64_t)P.nleaf, (cuuint64_t)N.in.nrhs};
+  const cuuint64_t hs[3] = {(cuuint64_t)kBB * 8, (cuuint64_t)P.nleaf * kBB * 8, (cuuint64_t)P.U * 8};
+  const cuuint32_t hb[4] = {32, (cuuint32_t)kHC, (cuuint32_t)kHR, 1};
+  const cuuint64_t ld[4] = {(cuuint64_t)(2 * P.ns_leaf), (cuuint64_t)P.nleaf, (cuuint64_t)P.nleaf,
                             (cuuint64_t)N.in.nrhs};
-  const cuuint64_t ls[4] = {(cuuint64_t)P.ns_leaf * 8, 32, (cuuint64_t)P.nleaf * P.ns_leaf * 8, (cuuint64_t)P.mp * 8};
-  const cuuint32_t lb[5] = {4, (cuuint32_t)kTX, (cuuint32_t)kNpKC, (cuuint32_t)(kPair * kTY), 1};
-  if (encode(&tmh, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, (void *)A.x, hd, hs, hb, one, CU_TENSOR_MAP_INTERLEAVE_NONE,
+  const cuuint64_t ls[3] = {(cuuint64_t)P.ns_leaf * 8, (cuuint64_t)P.nleaf * P.ns_leaf * 8, (cuuint64_t)P.mp * 8};
+  const cuuint32_t lb[4] = {32, (cuuint32_t)kTX, (cuuint32_t)(kPair * kTY), 1};
+  if (encode(&tmh, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, (void *)A.x, hd, hs, hb, one, CU_TENSOR_MAP_INTERLEAVE_NONE,
              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS ||
-      encode(&tml, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, (void *)loc_leaf, ld, ls, lb, one,
+      encode(&tml, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, (void *)loc_leaf, ld, ls, lb, one,
              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return false;

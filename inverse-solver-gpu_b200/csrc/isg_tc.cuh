@@ -85,6 +85,17 @@ __device__ __forceinline__ void tma_load_5d(void *dst, const void *tmap, int c0,
       : "memory");
 }
 
+// Tiled 4-D tensor load global -> shared (no multicast); c0 (innermost) must
+// address a 16-byte boundary.  Coordinates outside the tensor read as zero.
+__device__ __forceinline__ void tma_load_4d(void *dst, const void *tmap, int c0, int c1, int c2, int c3,
+                                            uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+      "[%6];\n" ::"r"(smem_u32(dst)),
+      "l"(tmap), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+      : "memory");
+}
+
 // Bulk prefetch of a contiguous global range into L2 (16-byte aligned, size a
 // multiple of 16).
 __device__ __forceinline__ void bulk_prefetch_l2(const void *src, uint32_t bytes) {
