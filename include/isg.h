@@ -102,8 +102,11 @@ typedef struct isg_solve_info {
  *      + setup_bicgs (bicgs_gpu.cu:89-113) ---- */
 void isg_default_opts(isg_opts *o);
 void isg_default_solve_opts(isg_solve_opts *o);
-/* Builds the host tables (tree, near/far lists, near-field block, translation,
- * interpolation, shift and receiver tables).  Touches no GPU. */
+/* Builds the host tables (tree, plane-wave, interpolation, shift and receiver
+ * tables).  Touches no GPU.  The near-field blocks and translation operators
+ * (setup_mlfma.cpp:492-543, the tables that evaluate Bessel functions) are
+ * computed on the device by isg_setup_gpu, or on the host if isg_host_table
+ * asks for them first. */
 isg_status isg_create(const isg_opts *opts, isg_ctx **out);
 /* Uploads the tables and allocates the device workspaces for max_rhs RHS. */
 isg_status isg_setup_gpu(isg_ctx *ctx);
@@ -150,6 +153,20 @@ isg_status isg_aggregate(isg_ctx *ctx, const void *x, void *rx, int nrhs, int or
 /* x[U] = back-projection of rx (aggregateh, matvec_gpu.cu:369-470;
  * solve.cpp:356-456), all levels on the device. */
 isg_status isg_aggregateh(isg_ctx *ctx, void *x, const void *rx, int nrhs, int order, isg_stream stream);
+
+/* ---- near-field receivers (the reference's commented dense form, setup_born.cpp:52-60) ----
+ * numrx receivers at radius * (cos 2 pi m / numrx, sin 2 pi m / numrx) wavelengths (the
+ * directions of mom.cpp:149-154 at a finite radius, outside the domain).  Builds on the device
+ * the dense operator go[m][n] = integrate(rx_m, pos_n) (integrate.cpp:15-41) as FP16 hi/lo
+ * tables for tcgen05 GEMMs (8 bytes per receiver and pixel, twice: forward and adjoint order);
+ * radius 0 removes it.  While it is set, isg_measure and isg_dbim use it in place of the
+ * far-field aggregate / aggregateh. */
+isg_status isg_set_nearfield_receivers(isg_ctx *ctx, double radius);
+/* rx[numrx] = go x per RHS (the near-field form of aggregate; the far-field aggregate when no
+ * near-field receivers are set). */
+isg_status isg_receive(isg_ctx *ctx, const void *x, void *rx, int nrhs, int order, isg_stream stream);
+/* x[U] = gh rx per RHS, gh = conj(go)^T (setup_born.cpp:57-59; aggregateh when none are set). */
+isg_status isg_receiveh(isg_ctx *ctx, void *x, const void *rx, int nrhs, int order, isg_stream stream);
 
 /* Size of the device array isg_aggregate_noalloc works in (one per device). */
 #define ISG_STATIC_SCRATCH_BYTES (64u << 20)

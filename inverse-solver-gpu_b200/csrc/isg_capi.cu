@@ -50,6 +50,14 @@ isg_status run_aggregateh(isg_ctx *c, float2 *xb, const float2 *rx, int nrhs, cu
   return cuda_check(c, cudaGetLastError(), "aggregateh");
 }
 
+isg_status run_receive(isg_ctx *c, const float2 *xb, float2 *rx, int nrhs, cudaStream_t st) {
+  return rxnear_active(c) ? rxnear_apply(c, xb, rx, nrhs, 0, st) : run_aggregate(c, xb, rx, nrhs, st);
+}
+
+isg_status run_receiveh(isg_ctx *c, float2 *xb, const float2 *rx, int nrhs, cudaStream_t st) {
+  return rxnear_active(c) ? rxnear_apply(c, rx, xb, nrhs, 1, st) : run_aggregateh(c, xb, rx, nrhs, st);
+}
+
 }  // namespace isg
 
 namespace {
@@ -395,6 +403,7 @@ void isg_destroy(isg_ctx *c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->graph_exec) cudaGraphExecDestroy((cudaGraphExec_t)c->graph_exec);
     fno_destroy(c);
+    rxnear_destroy(c);
     band_destroy(c);
     tc_destroy(c);
     for (void *p : c->dev_allocs) cudaFree(p);
@@ -552,6 +561,35 @@ isg_status isg_aggregateh(isg_ctx *c, void *x, const void *rx, int nrhs, int ord
   if ((e = run_aggregateh(c, y, (const float2 *)rx, nrhs, st)) != ISG_OK) return e;
   from_blocked(c, y, x, nrhs, order, st);
   return cuda_check(c, cudaGetLastError(), "aggregateh");
+}
+
+isg_status isg_set_nearfield_receivers(isg_ctx *c, double radius) {
+  isg_status e = need_gpu(c);
+  if (e != ISG_OK) return e;
+  if (!(radius >= 0)) {
+    c->err = "receiver radius must be >= 0";
+    return ISG_BAD_ARG;
+  }
+  return rxnear_setup(c, radius);
+}
+
+isg_status isg_receive(isg_ctx *c, const void *x, void *rx, int nrhs, int order, isg_stream stream) {
+  isg_status e = need_gpu(c);
+  if (e != ISG_OK) return e;
+  if (!x || !rx || bad_order(order) || (e = check_batch(c, nrhs)) != ISG_OK) return ISG_BAD_ARG;
+  cudaStream_t st = pick(c, stream);
+  return run_receive(c, to_blocked(c, x, c->wx, nrhs, order, st), (float2 *)rx, nrhs, st);
+}
+
+isg_status isg_receiveh(isg_ctx *c, void *x, const void *rx, int nrhs, int order, isg_stream stream) {
+  isg_status e = need_gpu(c);
+  if (e != ISG_OK) return e;
+  if (!x || !rx || bad_order(order) || (e = check_batch(c, nrhs)) != ISG_OK) return ISG_BAD_ARG;
+  cudaStream_t st = pick(c, stream);
+  float2 *y = order == ISG_ORDER_BLOCKED ? (float2 *)x : c->wy;
+  if ((e = run_receiveh(c, y, (const float2 *)rx, nrhs, st)) != ISG_OK) return e;
+  from_blocked(c, y, x, nrhs, order, st);
+  return cuda_check(c, cudaGetLastError(), "receiveh");
 }
 
 int64_t isg_kernel_launches(void) { return launch_count(); }

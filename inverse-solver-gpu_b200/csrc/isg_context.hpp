@@ -25,6 +25,7 @@ struct RhsState {
 struct TcPlan;    // tensor-core leaf stage tables (isg_tc.cu)
 struct FnoModel;  // learned warm start (isg_fno.cu)
 struct BandPlan;  // tensor-core M2M tables (isg_tc_band.cu)
+struct RxPlan;    // near-field receiver tables (isg_rxnear.cu)
 
 }  // namespace isg
 
@@ -55,6 +56,7 @@ struct isg_ctx {
   isg::TcPlan *tc = nullptr;
   isg::BandPlan *band = nullptr;
   isg::FnoModel *fno = nullptr;
+  isg::RxPlan *rx = nullptr;  // near-field receivers, when set
   // device address of isg_aggregate_noalloc's static array, resolved by isg_setup_gpu
   float2 *static_scratch = nullptr;
   // BiCGSTAB iteration block captured as a CUDA graph, and what it was captured for
@@ -86,6 +88,15 @@ isg_status cuda_check(isg_ctx *c, cudaError_t e, const char *what);
 isg_status run_aggregate(isg_ctx *c, const float2 *xb, float2 *rx, int nrhs, cudaStream_t st);
 isg_status run_aggregateh(isg_ctx *c, float2 *xb, const float2 *rx, int nrhs, cudaStream_t st);
 const int *order_perm(const isg_ctx *c, int order);
+// The receiver operators of the inversion loop: near-field receivers (dense
+// GEMMs, isg_rxnear.cu) when set, else the far-field aggregate / aggregateh.
+isg_status run_receive(isg_ctx *c, const float2 *xb, float2 *rx, int nrhs, cudaStream_t st);
+isg_status run_receiveh(isg_ctx *c, float2 *xb, const float2 *rx, int nrhs, cudaStream_t st);
+isg_status rxnear_setup(isg_ctx *c, double radius);
+void rxnear_destroy(isg_ctx *c);
+bool rxnear_active(const isg_ctx *c);
+isg_status rxnear_apply(isg_ctx *c, const float2 *in, float2 *out, int nrhs, int adjoint, cudaStream_t st);
+int rxnear_error(isg_ctx *c);
 // Tensor-core engine (isg_tc.cu).
 isg_status tc_setup(isg_ctx *c);
 void tc_destroy(isg_ctx *c);

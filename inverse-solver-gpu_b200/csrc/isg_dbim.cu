@@ -203,7 +203,7 @@ struct Dbim {
   }
   // far-field samples of X for transmitters [k R, k R + n), to the host
   isg_status far_field(const float2 *Xs, int k, int n, std::vector<zd> &out) {
-    isg_status e = run_aggregate(c, Xs, rxd, n, st);
+    isg_status e = run_receive(c, Xs, rxd, n, st);
     if (e != ISG_OK) return e;
     std::vector<float2> h((size_t)n * nrx);
     cudaMemcpyAsync(h.data(), rxd, h.size() * sizeof(float2), cudaMemcpyDeviceToHost, st);
@@ -230,7 +230,7 @@ struct Dbim {
         hm[q] = make_float2((float)v.real(), (float)v.imag());
       }
       cudaMemcpyAsync(rxd, hm.data(), (size_t)n * nrx * sizeof(float2), cudaMemcpyHostToDevice, st);
-      if ((e = run_aggregateh(c, Y, rxd, n, st)) != ISG_OK) return e;
+      if ((e = run_receiveh(c, Y, rxd, n, st)) != ISG_OK) return e;
       k_conj_g_mul<<<vgrid(n), 256, 0, st>>>(g, Y, C, U);
       count_launch();
       float2 *xa = warm ? adj + (size_t)k * R * U : X;  // the previous adjoint fields, when kept

@@ -104,6 +104,9 @@ SIGNATURES = {
     "isg_aggregate": (_I, [_P, _P, _P, _I, _I, _P]),
     "isg_aggregateh": (_I, [_P, _P, _P, _I, _I, _P]),
     "isg_aggregate_noalloc": (_I, [_P, _P, _P, _I, _I, _P]),
+    "isg_set_nearfield_receivers": (_I, [_P, _D]),
+    "isg_receive": (_I, [_P, _P, _P, _I, _I, _P]),
+    "isg_receiveh": (_I, [_P, _P, _P, _I, _I, _P]),
     "isg_default_dbim_opts": (None, [ctypes.POINTER(DbimOpts)]),
     "isg_measure": (_I, [_P, _I, _P, _P, _I, _D, ctypes.c_uint64, ctypes.POINTER(SolveOpts), _P, _P]),
     "isg_dbim": (_I, [_P, _I, _P, _P, _P, _P, _I, ctypes.POINTER(DbimOpts), ctypes.POINTER(DbimRecord), _P]),
@@ -292,6 +295,31 @@ class Solver:
             x = torch.empty((R, self.numunk) if rx.dim() == 2 else (self.numunk,), dtype=torch.complex64,
                             device=rx.device)
         self._check(lib().isg_aggregateh(self._h, _ptr(x), _ptr(rx), R, order, _stream(stream)), "aggregateh")
+        return x
+
+    # ---- near-field receivers ----
+    def set_nearfield_receivers(self, radius: float):
+        """numrx receivers on a circle of this radius (wavelengths); 0 returns to far field."""
+        self._check(lib().isg_set_nearfield_receivers(self._h, radius), "set_nearfield_receivers")
+
+    def receive(self, x, rx=None, order: int = ORDER_TREE, stream=None):
+        """Receiver samples go x (near-field receivers) or the far-field aggregate."""
+        import torch
+        R = self._nrhs(x)
+        if rx is None:
+            rx = torch.empty((R, self.numrx) if x.dim() == 2 else (self.numrx,), dtype=torch.complex64,
+                             device=x.device)
+        self._check(lib().isg_receive(self._h, _ptr(x), _ptr(rx), R, order, _stream(stream)), "receive")
+        return rx
+
+    def receiveh(self, rx, x=None, order: int = ORDER_TREE, stream=None):
+        """Back-projection conj(go)^T rx (near-field receivers) or the far-field aggregateh."""
+        import torch
+        R = 1 if rx.dim() == 1 else rx.shape[0]
+        if x is None:
+            x = torch.empty((R, self.numunk) if rx.dim() == 2 else (self.numunk,), dtype=torch.complex64,
+                            device=rx.device)
+        self._check(lib().isg_receiveh(self._h, _ptr(x), _ptr(rx), R, order, _stream(stream)), "receiveh")
         return x
 
     # ---- launch-shape autotuner ----

@@ -42,6 +42,7 @@ struct orc_ctx {
   int *antindh; /* [ns_0][2 ninter] */
   double complex **mul, **loc;
   double complex *buf;
+  double complex *go; /* near-field receivers: [numrx][U] integrate(rx_m, pos_n), or NULL */
 };
 
 /* integrate.cpp:7-9 */
@@ -396,6 +397,7 @@ orc_ctx *orc_create(int level, double k0, double res, int box, int beta, int nin
 
 void orc_destroy(orc_ctx *c) {
   if (!c) return;
+  free(c->go);
   for (int i = 0; i < c->L; i++) {
     free(c->cen[i]);
     free(c->par[i]);
@@ -711,6 +713,45 @@ void orc_aggregateh(orc_ctx *c, double complex *x, const double complex *rx) {
   l2p(c, x);
 }
 
+/* Near-field receivers (the reference's commented dense form, setup_born.cpp:52-60):
+ * numrx points at radius (cos, sin)(360 / numrx m degrees) (mom.cpp:149-154 at a
+ * finite radius), go[m][n] = integrate(rx_m, pos_n).  radius 0 removes them. */
+void orc_set_nearfield(orc_ctx *c, double radius) {
+  free(c->go);
+  c->go = NULL;
+  if (radius == 0) return;
+  c->go = malloc((size_t)c->numrx * c->U * sizeof(double complex));
+  for (int m = 0; m < c->numrx; m++) {
+    double ang = 360.0 / c->numrx * m;
+    double complex r = radius * (cos(ang / 360 * 2 * M_PI) + I * sin(ang / 360 * 2 * M_PI));
+    for (int n = 0; n < c->U; n++) c->go[(size_t)m * c->U + n] = orc_integrate(c, r, c->pos[n]);
+  }
+}
+
+/* rx = go x with near-field receivers, else the far-field aggregate. */
+void orc_receive(orc_ctx *c, const double complex *x, double complex *rx) {
+  if (!c->go) {
+    orc_aggregate(c, x, rx);
+    return;
+  }
+  for (int m = 0; m < c->numrx; m++) {
+    double complex s = 0;
+    for (int n = 0; n < c->U; n++) s += c->go[(size_t)m * c->U + n] * x[n];
+    rx[m] = s;
+  }
+}
+
+/* x = gh rx, gh = conj(go)^T (setup_born.cpp:57-59), else the far-field aggregateh. */
+void orc_receiveh(orc_ctx *c, double complex *x, const double complex *rx) {
+  if (!c->go) {
+    orc_aggregateh(c, x, rx);
+    return;
+  }
+  for (int n = 0; n < c->U; n++) x[n] = 0;
+  for (int m = 0; m < c->numrx; m++)
+    for (int n = 0; n < c->U; n++) x[n] += conj(c->go[(size_t)m * c->U + n]) * rx[m];
+}
+
 /* One write_error record (setup_born.cpp:171-242). */
 static void dbim_record(const orc_ctx *c, int ntx, const double complex *mesd, const double complex *od,
                         const double complex *o, const double complex *otrue, double regular, double mesnorm,
@@ -742,7 +783,7 @@ static void dbim_gradient(orc_ctx *c, int ntx, const double complex *o, const do
   double complex *g = malloc(U * sizeof(double complex)), *x = malloc(U * sizeof(double complex));
   for (int n = 0; n < U; n++) od[n] = 0;
   for (int i = 0; i < ntx; i++) {
-    orc_aggregateh(c, y, &mesd[i * c->numrx]);
+    orc_receiveh(c, y, &mesd[i * c->numrx]);
     for (int n = 0; n < U; n++) {
       cc[n] = conj(o[n] * k2) * y[n];
       g[n] = o[n] * k2;
@@ -779,7 +820,7 @@ int orc_dbim(orc_ctx *c, int ntx, const double complex *inc, const double comple
     for (int n = 0; n < U; n++) x[n] = 0;
     orc_bicgs(c, x, g, &inc[(size_t)i * U], 0, tol, maxit, NULL);
     for (int n = 0; n < U; n++) x[n] *= g[n];
-    orc_aggregate(c, x, &mes[i * nr]);
+    orc_receive(c, x, &mes[i * nr]);
   }
   double objnorm = 0, mesnorm = 0;
   for (int n = 0; n < U; n++) objnorm += creal(chi_true[n] * conj(chi_true[n]));
@@ -802,7 +843,7 @@ int orc_dbim(orc_ctx *c, int ntx, const double complex *inc, const double comple
       }
       orc_bicgs(c, x, g, cc, 0, tol, maxit, NULL);
       for (int n = 0; n < U; n++) y[n] += o[n] * k2 * x[n];
-      orc_aggregate(c, y, &rhs[i * nr]);
+      orc_receive(c, y, &rhs[i * nr]);
     }
     double complex t1 = 0;
     double t2 = 0;
@@ -820,7 +861,7 @@ int orc_dbim(orc_ctx *c, int ntx, const double complex *inc, const double comple
       for (int n = 0; n < U; n++) ti[n] = 0;
       orc_bicgs(c, ti, g, &inc[(size_t)i * U], 0, tol, maxit, NULL);
       for (int n = 0; n < U; n++) x[n] = ti[n] * o[n] * k2;
-      orc_aggregate(c, x, &rhs[i * nr]);
+      orc_receive(c, x, &rhs[i * nr]);
       for (int m = 0; m < nr; m++) mesd[i * nr + m] = rhs[i * nr + m] - mes[i * nr + m];
     }
     memcpy(save, od, U * sizeof(double complex));

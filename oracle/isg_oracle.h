@@ -66,6 +66,14 @@ int orc_dbim(orc_ctx *c, int ntx, const double complex *inc, const double comple
              double regular, double tol, int maxit, double complex *chi, double *hist, double *alpha,
              double complex *beta);
 
+/* Near-field receivers (setup_born.cpp:52-60): go[m][n] = integrate(rx_m, pos_n)
+ * for numrx points at the given radius; radius 0 removes them.  orc_receive /
+ * orc_receiveh apply go / conj(go)^T (the far-field aggregate / aggregateh when
+ * none are set), and orc_dbim uses them in place of aggregate / aggregateh. */
+void orc_set_nearfield(orc_ctx *c, double radius);
+void orc_receive(orc_ctx *c, const double complex *x, double complex *rx);
+void orc_receiveh(orc_ctx *c, double complex *x, const double complex *rx);
+
 /* Seeded inputs (isg_inputs.c): the library's random-ellipse contrast
  * chi = eps_r - 1 in raster order, and plane waves exp(i k0 d.r) of
  * transmitters first..first+count-1 of ntx, written in tree order through

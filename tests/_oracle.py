@@ -54,6 +54,9 @@ class Oracle:
                 getattr(L, f).argtypes = [_P, _P, _P]
             L.orc_matvec.argtypes = [_P, _P, _P, _P, _I]
             L.orc_bicgs.argtypes = [_P, _P, _P, _P, _I, _D, _I, ctypes.POINTER(_D)]
+            L.orc_set_nearfield.argtypes = [_P, _D]
+            L.orc_receive.argtypes = [_P, _P, _P]
+            L.orc_receiveh.argtypes = [_P, _P, _P]
             L.orc_bicgs.restype = _I
             cls._lib = L
         return cls._lib
@@ -130,6 +133,22 @@ class Oracle:
 
     def pos(self):
         return self.table("pos", 0, self.U, "c")
+
+    def set_nearfield(self, radius: float):
+        """Near-field receivers at this radius (orc_dbim then uses them); 0 removes them."""
+        self.L.orc_set_nearfield(self.h, radius)
+
+    def receive(self, x):
+        x = np.ascontiguousarray(x, np.complex128)
+        rx = self._out(self.numrx)
+        self.L.orc_receive(self.h, _arr(x), _arr(rx))
+        return rx
+
+    def receiveh(self, rx):
+        rx = np.ascontiguousarray(rx, np.complex128)
+        x = self._out(self.U)
+        self.L.orc_receiveh(self.h, _arr(x), _arr(rx))
+        return x
 
 
 def _oracle_lib():
