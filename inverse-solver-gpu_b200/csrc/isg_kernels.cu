@@ -88,15 +88,16 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // the same six-column window, each with 27 of the 40 translation weights
 // T[(dy+3)*7+dx+3][k] whose offset is not inside the 3x3.  A thread owns one
 // sample k of one column of sibling groups: it keeps the 40 weights in
-// registers and slides the window down `ty` groups, two new rows per step,
-// fetched one step ahead into a ring of eight row slots.  The step loop is
-// unrolled four times so every slot index is a compile-time constant (the
-// ring turns once per four steps): no register moves, and the four siblings'
-// locals accumulate in place (from the prefetched old values after L2L).
-// Rows outside the grid are the same for the whole block (a branch); a
-// column outside the grid reads a ring of zeros with row stride 0, so no load
-// needs a select.  108 complex FMAs per 12 loads; consecutive threads take
-// consecutive samples, so every load and store is coalesced.
+// registers and slides the window down `ty` groups, two new rows per step.
+// The window lives in a private ring of kM2lRing row slots in shared memory
+// (slot-major, thread-minor, so every access is conflict-free), filled by
+// 8-byte cp.async copies kM2lAhead steps ahead of the step being computed,
+// one commit group per step.  Each thread waits only for its own copies
+// (cp.async.wait_group), so there is no block barrier, and the loads in
+// flight hold no registers (155 registers, three blocks and 12 warps per SM).
+// Rows outside the grid are the same for the whole block and copy as zeros; a
+// column outside the grid copies zeros by a zero source size.  Consecutive
+// threads take consecutive samples, so every load and store is coalesced.
 struct M2lArgs {
   const float2 *mul;
   float2 *loc;
@@ -109,73 +110,27 @@ struct M2lArgs {
   int lvl;
 };
 
-// One thread's six source columns: base address and bytes per cluster row.
-struct M2lCols {
-  const char *base[6];
-  unsigned stride[6];
-};
+constexpr int kM2lAhead = 3;                 // steps of window rows in flight ahead of the computing step
+constexpr int kM2lRing = 6 + 2 * kM2lAhead;  // row slots per thread
+constexpr int kM2lThreads = 128;
+constexpr size_t kM2lSmem = (size_t)kM2lRing * 6 * kM2lThreads * sizeof(float2);  // 72 KB
 
-__device__ __forceinline__ void m2l_row(const M2lCols &C, int row, int n, float2 (&dst)[6]) {
-  if (row >= 0 && row < n) {
-#pragma unroll
-    for (int j = 0; j < 6; j++)
-      dst[j] = __ldg((const float2 *)(C.base[j] + (unsigned long long)(unsigned)row * C.stride[j]));
-  } else {
-#pragma unroll
-    for (int j = 0; j < 6; j++) dst[j] = make_float2(0.f, 0.f);
-  }
+__device__ __forceinline__ void cp_async8z(void *smem, const void *gmem, bool valid) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(valid ? 8 : 0) : "memory");
 }
-
-// The sibling group's locals at group row a (read before adding to them).
-template <bool ACC>
-__device__ __forceinline__ void m2l_old(const float2 *out, size_t row_stride, int ns, int b, int a,
-                                        float2 (&dst)[2][2]) {
-#pragma unroll
-  for (int oy = 0; oy < 2; oy++)
-#pragma unroll
-    for (int ox = 0; ox < 2; ox++)
-      dst[oy][ox] = ACC ? out[(size_t)(2 * a + oy) * row_stride + (size_t)(2 * b + ox) * ns] : make_float2(0.f, 0.f);
-}
-
-// Step S (mod 4) of the ring: group row a, window rows 2a-2+i in slot (2S+i) & 7.
-template <int S, bool ACC>
-__device__ __forceinline__ void m2l_step(const M2lArgs &A, const M2lCols &C, const float2 (&tw)[7][7],
-                                         float2 (&w)[8][6], float2 (&ob)[2][2][2], float2 *out, size_t row_stride,
-                                         int b, int a, int a1, float &mx) {
-  if (a + 1 < a1) {
-    m2l_row(C, 2 * a + 4, A.n, w[(2 * S + 6) & 7]);
-    m2l_row(C, 2 * a + 5, A.n, w[(2 * S + 7) & 7]);
-    m2l_old<ACC>(out, row_stride, A.ns, b, a + 1, ob[(S + 1) & 1]);
-  }
-  float2(&acc)[2][2] = ob[S & 1];
-#pragma unroll
-  for (int i = 0; i < 6; i++)
-#pragma unroll
-    for (int j = 0; j < 6; j++)
-#pragma unroll
-      for (int oy = 0; oy < 2; oy++)
-#pragma unroll
-        for (int ox = 0; ox < 2; ox++) {
-          const int dy = i - 2 - oy, dx = j - 2 - ox;  // source minus target
-          if (dy >= -1 && dy <= 1 && dx >= -1 && dx <= 1) continue;
-          cfma(acc[oy][ox], tw[dy + 3][dx + 3], w[(2 * S + i) & 7][j]);
-        }
-#pragma unroll
-  for (int oy = 0; oy < 2; oy++)
-#pragma unroll
-    for (int ox = 0; ox < 2; ox++) {
-      out[(size_t)(2 * a + oy) * row_stride + (size_t)(2 * b + ox) * A.ns] = acc[oy][ox];
-      mx = fmaxf(mx, fmaxf(fabsf(acc[oy][ox].x), fabsf(acc[oy][ox].y)));
-    }
-}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 template <bool ACC>
-__global__ void __launch_bounds__(128, 2) k_m2l(M2lArgs A) {
+__global__ void __launch_bounds__(kM2lThreads, 3) k_m2l(M2lArgs A) {
+  extern __shared__ __align__(16) float2 m2l_ring[];  // [kM2lRing][6][kM2lThreads]
   const int rhs = blockIdx.z;
   if (A.active && !A.active[rhs]) return;
   const int half = A.n >> 1, ns = A.ns;
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
-  if (f >= half * ns) return;
+  if (f >= half * ns) return;  // no block barrier below
   const int b = f / ns, k = f - b * ns;
   const int a0 = blockIdx.y * A.ty, a1 = min(a0 + A.ty, half);
   float2 tw[7][7];
@@ -188,32 +143,86 @@ __global__ void __launch_bounds__(128, 2) k_m2l(M2lArgs A) {
   const float2 *m = A.mul + (size_t)rhs * A.mp + A.off + k;
   float2 *out = A.loc + (size_t)rhs * A.mp + A.off + k;
   const size_t row_stride = (size_t)A.n * ns;
-  M2lCols C;
+  // the six window columns 2b-2 .. 2b+3: element offsets within a row, and which are inside the grid
+  int coff[6];
+  unsigned cin = 0;
 #pragma unroll
   for (int j = 0; j < 6; j++) {
     const int col = 2 * b - 2 + j;
     const bool ok = col >= 0 && col < A.n;
-    C.base[j] = ok ? (const char *)(m + (size_t)col * ns) : (const char *)(A.zeros + k);
-    C.stride[j] = ok ? (unsigned)(row_stride * sizeof(float2)) : 0u;
+    coff[j] = ok ? col * ns : 0;
+    cin |= ok ? 1u << j : 0u;
   }
-  float2 w[8][6], ob[2][2][2];
+  float2 *ring = m2l_ring + threadIdx.x;
+  const int r0 = 2 * a0 - 2;  // window row of slot 0
+  auto issue_row = [&](int r) {
+    const bool rok = r >= 0 && r < A.n;  // the same for the whole block
+    float2 *dst = ring + (size_t)((r - r0) % kM2lRing) * 6 * kM2lThreads;
+    const float2 *src = m + (rok ? (size_t)r * row_stride : 0);
 #pragma unroll
-  for (int i = 0; i < 6; i++) m2l_row(C, 2 * a0 - 2 + i, A.n, w[i]);
-  m2l_old<ACC>(out, row_stride, ns, b, a0, ob[0]);
+    for (int j = 0; j < 6; j++) cp_async8z(dst + j * kM2lThreads, src + coff[j], rok && ((cin >> j) & 1));
+  };
+  // groups: the first step's six rows, then two rows per step
+  for (int i = 0; i < 6; i++) issue_row(r0 + i);
+  cp_async_commit();
+#pragma unroll
+  for (int s = 1; s < kM2lAhead; s++) {
+    if (a0 + s < a1) {
+      issue_row(2 * (a0 + s) + 2);
+      issue_row(2 * (a0 + s) + 3);
+    }
+    cp_async_commit();
+  }
+  float2 ob[2][2];
+  auto old = [&](int a, float2(&dst)[2][2]) {
+#pragma unroll
+    for (int oy = 0; oy < 2; oy++)
+#pragma unroll
+      for (int ox = 0; ox < 2; ox++)
+        dst[oy][ox] =
+            ACC ? out[(size_t)(2 * a + oy) * row_stride + (size_t)(2 * b + ox) * ns] : make_float2(0.f, 0.f);
+  };
+  old(a0, ob);
   float mx = 0.f;
 #pragma unroll 1
-  for (int a = a0; a < a1; a += 4) {
-    m2l_step<0, ACC>(A, C, tw, w, ob, out, row_stride, b, a, a1, mx);
-    if (a + 1 >= a1) break;
-    m2l_step<1, ACC>(A, C, tw, w, ob, out, row_stride, b, a + 1, a1, mx);
-    if (a + 2 >= a1) break;
-    m2l_step<2, ACC>(A, C, tw, w, ob, out, row_stride, b, a + 2, a1, mx);
-    if (a + 3 >= a1) break;
-    m2l_step<3, ACC>(A, C, tw, w, ob, out, row_stride, b, a + 3, a1, mx);
+  for (int a = a0; a < a1; a++) {
+    if (a + kM2lAhead < a1) {
+      issue_row(2 * (a + kM2lAhead) + 2);
+      issue_row(2 * (a + kM2lAhead) + 3);
+    }
+    cp_async_commit();
+    float2 acc[2][2] = {{ob[0][0], ob[0][1]}, {ob[1][0], ob[1][1]}};
+    if (a + 1 < a1) old(a + 1, ob);  // the next step's old locals, in flight during this one
+    cp_async_wait_group<kM2lAhead>();  // this step's rows have landed
+#pragma unroll
+    for (int i = 0; i < 6; i++) {
+      const float2 *src = ring + (size_t)((2 * a - 2 + i - r0) % kM2lRing) * 6 * kM2lThreads;
+      float2 w[6];
+#pragma unroll
+      for (int j = 0; j < 6; j++) w[j] = src[j * kM2lThreads];
+#pragma unroll
+      for (int j = 0; j < 6; j++)
+#pragma unroll
+        for (int oy = 0; oy < 2; oy++)
+#pragma unroll
+          for (int ox = 0; ox < 2; ox++) {
+            const int dy = i - 2 - oy, dx = j - 2 - ox;  // source minus target
+            if (dy >= -1 && dy <= 1 && dx >= -1 && dx <= 1) continue;
+            cfma(acc[oy][ox], tw[dy + 3][dx + 3], w[j]);
+          }
+    }
+#pragma unroll
+    for (int oy = 0; oy < 2; oy++)
+#pragma unroll
+      for (int ox = 0; ox < 2; ox++) {
+        out[(size_t)(2 * a + oy) * row_stride + (size_t)(2 * b + ox) * ns] = acc[oy][ox];
+        mx = fmaxf(mx, fmaxf(fabsf(acc[oy][ox].x), fabsf(acc[oy][ox].y)));
+      }
   }
+  cp_async_wait_group<0>();
   if (A.locmax) {  // the level's maximum, for the power-of-two scale of the tensor-core L2L below it
-    const unsigned m = __activemask(), bits = __reduce_max_sync(m, __float_as_uint(mx));
-    if ((threadIdx.x & 31) == __ffs(m) - 1 && bits) atomicMax(&A.locmax[rhs * kMaxLevels + A.lvl], bits);
+    const unsigned mm = __activemask(), bits = __reduce_max_sync(mm, __float_as_uint(mx));
+    if ((threadIdx.x & 31) == __ffs(mm) - 1 && bits) atomicMax(&A.locmax[rhs * kMaxLevels + A.lvl], bits);
   }
 }
 
@@ -661,9 +670,9 @@ void launch_m2l(const DevPlan &P, int lvl, const float2 *mul, float2 *loc, int n
   count_launch();
   const dim3 grid(bx, (half + ty - 1) / ty, nrhs);
   if (accumulate)
-    k_m2l<true><<<grid, 128, 0, st>>>(A);
+    k_m2l<true><<<grid, kM2lThreads, kM2lSmem, st>>>(A);
   else
-    k_m2l<false><<<grid, 128, 0, st>>>(A);
+    k_m2l<false><<<grid, kM2lThreads, kM2lSmem, st>>>(A);
 }
 
 void launch_l2l(const DevPlan &P, int lvl, float2 *loc, int nrhs, const int *active, cudaStream_t st) {
@@ -730,6 +739,8 @@ cudaError_t kernels_setup() {
   if (e == cudaSuccess) e = allow_max_smem(k_m2m_tile, optin);
   if (e == cudaSuccess) e = allow_max_smem(k_l2l_tile, optin);
   if (e == cudaSuccess) e = allow_max_smem(k_near, optin);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_m2l<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kM2lSmem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_m2l<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kM2lSmem);
   return e;
 }
 
