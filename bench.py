@@ -163,8 +163,10 @@ def near_field_flops_per_rhs(s) -> tuple[float, float]:
 
 # DRAM bytes (read + write) of one near-field launch over 16 RHS of the 1024^2
 # workload: a constant captured once with ncu (dram__bytes_read.sum +
-# dram__bytes_write.sum, one launch, --set full), not measured by this run.
-NEAR_TRAFFIC_16RHS_CAPTURED = 293.4e6 + 109.0e6
+# dram__bytes_write.sum, one launch, --set full), not measured by this run;
+# the traffic grows with the RHS processed, so a launch over R RHS is R / 16
+# of it scaled.
+NEAR_TRAFFIC_16RHS_CAPTURED = 389.3e6 + 100.3e6
 
 
 def cpu_reference_sample(ref, g, b, budget_s: float, max_solves: int):
@@ -305,6 +307,131 @@ def learned_arm(s, isg, g, b, stream, pairs: int, steps: int, zero_iterations: f
             "pays": its < zero_iterations}
 
 
+def status_counts(infos) -> dict:
+    names = {0: "ok", 1: "not_converged", 2: "breakdown", 3: "nonfinite", 6: "timeout"}
+    c = {}
+    for i in infos:
+        k = names.get(i["status"], str(i["status"]))
+        c[k] = c.get(k, 0) + 1
+    return c
+
+
+def run_config3(isg, torch, dev, seed: int = 3000) -> dict:
+    """64 independent forward problems, grid sides drawn from {128, 256, 512,
+    1024}, 16-128 plane-wave transmitters each, random ellipses eps_r in
+    [1.1, 1.8], solved together by isg.multi.MultiSolver (one multi-RHS block
+    per grid size, per-RHS contrasts and masks, the size groups on concurrent
+    streams) to true residual 1e-5."""
+    from isg.multi import MultiSolver, level_of
+    rng = np.random.default_rng(seed)
+    ms = MultiSolver(max_rhs=256, device=dev.index or 0, engine=isg.ENGINE_TENSOR)
+    ellipses = {5: 3, 6: 5, 7: 10, 8: 20}
+    problems = []
+    for p in range(64):
+        lvl = int(rng.choice([5, 6, 7, 8]))
+        s = ms.solver(lvl)
+        chi = s.raster_to_tree(s.phantom(seed=seed + p, count=ellipses[lvl], axis=(1.0, 3.0), eps=(1.1, 1.8)))
+        ntx = int(rng.integers(16, 129))
+        b = s.plane_waves(ntx, order=isg.ORDER_TREE)
+        problems.append((torch.from_numpy(((2 * np.pi) ** 2 * chi).astype(np.complex64)).to(dev),
+                         torch.from_numpy(b.astype(np.complex64)).to(dev)))
+    ms.solve(problems[:4], tol=TOL, maxit=1000)  # warm-up: graphs, kernels, launch attributes
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    out = ms.solve(problems, tol=TOL, maxit=1000)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_total = e0.elapsed_time(e1)
+    infos = [i for _, inf in out for i in inf]
+    by = {}
+    for (g, b), (_, inf) in zip(problems, out):
+        n = int(round(g.shape[-1] ** 0.5))
+        d = by.setdefault(n, {"problems": 0, "solves": 0, "iterations": []})
+        d["problems"] += 1
+        d["solves"] += b.shape[0]
+        d["iterations"] += [i["iterations"] for i in inf]
+    for d in by.values():
+        d["mean_iterations"] = float(np.mean(d.pop("iterations")))
+    return {"workload": "64 problems, sides U{128,256,512,1024}, 16-128 plane-wave Tx, ellipses eps_r U[1.1,1.8]",
+            "solves": len(infos), "seconds": ms_total / 1e3, "value": len(infos) * 1000.0 / ms_total,
+            "unit": "solves/s", "all_converged": all(i["status"] == 0 and 0 <= i["true_residual"] <= TOL
+                                                    for i in infos),
+            "status_counts": status_counts(infos), "max_true_residual": max(i["true_residual"] for i in infos),
+            "by_side": {str(k): v for k, v in sorted(by.items())}}
+
+
+def run_config4(isg, torch, dev, fp64_fields: int = 2, nrhs: int = 64) -> dict:
+    """4096 x 4096 pixels (409.6 wavelengths, 9 MLFMA levels), Gaussian
+    random field contrast (correlation length 2 wavelengths).  Timed: one batch
+    of `nrhs` plane-wave illuminations (128 illuminations are two such
+    batches) at eps_r in [1.0, 1.1], tensor engine, true residual 1e-5.
+    Probed: the configured eps_r in [1.0, 1.6] on 8 illuminations for 400
+    iterations (the residual it reaches).  FP64: for `fp64_fields` fields, the
+    FP64 solution of the same system obtained by iterative refinement whose
+    residuals b - (x - G(g x)) come from the reference's own FP64 MLFMA
+    operator (oracle/_ref, solve.cpp:25-248), refined until that FP64 residual
+    is below 1e-10; the error of the 1e-5 field against it is reported."""
+    from _oracle import Reference, rel
+    level = 10
+    s = isg.Solver(level, numrx=32, max_rhs=nrhs, device=dev.index or 0)
+    s.setup_gpu()
+    out = {"workload": "4096x4096 px (409.6 lambda), 9 MLFMA levels, GRF corr 2 lambda", "nrhs": nrhs}
+    chi = s.phantom(seed=4010, kind=1, eps=(1.0, 1.1), corr_len=2.0)
+    g_np = (s.opts.k0 ** 2) * s.raster_to_tree(chi)
+    b_np = s.plane_waves(128, first=0, count=nrhs)
+    g = torch.from_numpy(g_np.astype(np.complex64)).to(dev)
+    b = torch.from_numpy(b_np.astype(np.complex64)).to(dev)
+    opts = isg.default_solve_opts(tol=TOL, maxit=3000, engine=isg.ENGINE_TENSOR, check_every=4)
+    stream = torch.cuda.Stream(dev)
+    x = torch.zeros_like(b)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    infos = s.bicgs(x, g, b, opts=opts, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    out["eps_1.0_1.1"] = {"value": nrhs * 1000.0 / ms, "unit": "solves/s", "seconds": ms / 1e3,
+                          "mean_iterations": float(np.mean([i["iterations"] for i in infos])),
+                          "all_converged": all(i["status"] == 0 and 0 <= i["true_residual"] <= TOL for i in infos),
+                          "status_counts": status_counts(infos),
+                          "max_true_residual": max(i["true_residual"] for i in infos)}
+    # the configured contrast, bounded
+    chi6 = s.phantom(seed=4010, kind=1, eps=(1.0, 1.6), corr_len=2.0)
+    g6 = torch.from_numpy(((s.opts.k0 ** 2) * s.raster_to_tree(chi6)).astype(np.complex64)).to(dev)
+    x6 = torch.zeros_like(b[:8])
+    i6 = s.bicgs(x6, g6, b[:8], opts=isg.default_solve_opts(tol=TOL, maxit=400, engine=isg.ENGINE_TENSOR,
+                                                             check_every=4), stream=stream)
+    out["eps_1.0_1.6_probe"] = {"iterations": 400, "residuals": [i["residual"] for i in i6]}
+    # FP64 solutions by refinement with the reference's FP64 operator
+    if fp64_fields and Reference.available():
+        ref = Reference(level, 2 * math.pi, 32)
+        x_h = x[:fp64_fields].cpu().numpy().astype(np.complex128)
+        errs = []
+        o1 = isg.default_solve_opts(tol=1e-6, maxit=3000, engine=isg.ENGINE_TENSOR, check_every=4)
+        for j in range(fp64_fields):
+            bj = b_np[j]
+            xr = x_h[j].copy()
+            hist = []
+            for _ in range(6):
+                r = bj - (xr - ref.mlfma(g_np * xr))
+                hist.append(float(np.linalg.norm(r) / np.linalg.norm(bj)))
+                if hist[-1] < 1e-10:
+                    break
+                rd = torch.from_numpy(r.astype(np.complex64)).to(dev)
+                dd = torch.zeros_like(rd)
+                s.bicgs(dd, g, rd, opts=o1, stream=stream)
+                xr = xr + dd.cpu().numpy().astype(np.complex128)
+            # the same field solved to 1e-6: what is left at 1e-5 is the stopping tolerance, not the arithmetic
+            xt = torch.zeros_like(b[j])
+            s.bicgs(xt, g, b[j], opts=isg.default_solve_opts(tol=1e-6, maxit=5000, engine=isg.ENGINE_TENSOR,
+                                                            check_every=4), stream=stream)
+            errs.append({"tx": j, "field_err_vs_fp64": rel(x_h[j], xr), "fp64_residual_history": hist,
+                         "tol_1e-6_field_err_vs_fp64": rel(xt.cpu().numpy().astype(np.complex128), xr)})
+        out["parity"] = errs
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -317,6 +444,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline and the FP64 field check")
     ap.add_argument("--learned-pairs", type=int, default=16, help="solver-generated training pairs (0: no learned arm)")
     ap.add_argument("--learned-steps", type=int, default=150)
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4"],
+                    help="c2: the headline 1024^2 / 256-Tx line (default); c3, c4: the mixed-size and 4096^2 "
+                         "measurements, one JSON line of their own")
     ap.add_argument("--stages-only", type=int, default=0,
                     help="only time the matvec stages on this many RHS of the workload (profiling case)")
     args = ap.parse_args()
@@ -337,6 +467,11 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
+    if args.workload != "c2":
+        dev = torch.device("cuda", local)
+        res = (run_config3 if args.workload == "c3" else run_config4)(isg, torch, dev)
+        print(json.dumps({"workload": args.workload, **res}))
+        return
     if args.stages_only:
         s = isg.Solver(LEVEL, numrx=32, max_rhs=args.stages_only, device=local)
         for eng in ([isg.ENGINE_SIMT, isg.ENGINE_TENSOR] if args.engine == "auto" else
@@ -425,14 +560,16 @@ def main():
                                                                check_every=1), stream, args.plain_sample)
 
     # Roofline: the dominant kernel (near field + L2P on the tensor cores) and,
-    # beside it, the whole matvec against HBM; both on a 16-RHS batch, each
-    # stage timed alone with CUDA events on the launching stream.
-    st = s.time_stages(nrhs=16, engine=engine, reps=5)
+    # beside it, the whole matvec against HBM; both on the step's own batch of
+    # NTX RHS (the launch shape of the timed region), each stage timed alone
+    # with CUDA events on the launching stream.
+    RB = NTX
+    st = s.time_stages(nrhs=RB, engine=engine, reps=3)
     pk = peaks()
-    bytes_mv = algorithmic_bytes_per_matvec(s) * 16
+    bytes_mv = algorithmic_bytes_per_matvec(s) * RB
     achieved = bytes_mv / (st["total"] * 1e-3) / 1e9
     exe, useful = near_field_flops_per_rhs(s)
-    near_useful = 16 * useful / (st["near"] * 1e-3) / 1e12
+    near_useful = RB * useful / (st["near"] * 1e-3) / 1e12
     tc = engine == isg.ENGINE_TENSOR
 
     out = {
@@ -448,18 +585,20 @@ def main():
                    "autotuned": tuned},
         "mean_iterations": float(np.mean(iters)), "all_converged": not bad,
         "max_true_residual": max(i["true_residual"] for i in infos),
-        "roofline": ({"bound": "tensor", "kernel": "k_tc_near (near field + L2P, 3xFP16 split tcgen05), 16 RHS",
+        "roofline": ({"bound": "tensor",
+                      "kernel": f"k_tc_near_pipe (near field + L2P, 3xFP16 split tcgen05), {RB} RHS per launch",
                       "achieved": near_useful, "peak": pk["bf16_tflops"], "unit": "TFLOP/s",
                       "frac": near_useful / pk["bf16_tflops"], "peak_src": pk["src"] + " (bf16 burst)",
                       "flops": "useful complex work: (9 x 64 + ns_leaf) complex MACs x 8 per pixel",
-                      "traffic": NEAR_TRAFFIC_16RHS_CAPTURED, "traffic_src": "captured constant (one ncu launch)",
+                      "traffic": NEAR_TRAFFIC_16RHS_CAPTURED * RB / 16,
+                      "traffic_src": "one ncu capture of a 16-RHS launch, scaled by RHS",
                       "launch_ms": st["near"],
-                      "executed_tflops": 16 * exe / (st["near"] * 1e-3) / 1e12,
+                      "executed_tflops": RB * exe / (st["near"] * 1e-3) / 1e12,
                       "executed_flops_per_rhs": exe} if tc else
-                     {"bound": "hbm", "kernel": "MLFMA matvec (SIMT engine), 16 RHS", "achieved": achieved,
+                     {"bound": "hbm", "kernel": f"MLFMA matvec (SIMT engine), {RB} RHS", "achieved": achieved,
                       "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved / pk["hbm_gbs"], "peak_src": pk["src"],
                       "traffic": None}),
-        "roofline_matvec": {"bound": "hbm", "kernel": "MLFMA matvec (P2M, M2M, M2L+L2L, L2P+near), 16 RHS",
+        "roofline_matvec": {"bound": "hbm", "kernel": f"MLFMA matvec (P2M, M2M, M2L+L2L, L2P+near), {RB} RHS",
                             "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
                             "frac": achieved / pk["hbm_gbs"], "peak_src": pk["src"], "stage_ms": st,
                             "algorithmic_bytes_per_rhs": algorithmic_bytes_per_matvec(s)},
