@@ -561,6 +561,30 @@ __host__ __device__ inline int np_stage(int a, int nl2p, int &idx) {
   return 1;
 }
 
+// A dot product's terms over one epilogue chunk at FP32 instruction cost:
+// each product a b is split exactly into its rounded value p and its rounding
+// error fma(a, b, -p) (Dekker's TwoProduct); the p go round-robin into four
+// independent FP32 partial sums (short dependency chains), the errors into a
+// fifth, and the five are added into the FP64 sum once per chunk.  Each
+// partial sum rounds three times over a 16-term chunk, below the rounding of
+// the complex64 vectors themselves; the _rn intrinsics keep the compiler from
+// contracting the exact split.  (Converting every product to FP64 cost 1.75
+// ms of a 4.4 ms 256-RHS launch; Kahan compensation, a four-add dependency
+// chain per term, cost more than that.)
+struct Acc32 {
+  float p[4] = {0.f, 0.f, 0.f, 0.f}, e = 0.f;
+  __device__ __forceinline__ void add_prod(int j, float a, float b) {
+    const float q = __fmul_rn(a, b);
+    e = __fadd_rn(e, fmaf(a, b, -q));
+    p[j & 3] = __fadd_rn(p[j & 3], q);
+  }
+  __device__ __forceinline__ double take() {
+    const double v = (((double)p[0] + (double)p[1]) + ((double)p[2] + (double)p[3])) + (double)e;
+    p[0] = p[1] = p[2] = p[3] = e = 0.f;
+    return v;
+  }
+};
+
 struct TcNearPipeArgs {
   const float2 *x, *g;  // operator input (transformed by mode)
   const float2 *xe;     // x of the `x - ...` epilogue
@@ -636,9 +660,22 @@ __global__ void __launch_bounds__(kNpThreads, 1) k_tc_near_pipe(TcNearPipeArgs A
     // ---- A-stage tensor loads into the staging buffers: rows of 32 reals ----
     if (lane == 0) {
       int ka = 0;
+      const bool pre_x = A.epi == EPI_FWD || A.epi == EPI_ADJ || A.red == RED_TS;
       for (int w = first; w < A.nitems && !*abort; w = next_item(w)) {
         int rhs, ty0, tx0, ntile;
         geom(w, rhs, ty0, tx0, ntile);
+        // the rows the epilogue will read for this item (x, the dot vector, g), into L2
+        // about one item ahead of it: its loads then wait on L2, not on HBM
+        {
+          const uint32_t run = (uint32_t)min(kTX, A.nleaf - tx0) * kBB * 8;
+          const size_t rb = (size_t)rhs * A.U;
+          for (int r = 0; r < ntile * kTY && ty0 + r < A.nleaf; r++) {
+            const size_t at = (size_t)((ty0 + r) * A.nleaf + tx0) * kBB;
+            if (pre_x) bulk_prefetch_l2(A.xe + rb + at, run);
+            if (A.red == RED_DOT) bulk_prefetch_l2(A.dot_a + rb + at, run);
+            if (A.epi == EPI_ADJ) bulk_prefetch_l2(A.g + rhs * A.gstride + at, run);
+          }
+        }
         for (int a = 0; a < na; a++, ka++) {
           const int i = ka % kNpNS;
           if (!mbar_wait_or(sfree + i, ((ka / kNpNS) & 1) ^ 1, abort, A.err, kErrNp)) break;
@@ -819,25 +856,30 @@ __global__ void __launch_bounds__(kNpThreads, 1) k_tc_near_pipe(TcNearPipeArgs A
       const float *xr = xf + 2 * rbase, *ar = af + 2 * rbase;
       float *yr = yf + 2 * rbase;
       double r0 = 0, r1 = 0, r2 = 0;
+      Acc32 q0, q1, q2;
       if (hh < ntile) {  // warp-uniform
-#pragma unroll 1
-        for (int ch = 0; ch < 8; ch++) {
-          float d[16], xv[16], av[16], gv[16];
-          tmem_ld16(tmem + ((uint32_t)(32 * qd) << 16) + (uint32_t)(set * 256 + 128 * hh + 16 * ch), d);
-          int fi[16];  // float offset within the RHS: 2 (leaf * 64 + pixel) + component
-          bool live[16];
+        // chunks of 8 leaves (one leaf row of the tile); the loads of chunk ch + 1 are in
+        // flight while chunk ch is computed and stored
+        const int lyb = ty0 + hh * kTY;
+        auto fidx = [&](int ch, int j) { return 2 * ((lyb + ch) * A.nleaf + tx0 + j) * kBB + 32 * qd + lane; };
+        auto load = [&](int ch, float (&xv)[8], float (&av)[8], float (&gv)[8], unsigned &live) {
+          live = 0;
 #pragma unroll
-          for (int j = 0; j < 16; j++) {  // loads first: one round trip per chunk
-            const int n = 16 * ch + j, ly = ty0 + hh * kTY + n / kTX, lx = tx0 + n % kTX;
-            live[j] = ok && ly < A.nleaf && lx < A.nleaf;
-            fi[j] = 2 * (ly * A.nleaf + lx) * kBB + 32 * qd + lane;
-            xv[j] = (need_x && live[j]) ? xr[fi[j]] : 0.f;
-            av[j] = (A.red == RED_DOT && live[j]) ? ar[fi[j]] : 0.f;
-            gv[j] = (A.epi == EPI_ADJ && live[j]) ? gf[fi[j]] : 0.f;
+          for (int j = 0; j < 8; j++) {
+            const bool lv = ok && lyb + ch < A.nleaf && tx0 + j < A.nleaf;
+            live |= lv ? 1u << j : 0u;
+            const int fi = fidx(ch, j);
+            xv[j] = (need_x && lv) ? xr[fi] : 0.f;
+            av[j] = (A.red == RED_DOT && lv) ? ar[fi] : 0.f;
+            gv[j] = (A.epi == EPI_ADJ && lv) ? gf[fi] : 0.f;
           }
+        };
+        auto process = [&](int ch, const float (&xv)[8], const float (&av)[8], const float (&gv)[8], unsigned live) {
+          float d[8];
+          tmem_ld8(tmem + ((uint32_t)(32 * qd) << 16) + (uint32_t)(set * 256 + 128 * hh + 8 * ch), d);
 #pragma unroll
-          for (int j = 0; j < 16; j++) {
-            if (!live[j]) continue;  // warp-uniform
+          for (int j = 0; j < 8; j++) {
+            if (!((live >> j) & 1)) continue;  // warp-uniform
             const float o = d[j] * inv;
             float v = o;
             if (A.epi == EPI_FWD) {
@@ -848,18 +890,33 @@ __global__ void __launch_bounds__(kNpThreads, 1) k_tc_near_pipe(TcNearPipeArgs A
             } else if (A.epi == EPI_CONJ) {
               v = odd ? -o : o;
             }
-            yr[fi[j]] = v;
+            yr[fidx(ch, j)] = v;
             if (A.red == RED_DOT) {  // conj(a) y
               const float vp = __shfl_xor_sync(0xffffffffu, v, 1);
-              r0 += (double)av[j] * v;
-              r1 += (odd ? -1.0 : 1.0) * (double)av[j] * vp;
+              q0.add_prod(j, av[j], v);
+              q1.add_prod(j, odd ? -av[j] : av[j], vp);
             } else if (A.red == RED_TS) {  // conj(y) x and |y|^2
               const float xp = __shfl_xor_sync(0xffffffffu, xv[j], 1);
-              r0 += (double)v * xv[j];
-              r1 += (odd ? -1.0 : 1.0) * (double)v * xp;
-              r2 += (double)v * v;
+              q0.add_prod(j, v, xv[j]);
+              q1.add_prod(j, odd ? -v : v, xp);
+              q2.add_prod(j, v, v);
             }
           }
+          if (A.red != RED_NONE && (ch & 1)) {  // two chunks' FP32 partial sums into the FP64 ones
+            r0 += q0.take();
+            r1 += q1.take();
+            r2 += q2.take();
+          }
+        };
+        float xa[8], aa[8], ga[8], xb[8], ab[8], gb[8];
+        unsigned la, lb;
+        load(0, xa, aa, ga, la);
+#pragma unroll 1
+        for (int ch = 0; ch < 16; ch += 2) {
+          load(ch + 1, xb, ab, gb, lb);
+          process(ch, xa, aa, ga, la);
+          if (ch + 2 < 16) load(ch + 2, xa, aa, ga, la);
+          process(ch + 1, xb, ab, gb, lb);
         }
       }
       if (A.red != RED_NONE) {
