@@ -83,7 +83,8 @@ typedef struct isg_solve_opts {
   int guess;           /* isg_guess */
   int check_every;     /* iterations between host convergence polls (>= 1) */
   int true_residual;   /* 1: after convergence recompute b - A x and restart any RHS above tol */
-  int max_restarts;    /* restarts allowed by the true-residual check */
+  int max_restarts;    /* restarts allowed by the true-residual check; each restart halves the
+                          recursive-residual target of that RHS */
   int engine;          /* isg_engine */
   int graph;           /* 1: replay the check_every-iteration block as a CUDA graph captured on the
                           first poll (streams other than the legacy default stream); 0: launch directly */
@@ -295,6 +296,11 @@ typedef struct isg_fno_opts {
   int layers;    /* spectral layers (default 4) */
   int batch;     /* samples per device pass; sizes the activation buffers (default 4) */
   uint64_t seed; /* parameter initialisation */
+  int tensor;    /* 1 (default): every GEMM of the network (lift, channel mixes, x transforms,
+                    projection, and their backward products) runs on the tcgen05 tensor cores with
+                    BF16 operands and FP32 accumulation, and the spectral weights are rounded to
+                    BF16 where they multiply; the FP32 master parameters take the Adam updates.
+                    0: the same network in FP32 on the CUDA cores. */
 } isg_fno_opts;
 void isg_default_fno_opts(isg_fno_opts *o);
 /* Attach a freshly initialised network to the context (replaces any). */

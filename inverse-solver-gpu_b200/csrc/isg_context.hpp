@@ -15,6 +15,7 @@ struct RhsState {
   double bn;          // ||b|| (1 when ||b|| < 1e-20, bicgs.cpp:111-113)
   double err;         // recursive ||r|| / ||b||
   double tres;        // true residual after the final check, -1 if not computed
+  double target;      // recursive-residual stopping target: tol, halved at each true-residual restart
   double rho[2];      // current <r~, r>
   double rho1[2];     // previous rho
   double alpha[2];
