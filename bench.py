@@ -432,6 +432,128 @@ def run_config4(isg, torch, dev, fp64_fields: int = 2, nrhs: int = 64) -> dict:
     return out
 
 
+def run_config5(isg, torch, dev, triples: int = 4096, epochs: float = 2.0, iters: int = 10, reg: float = 0.5,
+                fno_batch: int = 8) -> dict:
+    """Full inversion with the learned warm start: 512 x 512 pixels (51.2
+    lambda, 7 MLFMA levels), 128 line-source transmitters and 256 near-field
+    receivers on a 40-wavelength circle, an 8-ellipse contrast (semi-axes 1-3
+    lambda) with eps_r in [1.1, 1.5], measurements with 1 % complex Gaussian
+    noise, `iters` Polak-Ribiere iterations with Tikhonov weight `reg`, every
+    forward and adjoint solve to true residual 1e-5 on the tensor engine.
+
+    The network (width 32, 4 spectral layers, 12 x 24 modes, BF16 tcgen05
+    products with FP32 accumulation) is trained first on `triples`
+    solver-generated (contrast, incident field, total field) triples: contrasts
+    of the same distribution (other seeds), 16 random transmitters each.  The
+    same inversion then runs with every solve from zero (the reference's
+    method), from the previous iteration's fields, from the network (forward
+    and adjoint solves), and from both (network on the first iteration, then
+    the previous fields); each is timed on the device.  The plain single-RHS
+    FP32 solver (one transmitter at a time, SIMT engine, zero start) runs the
+    same inversion for the comparison the metric names."""
+    level, ntx, nrx, radius = 7, 128, 256, 40.0
+    s = isg.Solver(level, numrx=nrx, max_rhs=ntx, device=dev.index or 0)
+    s.setup_gpu()
+    s.set_nearfield_receivers(radius)
+    k2 = s.opts.k0 ** 2
+    U = s.numunk
+    stream = torch.cuda.Stream(dev)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+
+    def timed(fn):
+        ev[0].record(stream)
+        out = fn()
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        return out, ev[0].elapsed_time(ev[1]) / 1e3
+
+    def ellipses(seed):
+        return s.raster_to_tree(s.phantom(seed=seed, count=8, axis=(1.0, 3.0), eps=(1.1, 1.5)))
+
+    inc = torch.from_numpy(s.line_sources(ntx, radius).astype(np.complex64)).to(dev)
+    chi_true = torch.from_numpy(ellipses(5000)).to(dev)
+    mes = s.measure(inc, chi_true, noise=0.01, seed=5001, tol=1e-6, engine=isg.ENGINE_TENSOR, stream=stream)
+    out = {"workload": "512x512 px (51.2 lambda), 128 line-source Tx x 256 near-field Rx on r=40 lambda, "
+                       "8 ellipses eps_r U[1.1,1.5], 1% noise, %d PR iterations, Tikhonov %.2g" % (iters, reg),
+           "tol": TOL}
+
+    # training triples: contrast j (one of triples / 16), transmitter t, total field u
+    rng = np.random.default_rng(5100)
+    ncon = triples // 16
+    t0 = time.perf_counter()
+    gall = torch.from_numpy(np.stack([k2 * ellipses(6000 + j) for j in range(ncon)]).astype(np.complex64)).to(dev)
+    cid = np.repeat(np.arange(ncon), 16)
+    tid = np.concatenate([rng.choice(ntx, 16, replace=False) for _ in range(ncon)])
+    cid_t, tid_t = torch.from_numpy(cid).to(dev), torch.from_numpy(tid).to(dev)
+    uall = torch.zeros((ncon * 16, U), dtype=torch.complex64, device=dev)
+    data_its = []
+    opts_t = isg.default_solve_opts(tol=TOL, maxit=1000, engine=isg.ENGINE_TENSOR, check_every=2)
+    for j in range(0, ncon * 16, ntx):
+        sl = slice(j, min(j + ntx, ncon * 16))
+        ub = torch.zeros_like(uall[sl])
+        info = s.bicgs(ub, gall[cid_t[sl]], inc[tid_t[sl]], opts=opts_t, stream=stream)
+        uall[sl] = ub
+        data_its += [i["iterations"] for i in info]
+    torch.cuda.synchronize()
+    t_data = time.perf_counter() - t0
+    s.fno_create(width=32, modes=12, layers=4, batch=fno_batch, seed=1)
+    steps = int(epochs * ncon * 16 / fno_batch)
+    losses = []
+    t0 = time.perf_counter()
+    for k in range(steps):
+        sel = torch.from_numpy(rng.choice(ncon * 16, fno_batch, replace=False)).to(dev)
+        losses.append(s.fno_train_step(gall[cid_t[sel]], inc[tid_t[sel]], uall[sel],
+                                       lr=3e-3 if k < 2 * steps // 3 else 1e-3, stream=stream))
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    del uall
+    out["training"] = {"triples": ncon * 16, "contrasts": ncon, "data_s": round(t_data, 2),
+                       "data_mean_iterations": float(np.mean(data_its)), "steps": steps, "batch": fno_batch,
+                       "train_s": round(t_train, 2), "loss_first": float(np.mean(losses[:20])),
+                       "loss_last": float(np.mean(losses[-20:])),
+                       "network": "FNO width 32, 4 spectral layers, 12x24 modes, BF16 tcgen05 products, FP32 accumulate"}
+
+    # what the network gains on the forward solves at the true contrast (held out)
+    g_true = (k2 * chi_true).to(torch.complex64)
+    fwd = {}
+    for name, guess in (("zero", isg.GUESS_ZERO), ("learned", isg.GUESS_LEARNED)):
+        x = torch.zeros_like(inc)
+        o = isg.default_solve_opts(tol=TOL, maxit=1000, engine=isg.ENGINE_TENSOR, check_every=2, guess=guess)
+        info, sec = timed(lambda: s.bicgs(x, g_true, inc, opts=o, stream=stream))
+        fwd[name] = {"mean_iterations": float(np.mean([i["iterations"] for i in info])), "seconds": round(sec, 4),
+                     "all_converged": all(i["status"] == 0 and 0 <= i["true_residual"] <= TOL for i in info)}
+    out["forward_at_true_contrast"] = fwd
+
+    def inversion(solver, engine, **kw):
+        chi0 = torch.zeros(U, dtype=torch.complex128, device=dev)
+        (chi, hist), sec = timed(lambda: solver.dbim(inc, mes, chi=chi0, chi_true=chi_true, iterations=iters,
+                                                      regular=reg, stream=stream, tol=TOL, maxit=1000,
+                                                      engine=engine, check_every=2, **kw))
+        return {"seconds": round(sec, 3), "seconds_per_iteration": round(sec / iters, 4),
+                "solves": int(hist[-1]["solves"]), "bicgs_iterations": int(hist[-1]["iterations"]),
+                "misfit": [round(h["misfit"], 6) for h in hist], "object_error_last": hist[-1]["object_error"]}, chi
+
+    runs, chis = {}, {}
+    for name, kw in (("zero_start", {}), ("previous_iterate", {"warm_start": True}),
+                     ("learned", {"guess": isg.GUESS_LEARNED}),
+                     ("learned_then_previous", {"guess": isg.GUESS_LEARNED, "warm_start": True})):
+        runs[name], chis[name] = inversion(s, isg.ENGINE_TENSOR, **kw)
+    ref = chis["zero_start"].cpu().numpy()
+    for name in runs:
+        runs[name]["contrast_vs_zero_start"] = float(np.linalg.norm(chis[name].cpu().numpy() - ref) /
+                                                     np.linalg.norm(ref))
+    del s
+    s1 = isg.Solver(level, numrx=nrx, max_rhs=1, device=dev.index or 0)
+    s1.setup_gpu()
+    s1.set_nearfield_receivers(radius)
+    runs["plain_single_rhs_fp32"], _ = inversion(s1, isg.ENGINE_SIMT)
+    base = runs["plain_single_rhs_fp32"]["seconds"]
+    for name in runs:
+        runs[name]["speedup_vs_plain_single_rhs"] = round(base / runs[name]["seconds"], 2)
+    out["inversions"] = runs
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -444,9 +566,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline and the FP64 field check")
     ap.add_argument("--learned-pairs", type=int, default=16, help="solver-generated training pairs (0: no learned arm)")
     ap.add_argument("--learned-steps", type=int, default=150)
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4"],
-                    help="c2: the headline 1024^2 / 256-Tx line (default); c3, c4: the mixed-size and 4096^2 "
-                         "measurements, one JSON line of their own")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5"],
+                    help="c2: the headline 1024^2 / 256-Tx line (default); c3, c4, c5: the mixed-size, 4096^2 and "
+                         "learned-warm-start inversion measurements, one JSON line of their own")
     ap.add_argument("--stages-only", type=int, default=0,
                     help="only time the matvec stages on this many RHS of the workload (profiling case)")
     args = ap.parse_args()
@@ -469,7 +591,7 @@ def main():
 
     if args.workload != "c2":
         dev = torch.device("cuda", local)
-        res = (run_config3 if args.workload == "c3" else run_config4)(isg, torch, dev)
+        res = {"c3": run_config3, "c4": run_config4, "c5": run_config5}[args.workload](isg, torch, dev)
         print(json.dumps({"workload": args.workload, **res}))
         return
     if args.stages_only:

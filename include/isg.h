@@ -73,8 +73,10 @@ typedef enum isg_engine {
 typedef enum isg_guess {
   ISG_GUESS_ZERO = 0,   /* x0 = 0, as every reference call site (mom.cpp:254,286,324) */
   ISG_GUESS_CALLER = 1, /* x0 = the caller's x on entry (bicgs.cpp:115) */
-  ISG_GUESS_LEARNED = 2 /* x0 from the context's neural-operator warm start (isg_fno_create); forward
-                           solves only, adjoint solves start from zero */
+  ISG_GUESS_LEARNED = 2 /* x0 from the context's neural-operator warm start (isg_fno_create).  isg_bicgs:
+                           forward solves (adjoint solves start from zero).  isg_dbim: the forward
+                           solves and the adjoint solves, the latter through the same network
+                           (x0 = conj(g N(g, conj(y))), y the back-projected data residual) */
 } isg_guess;
 
 typedef struct isg_solve_opts {

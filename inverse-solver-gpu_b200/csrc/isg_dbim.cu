@@ -48,6 +48,19 @@ __global__ void k_conj_g_mul(const float2 *__restrict__ g, const float2 *__restr
     C[r * U + i] = cmul(cconj(g[i]), Y[r * U + i]);
 }
 
+// x = conj(y) per RHS
+__global__ void k_conj_copy(const float2 *__restrict__ y, float2 *__restrict__ x, int U) {
+  const size_t r = blockIdx.y;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < U; i += gridDim.x * blockDim.x) x[r * U + i] = cconj(y[r * U + i]);
+}
+
+// x = conj(g x) per RHS
+__global__ void k_conj_g_times(const float2 *__restrict__ g, float2 *__restrict__ x, int U) {
+  const size_t r = blockIdx.y;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < U; i += gridDim.x * blockDim.x)
+    x[r * U + i] = cconj(cmul(g[i], x[r * U + i]));
+}
+
 // Y += C (mom.cpp:262)
 __global__ void k_add(float2 *__restrict__ Y, const float2 *__restrict__ C, int U) {
   const size_t r = blockIdx.y;
@@ -234,7 +247,21 @@ struct Dbim {
       k_conj_g_mul<<<vgrid(n), 256, 0, st>>>(g, Y, C, U);
       count_launch();
       float2 *xa = warm ? adj + (size_t)k * R * U : X;  // the previous adjoint fields, when kept
-      if ((e = solve(xa, C, n, 1, warm && warm_ready ? ISG_GUESS_CALLER : ISG_GUESS_ZERO)) != ISG_OK) return e;
+      int guess = warm && warm_ready ? ISG_GUESS_CALLER : ISG_GUESS_ZERO;
+      if (guess == ISG_GUESS_ZERO && so.guess == ISG_GUESS_LEARNED && c->fno) {
+        // The adjoint system x - conj(g G conj(x)) = conj(g) y (the adjoint matvec of bicgs.cpp:62-87)
+        // is the forward one in disguise: with z = conj(x) it reads z = g (conj(y) + G z), so
+        // x = conj(g w) with (I - G g) w = conj(y), a forward solve whose incident field conj(y) is
+        // radiated by sources at the receivers.  The forward network's w0 = N(g, conj(y)) therefore
+        // seeds it: x0 = conj(g w0).
+        k_conj_copy<<<vgrid(n), 256, 0, st>>>(Y, xa, U);
+        count_launch();
+        if ((e = fno_apply(c, g, 0, xa, xa, n, ISG_ORDER_BLOCKED, st)) != ISG_OK) return e;
+        k_conj_g_times<<<vgrid(n), 256, 0, st>>>(g, xa, U);
+        count_launch();
+        guess = ISG_GUESS_CALLER;
+      }
+      if ((e = solve(xa, C, n, 1, guess)) != ISG_OK) return e;
       if (warm) cudaMemcpyAsync(X, xa, (size_t)n * U * sizeof(float2), cudaMemcpyDeviceToDevice, st);
       if ((e = run_matvec(c, X, nullptr, 0, C, n, OP_GCONJ, so.engine, RED_NONE, nullptr, nullptr, st)) != ISG_OK)
         return e;

@@ -16,11 +16,14 @@
 // (k_fy_*), a per-mode channel mix (k_mix_*) or an elementwise kernel.  The
 // backward pass applies the exact transposes of the same real-linear maps;
 // Adam updates the FP32 parameters.  Everything runs in this file's kernels.
+#include <cuda_bf16.h>
+
 #include <cmath>
 #include <cstring>
 #include <vector>
 
 #include "isg_context.hpp"
+#include "isg_tc.cuh"
 
 namespace isg {
 
@@ -32,6 +35,8 @@ struct FnoModel {
   std::vector<size_t> off_R, off_W, off_bw;
   float *param = nullptr, *grad = nullptr, *am = nullptr, *av = nullptr;
   int adam_t = 0;
+  bool tensor = true;  // products as BF16 tcgen05 MMAs (FP32 accumulation); false: FP32 k_gemm
+  int *err = nullptr;  // wait-limit flag of the tensor-core GEMM
   float *Ex = nullptr, *Ix = nullptr;  // [N][2M], [2M][N]
   float2 *Fy = nullptr;                // [KY][N]
   float *in = nullptr, *spec = nullptr, *out = nullptr, *dout = nullptr, *dva = nullptr, *dvb = nullptr;
@@ -162,25 +167,34 @@ __global__ void k_fy_inv(const float2 *__restrict__ in, float2 *__restrict__ out
   out[(b * N + y) * M + kx] = acc;
 }
 
+// The weight as the products use it: rounded to BF16 in the tensor-core
+// model (whose GEMMs see BF16 weights), unchanged in the FP32 model.
+__device__ __forceinline__ float2 wround(float2 w, int bf16) {
+  return bf16 ? make_float2(__bfloat162float(__float2bfloat16_rn(w.x)), __bfloat162float(__float2bfloat16_rn(w.y)))
+              : w;
+}
+
 // Y[s][o][k] = sum_c R[k][o][c] X[s][c][k]
 __global__ void k_mix_fwd(const float2 *__restrict__ X, const float2 *__restrict__ R, float2 *__restrict__ Y, int S,
-                          int C, int NM) {
+                          int C, int NM, int bf16) {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= S * C * NM) return;
   const int k = idx % NM, o = (idx / NM) % C, s = idx / (NM * C);
   float2 acc = make_float2(0.f, 0.f);
-  for (int c = 0; c < C; c++) cfma(acc, __ldg(&R[((size_t)k * C + o) * C + c]), X[((size_t)s * C + c) * NM + k]);
+  for (int c = 0; c < C; c++)
+    cfma(acc, wround(__ldg(&R[((size_t)k * C + o) * C + c]), bf16), X[((size_t)s * C + c) * NM + k]);
   Y[((size_t)s * C + o) * NM + k] = acc;
 }
 
 // dX[s][c][k] = sum_o conj(R[k][o][c]) dY[s][o][k]
 __global__ void k_mix_bwd_x(const float2 *__restrict__ dY, const float2 *__restrict__ R, float2 *__restrict__ dX, int S,
-                            int C, int NM) {
+                            int C, int NM, int bf16) {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= S * C * NM) return;
   const int k = idx % NM, c = (idx / NM) % C, s = idx / (NM * C);
   float2 acc = make_float2(0.f, 0.f);
-  for (int o = 0; o < C; o++) cfma(acc, cconj(__ldg(&R[((size_t)k * C + o) * C + c])), dY[((size_t)s * C + o) * NM + k]);
+  for (int o = 0; o < C; o++)
+    cfma(acc, cconj(wround(__ldg(&R[((size_t)k * C + o) * C + c]), bf16)), dY[((size_t)s * C + o) * NM + k]);
   dX[((size_t)s * C + c) * NM + k] = acc;
 }
 
@@ -354,9 +368,173 @@ __global__ void k_adam(float *__restrict__ w, const float *__restrict__ g, float
 
 inline unsigned blocks(long long n, int t = 256) { return (unsigned)((n + t - 1) / t); }
 
-void gemm(cudaStream_t st, int batch, int M, int N, int K, const float *A, long long sAm, long long sAk, long long bA,
+// ---------------- batched strided GEMM on the tcgen05 tensor cores ----------------
+// The same product as k_gemm with BF16 operands and FP32 accumulation: each
+// CTA computes a 128 x NT tile of C (NT = BfArgs::nt, a multiple of 16, at
+// most 256) in TMEM.  Per K-stage of 64 all 256 threads read the FP32 A and B
+// tiles through their strides (consecutive threads along whichever of the two
+// indices is contiguous), round them to BF16 and store them in the K-major
+// no-swizzle core-matrix layout (8 rows x 16 bytes per core matrix); one
+// thread issues the stage's four K = 16 MMAs while the threads fill the other
+// stage buffer.  The epilogue reads TMEM lane = row of the tile, column = n.
+// Rows, columns and K beyond the problem are zero-filled, so any M, N, K work.
+namespace bf {
+using namespace tc;
+constexpr int KC = 64;                 // K per stage
+constexpr int kA = 128 * KC * 2;       // 16 KB: A tile
+constexpr int kB = 256 * KC * 2;       // 32 KB: B tile at NT = 256
+constexpr int kStage = kA + kB;
+constexpr int kSmem = 2 * kStage + 64;  // two stages, mbarriers, TMEM slot
+constexpr int kThreads = 256;
+constexpr int kErr = 151;
+
+__host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N) {
+  return (1u << 4)                      // D format F32
+         | (1u << 7) | (1u << 10)       // A, B format BF16
+         | ((uint32_t)(N >> 3) << 17)   // N / 8
+         | ((uint32_t)(M >> 4) << 24);  // M / 16
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, int acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+// byte offset of element (row, k) in a K-major tile of KC columns
+__device__ __forceinline__ int core_off(int row, int k) {
+  return (((row >> 3) * (KC / 8) + (k >> 3)) * 64 + (row & 7) * 8 + (k & 7)) * 2;
+}
+
+__device__ __forceinline__ uint32_t pack(float a, float b) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);  // a in the low half
+  return *reinterpret_cast<const uint32_t *>(&h);
+}
+
+// rows [r0, r0 + nrows) x K [k0, k0 + KC) of X (element (r, k) at r sr + k sk)
+// as BF16 into dst; rows >= rvalid and k >= kend read as zero
+__device__ __forceinline__ void stage(char *dst, const float *X, long long sr, long long sk, int r0, int nrows,
+                                      int rvalid, int k0, int kend) {
+  const bool kcontig = sk == 1;
+  for (int e = threadIdx.x; e < nrows * (KC / 8); e += kThreads) {
+    const int row = kcontig ? e / (KC / 8) : e % nrows, kc = kcontig ? e % (KC / 8) : e / nrows;
+    const int r = r0 + row, kb = k0 + kc * 8;
+    float v[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) v[q] = (r < rvalid && kb + q < kend) ? X[(long long)r * sr + (long long)(kb + q) * sk] : 0.f;
+    *(uint4 *)(dst + core_off(row, kc * 8)) = make_uint4(pack(v[0], v[1]), pack(v[2], v[3]), pack(v[4], v[5]),
+                                                         pack(v[6], v[7]));
+  }
+}
+
+struct Args {
+  const float *A, *B;
+  float *C;
+  int M, N, K, ksplit, mode, nt;
+  long long sAm, sAk, sBk, sBn, sCm, sCn, bA, bB, bC;
+  float alpha;
+  int *err;
+};
+
+__global__ void __launch_bounds__(kThreads, 1) k_gemm_bf16(Args g) {
+  extern __shared__ __align__(1024) char sm[];
+  uint64_t *mdone = (uint64_t *)(sm + 2 * kStage), *fin = mdone + 2;
+  uint32_t *tslot = (uint32_t *)(mdone + 4);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int batch = blockIdx.z / g.ksplit, ks = blockIdx.z % g.ksplit;
+  const float *A = g.A + batch * g.bA, *B = g.B + batch * g.bB;
+  float *C = g.C + batch * g.bC;
+  const int m0 = blockIdx.y * 128, n0 = blockIdx.x * g.nt;
+  const int kper = ((g.K + g.ksplit - 1) / g.ksplit + KC - 1) / KC * KC;
+  const int kbeg = ks * kper, kend = min(g.K, kbeg + kper);
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < 3; i++) mbar_init(mdone + i, 1);
+    fence_mbar_init();
+  }
+  if (warp == 0) tmem_alloc(tslot, 256);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot, idesc = idesc_bf16_f32(128, g.nt), sbase = smem_u32(sm);
+  bool ok = true;
+  int it = 0;
+  for (int k0 = kbeg; k0 < kend; k0 += KC, it++) {
+    const int b = it & 1;
+    // stage buffer b is free once the MMAs of stage it - 2 are done
+    if (it >= 2) ok = mbar_wait(mdone + b, ((it >> 1) - 1) & 1, g.err, kErr) && ok;
+    char *sa = sm + b * kStage;
+    stage(sa, A, g.sAm, g.sAk, m0, 128, g.M, k0, kend);
+    stage(sa + kA, B, g.sBn, g.sBk, n0, g.nt, g.N, k0, kend);
+    fence_proxy_async();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      tc_fence_after();
+      if (ok) {
+        const uint64_t ad = smem_desc(sbase + b * kStage, 128, KC / 8 * 128);
+        const uint64_t bd = smem_desc(sbase + b * kStage + kA, 128, KC / 8 * 128);
+#pragma unroll
+        for (int q = 0; q < KC / 16; q++)
+          mma_bf16(tmem, desc_add(ad, q * 256), desc_add(bd, q * 256), idesc, (it > 0 || q > 0) ? 1 : 0);
+      }
+      mma_commit(mdone + b);
+    }
+  }
+  if (threadIdx.x == 0) mma_commit(fin);
+  ok = mbar_wait(fin, 0, g.err, kErr) && ok && kend > kbeg;
+  tc_fence_after();
+  // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31, column groups of 16 alternating between w < 4 and w >= 4
+  const int qd = warp & 3, half = warp >> 2, row = m0 + 32 * qd + lane;
+  const int nvalid = min(g.nt, g.N - n0);
+  for (int c0 = 16 * half; c0 < g.nt; c0 += 32) {
+    __syncwarp();
+    float d[16];
+    tmem_ld16(tmem + ((uint32_t)(32 * qd) << 16) + (uint32_t)c0, d);
+    if (!ok || row >= g.M) continue;
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+      if (c0 + q >= nvalid) break;
+      float *c = C + (long long)row * g.sCm + (long long)(n0 + c0 + q) * g.sCn;
+      const float v = g.alpha * d[q];
+      if (g.mode == 2)
+        atomicAdd(c, v);
+      else
+        *c = g.mode == 1 ? *c + v : v;
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, 256);
+}
+}  // namespace bf
+
+void gemm_bf16(cudaStream_t st, int *err, int batch, int M, int N, int K, const float *A, long long sAm, long long sAk,
+               long long bA, const float *B, long long sBk, long long sBn, long long bB, float *C, long long sCm,
+               long long sCn, long long bC, int mode, int ksplit, float alpha) {
+  // rows of the tile come from the larger of M and N: C^T = B^T A^T when M is the small side
+  if (M < 128 && N > M) {
+    std::swap(M, N);
+    std::swap(A, B);
+    std::swap(bA, bB);
+    std::swap(sCm, sCn);
+    const long long am = sBn, ak = sBk, bk = sAk, bn = sAm;
+    sAm = am, sAk = ak, sBk = bk, sBn = bn;
+  }
+  const int nt = std::min(256, (N + 15) / 16 * 16);
+  bf::Args g{A, B, C, M, N, K, ksplit, mode, nt, sAm, sAk, sBk, sBn, sCm, sCn, bA, bB, bC, alpha, err};
+  count_launch();
+  bf::k_gemm_bf16<<<dim3((N + nt - 1) / nt, (M + 127) / 128, batch * ksplit), bf::kThreads, bf::kSmem, st>>>(g);
+}
+
+// The model's GEMMs: BF16 tcgen05 (the default) or FP32 k_gemm.
+void gemm(const FnoModel &F, cudaStream_t st, int batch, int M, int N, int K, const float *A, long long sAm, long long sAk, long long bA,
           const float *B, long long sBk, long long sBn, long long bB, float *C, long long sCm, long long sCn,
           long long bC, int mode, int ksplit = 1, float alpha = 1.f) {
+  if (F.tensor) {
+    gemm_bf16(st, F.err, batch, M, N, K, A, sAm, sAk, bA, B, sBk, sBn, bB, C, sCm, sCn, bC, mode, ksplit,
+              alpha);
+    return;
+  }
   GemmArgs g{A, B, C, M, N, K, ksplit, mode, sAm, sAk, sBk, sBn, sCm, sCn, bA, bB, bC, alpha};
   count_launch();
   k_gemm<<<dim3((N + kGT - 1) / kGT, (M + kGT - 1) / kGT, batch * ksplit), 256, 0, st>>>(g);
@@ -394,6 +572,11 @@ isg_status fno_create(isg_ctx *c, const isg_fno_opts *o) {
   F->NM = F->KY * F->M;
   F->N = N;
   F->P = N * N;
+  F->tensor = o->tensor != 0;
+  if (F->tensor && !tc_available(c)) {
+    c->err = "fno: BF16 tensor-core products need an sm_100 device (set tensor = 0 for FP32)";
+    return ISG_UNSUPPORTED;
+  }
   const int C = F->C, M = F->M, L = F->L, S = F->S, KY = F->KY, NM = F->NM, P = F->P;
   // parameter layout, each block on a 4-float boundary
   size_t off = 0;
@@ -449,7 +632,11 @@ isg_status fno_create(isg_ctx *c, const isg_fno_opts *o) {
   if ((e = ck(F->alloc(&F->param, F->nparam))) || (e = ck(F->alloc(&F->grad, F->nparam))) ||
       (e = ck(F->alloc(&F->am, F->nparam))) || (e = ck(F->alloc(&F->av, F->nparam))) ||
       (e = ck(F->alloc(&F->Ex, ex.size()))) || (e = ck(F->alloc(&F->Ix, ix.size()))) ||
-      (e = ck(F->alloc(&F->Fy, fy.size()))))
+      (e = ck(F->alloc(&F->Fy, fy.size()))) || (e = ck(F->alloc(&F->err, 1))) ||
+      (e = ck(cudaMemset(F->err, 0, sizeof(int)))))
+    return e;
+  if (F->tensor &&
+      (e = ck(cudaFuncSetAttribute(bf::k_gemm_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, bf::kSmem))))
     return e;
   const size_t act = (size_t)S * C * P;
   F->v.assign(L + 1, nullptr);
@@ -499,24 +686,25 @@ void fno_forward(isg_ctx *c, int n, int g_per_sample, cudaStream_t st) {
   count_launch();
   const long long IP = (long long)kFnoIn * P;
   // lift
-  gemm(st, n, C, P, kFnoIn, W + F.off_Wl, kFnoIn, 1, 0, F.in, P, 1, IP, F.v[0], P, 1, (long long)C * P, 0);
+  gemm(F, st, n, C, P, kFnoIn, W + F.off_Wl, kFnoIn, 1, 0, F.in, P, 1, IP, F.v[0], P, 1, (long long)C * P, 0);
   k_act_fwd<<<blocks((long long)n * C * P), 256, 0, st>>>(F.v[0], W + F.off_bl, nullptr, F.v[0], n, C, P, 0);
   count_launch();
   for (int l = 0; l < F.L; l++) {
     const int rows = n * C * N;
-    gemm(st, 1, rows, 2 * M, N, F.v[l], N, 1, 0, F.Ex, 2 * M, 1, 0, F.T, 2 * M, 1, 0, 0);
+    gemm(F, st, 1, rows, 2 * M, N, F.v[l], N, 1, 0, F.Ex, 2 * M, 1, 0, F.T, 2 * M, 1, 0, 0);
     k_fy_fwd<<<blocks((long long)n * C * KY * M), 256, 0, st>>>((const float2 *)F.T, F.X[l], F.Fy, n * C, N, M, KY);
-    k_mix_fwd<<<blocks((long long)n * C * NM), 256, 0, st>>>(F.X[l], (const float2 *)(W + F.off_R[l]), F.Y, n, C, NM);
+    k_mix_fwd<<<blocks((long long)n * C * NM), 256, 0, st>>>(F.X[l], (const float2 *)(W + F.off_R[l]), F.Y, n, C, NM,
+                                                             F.tensor);
     k_fy_inv<<<blocks((long long)n * C * N * M), 256, 0, st>>>(F.Y, (float2 *)F.Z, F.Fy, n * C, N, M, KY);
     count_launch(3);
-    gemm(st, 1, rows, N, 2 * M, F.Z, 2 * M, 1, 0, F.Ix, N, 1, 0, F.spec, N, 1, 0, 0);
-    gemm(st, n, C, P, C, W + F.off_W[l], C, 1, 0, F.v[l], P, 1, (long long)C * P, F.h[l], P, 1, (long long)C * P, 0);
+    gemm(F, st, 1, rows, N, 2 * M, F.Z, 2 * M, 1, 0, F.Ix, N, 1, 0, F.spec, N, 1, 0, 0);
+    gemm(F, st, n, C, P, C, W + F.off_W[l], C, 1, 0, F.v[l], P, 1, (long long)C * P, F.h[l], P, 1, (long long)C * P, 0);
     k_act_fwd<<<blocks((long long)n * C * P), 256, 0, st>>>(F.h[l], W + F.off_bw[l], F.spec, F.v[l + 1], n, C, P,
                                                             l + 1 < F.L);
     count_launch();
   }
-  gemm(st, n, 2, P, C, W + F.off_Wp, C, 1, 0, F.v[F.L], P, 1, (long long)C * P, F.out, P, 1, 2LL * P, 0);
-  gemm(st, n, 2, P, kFnoIn, W + F.off_Ws, kFnoIn, 1, 0, F.in, P, 1, IP, F.out, P, 1, 2LL * P, 1);
+  gemm(F, st, n, 2, P, C, W + F.off_Wp, C, 1, 0, F.v[F.L], P, 1, (long long)C * P, F.out, P, 1, 2LL * P, 0);
+  gemm(F, st, n, 2, P, kFnoIn, W + F.off_Ws, kFnoIn, 1, 0, F.in, P, 1, IP, F.out, P, 1, 2LL * P, 1);
   k_act_fwd<<<blocks((long long)n * 2 * P), 256, 0, st>>>(F.out, W + F.off_bp, nullptr, F.out, n, 2, P, 0);
   count_launch();
 }
@@ -531,12 +719,12 @@ void fno_backward(isg_ctx *c, int n, cudaStream_t st) {
   const int ks = ksplit_for(P);
   // projection
   const long long IP = (long long)kFnoIn * P;
-  gemm(st, n, 2, C, P, F.dout, P, 1, 2LL * P, F.v[F.L], 1, P, CP, G + F.off_Wp, C, 1, 0, 2, ks);
-  gemm(st, n, 2, kFnoIn, P, F.dout, P, 1, 2LL * P, F.in, 1, P, IP, G + F.off_Ws, kFnoIn, 1, 0, 2, ks);
+  gemm(F, st, n, 2, C, P, F.dout, P, 1, 2LL * P, F.v[F.L], 1, P, CP, G + F.off_Wp, C, 1, 0, 2, ks);
+  gemm(F, st, n, 2, kFnoIn, P, F.dout, P, 1, 2LL * P, F.in, 1, P, IP, G + F.off_Ws, kFnoIn, 1, 0, 2, ks);
   k_bias_grad<<<dim3(2, 64), 256, 0, st>>>(F.dout, G + F.off_bp, n, 2, P);
   count_launch();
   float *dv = F.dva, *dn = F.dvb;
-  gemm(st, n, C, P, 2, W + F.off_Wp, 1, C, 0, F.dout, P, 1, 2LL * P, dv, P, 1, CP, 0);
+  gemm(F, st, n, C, P, 2, W + F.off_Wp, 1, C, 0, F.dout, P, 1, 2LL * P, dv, P, 1, CP, 0);
   for (int l = F.L - 1; l >= 0; l--) {
     if (l + 1 < F.L) {
       k_act_bwd<<<blocks((long long)n * CP), 256, 0, st>>>(dv, F.h[l], (long long)n * CP);
@@ -545,23 +733,23 @@ void fno_backward(isg_ctx *c, int n, cudaStream_t st) {
     // dv now holds dh
     k_bias_grad<<<dim3(C, 64), 256, 0, st>>>(dv, G + F.off_bw[l], n, C, P);
     count_launch();
-    gemm(st, n, C, C, P, dv, P, 1, CP, F.v[l], 1, P, CP, G + F.off_W[l], C, 1, 0, 2, ks);
+    gemm(F, st, n, C, C, P, dv, P, 1, CP, F.v[l], 1, P, CP, G + F.off_W[l], C, 1, 0, 2, ks);
     const int rows = n * C * N;
-    gemm(st, 1, rows, 2 * M, N, dv, N, 1, 0, F.Ix, 1, N, 0, F.Z, 2 * M, 1, 0, 0);
+    gemm(F, st, 1, rows, 2 * M, N, dv, N, 1, 0, F.Ix, 1, N, 0, F.Z, 2 * M, 1, 0, 0);
     k_fy_fwd<<<blocks((long long)n * C * KY * M), 256, 0, st>>>((const float2 *)F.Z, F.Y, F.Fy, n * C, N, M, KY);
     k_mix_bwd_r<<<blocks((long long)NM * C * C), 256, 0, st>>>(F.Y, F.X[l], (float2 *)(G + F.off_R[l]), n, C, NM);
     // dX into the (free) layer-l spectrum buffer of the next pass: reuse T as scratch for dX
     k_mix_bwd_x<<<blocks((long long)n * C * NM), 256, 0, st>>>(F.Y, (const float2 *)(W + F.off_R[l]),
-                                                               (float2 *)F.T, n, C, NM);
+                                                               (float2 *)F.T, n, C, NM, F.tensor);
     k_fy_inv<<<blocks((long long)n * C * N * M), 256, 0, st>>>((const float2 *)F.T, (float2 *)F.Z, F.Fy, n * C, N, M,
                                                                KY);
     count_launch(4);
-    gemm(st, 1, rows, N, 2 * M, F.Z, 2 * M, 1, 0, F.Ex, 1, 2 * M, 0, dn, N, 1, 0, 0);
-    gemm(st, n, C, P, C, W + F.off_W[l], 1, C, 0, dv, P, 1, CP, dn, P, 1, CP, 1);
+    gemm(F, st, 1, rows, N, 2 * M, F.Z, 2 * M, 1, 0, F.Ex, 1, 2 * M, 0, dn, N, 1, 0, 0);
+    gemm(F, st, n, C, P, C, W + F.off_W[l], 1, C, 0, dv, P, 1, CP, dn, P, 1, CP, 1);
     std::swap(dv, dn);
   }
   // lift
-  gemm(st, n, C, kFnoIn, P, dv, P, 1, CP, F.in, 1, P, IP, G + F.off_Wl, kFnoIn, 1, 0, 2, ks);
+  gemm(F, st, n, C, kFnoIn, P, dv, P, 1, CP, F.in, 1, P, IP, G + F.off_Wl, kFnoIn, 1, 0, 2, ks);
   k_bias_grad<<<dim3(C, 64), 256, 0, st>>>(dv, G + F.off_bl, n, C, P);
   count_launch();
 }
@@ -598,6 +786,19 @@ isg_status fno_gather(isg_ctx *c, const float2 *g, int64_t gs, const float2 *b, 
 
 }  // namespace
 
+// ISG_TIMEOUT once a tensor-core GEMM of the model has hit its wait limit
+// (synchronises the stream).
+isg_status fno_status(isg_ctx *c, cudaStream_t st) {
+  int h = 0;
+  isg_status e = cuda_check(c, cudaMemcpyAsync(&h, c->fno->err, sizeof(int), cudaMemcpyDeviceToHost, st), "fno status");
+  if (e == ISG_OK) e = cuda_check(c, cudaStreamSynchronize(st), "fno status");
+  if (e == ISG_OK && h) {
+    c->err = "a tensor-core GEMM of the warm-start network hit its wait limit";
+    return ISG_TIMEOUT;
+  }
+  return e;
+}
+
 // x0 = b + N(g, b) for nrhs samples, all vectors in the caller's order.
 isg_status fno_apply(isg_ctx *c, const float2 *g, int64_t gs, const float2 *b, float2 *x, int nrhs, int order,
                      cudaStream_t st) {
@@ -621,7 +822,8 @@ isg_status fno_apply(isg_ctx *c, const float2 *g, int64_t gs, const float2 *b, f
       launch_permute(c->P.perm_tree, F.xr, dst, (int)U, n, false, st);
     }
   }
-  return cuda_check(c, cudaGetLastError(), "fno apply");
+  isg_status e = cuda_check(c, cudaGetLastError(), "fno apply");
+  return e == ISG_OK ? fno_status(c, st) : e;
 }
 
 // Gradient of the mean loss over nrhs samples into F.grad (zeroed first); the
@@ -671,7 +873,8 @@ isg_status fno_gradient(isg_ctx *c, const float2 *g, int64_t gs, const float2 *b
     for (int s = 0; s < n; s++) total += h[2 * s + 1] / std::max(h[2 * s], 1e-30);
   }
   if (loss) *loss = total / nrhs;
-  return cuda_check(c, cudaGetLastError(), "fno gradient");
+  isg_status e = cuda_check(c, cudaGetLastError(), "fno gradient");
+  return e == ISG_OK ? fno_status(c, st) : e;
 }
 
 isg_status fno_adam(isg_ctx *c, float lr, cudaStream_t st) {
@@ -723,6 +926,7 @@ void isg_default_fno_opts(isg_fno_opts *o) {
   o->layers = 4;
   o->batch = 4;
   o->seed = 1;
+  o->tensor = 1;
 }
 
 isg_status isg_fno_create(isg_ctx *c, const isg_fno_opts *o) {

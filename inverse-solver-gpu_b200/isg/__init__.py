@@ -77,7 +77,7 @@ class Phantom(ctypes.Structure):
 
 class FnoOpts(ctypes.Structure):
     _fields_ = [("width", ctypes.c_int), ("modes", ctypes.c_int), ("layers", ctypes.c_int), ("batch", ctypes.c_int),
-                ("seed", ctypes.c_uint64)]
+                ("seed", ctypes.c_uint64), ("tensor", ctypes.c_int)]
 
 
 _lib = None
@@ -341,11 +341,13 @@ class Solver:
         return out
 
     # ---- learned warm start ----
-    def fno_create(self, width: int = 32, modes: int = 12, layers: int = 4, batch: int = 4, seed: int = 1):
-        """Attach a freshly initialised neural-operator warm start (ISG_GUESS_LEARNED)."""
+    def fno_create(self, width: int = 32, modes: int = 12, layers: int = 4, batch: int = 4, seed: int = 1,
+                   tensor: bool = True):
+        """Attach a freshly initialised neural-operator warm start (ISG_GUESS_LEARNED); tensor: BF16
+        tcgen05 products with FP32 accumulation (default), else FP32 on the CUDA cores."""
         o = FnoOpts()
         lib().isg_default_fno_opts(ctypes.byref(o))
-        o.width, o.modes, o.layers, o.batch, o.seed = width, modes, layers, batch, seed
+        o.width, o.modes, o.layers, o.batch, o.seed, o.tensor = width, modes, layers, batch, seed, int(tensor)
         self._check(lib().isg_fno_create(self._h, ctypes.byref(o)), "fno_create")
 
     def fno_params(self, which: int = 0) -> np.ndarray:
