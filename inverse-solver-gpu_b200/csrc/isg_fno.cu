@@ -376,15 +376,16 @@ inline unsigned blocks(long long n, int t = 256) { return (unsigned)((n + t - 1)
 // indices is contiguous), round them to BF16 and store them in the K-major
 // no-swizzle core-matrix layout (8 rows x 16 bytes per core matrix); one
 // thread issues the stage's four K = 16 MMAs while the threads fill the other
-// stage buffer.  The epilogue reads TMEM lane = row of the tile, column = n.
+// stage buffer.  Shared memory and TMEM are sized to the tile (one stage
+// buffer when K fits in one, TMEM columns rounded up from NT), so the skinny
+// products of the network (K and N of 32) run many CTAs per SM.  The epilogue reads TMEM lane = row of the tile, column = n.
 // Rows, columns and K beyond the problem are zero-filled, so any M, N, K work.
 namespace bf {
 using namespace tc;
 constexpr int KC = 64;                 // K per stage
 constexpr int kA = 128 * KC * 2;       // 16 KB: A tile
 constexpr int kB = 256 * KC * 2;       // 32 KB: B tile at NT = 256
-constexpr int kStage = kA + kB;
-constexpr int kSmem = 2 * kStage + 64;  // two stages, mbarriers, TMEM slot
+constexpr int kSmem = 2 * (kA + kB) + 64;  // at most: two stages at NT = 256, mbarriers, TMEM slot
 constexpr int kThreads = 256;
 constexpr int kErr = 151;
 
@@ -432,6 +433,7 @@ struct Args {
   const float *A, *B;
   float *C;
   int M, N, K, ksplit, mode, nt;
+  int stage, tcols;  // bytes of one stage buffer (A tile + nt B rows); TMEM columns (power of two >= nt, >= 32)
   long long sAm, sAk, sBk, sBn, sCm, sCn, bA, bB, bC;
   float alpha;
   int *err;
@@ -439,8 +441,6 @@ struct Args {
 
 __global__ void __launch_bounds__(kThreads, 1) k_gemm_bf16(Args g) {
   extern __shared__ __align__(1024) char sm[];
-  uint64_t *mdone = (uint64_t *)(sm + 2 * kStage), *fin = mdone + 2;
-  uint32_t *tslot = (uint32_t *)(mdone + 4);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int batch = blockIdx.z / g.ksplit, ks = blockIdx.z % g.ksplit;
   const float *A = g.A + batch * g.bA, *B = g.B + batch * g.bB;
@@ -448,11 +448,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_bf16(Args g) {
   const int m0 = blockIdx.y * 128, n0 = blockIdx.x * g.nt;
   const int kper = ((g.K + g.ksplit - 1) / g.ksplit + KC - 1) / KC * KC;
   const int kbeg = ks * kper, kend = min(g.K, kbeg + kper);
+  const int nbuf = kper > KC ? 2 : 1;  // one stage buffer when the split's K fits in one
+  uint64_t *mdone = (uint64_t *)(sm + nbuf * g.stage), *fin = mdone + 2;
+  uint32_t *tslot = (uint32_t *)(mdone + 4);
   if (threadIdx.x == 0) {
     for (int i = 0; i < 3; i++) mbar_init(mdone + i, 1);
     fence_mbar_init();
   }
-  if (warp == 0) tmem_alloc(tslot, 256);
+  if (warp == 0) tmem_alloc(tslot, g.tcols);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -463,7 +466,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_bf16(Args g) {
     const int b = it & 1;
     // stage buffer b is free once the MMAs of stage it - 2 are done
     if (it >= 2) ok = mbar_wait(mdone + b, ((it >> 1) - 1) & 1, g.err, kErr) && ok;
-    char *sa = sm + b * kStage;
+    char *sa = sm + b * g.stage;
     stage(sa, A, g.sAm, g.sAk, m0, 128, g.M, k0, kend);
     stage(sa + kA, B, g.sBn, g.sBk, n0, g.nt, g.N, k0, kend);
     fence_proxy_async();
@@ -471,8 +474,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_bf16(Args g) {
     if (threadIdx.x == 0) {
       tc_fence_after();
       if (ok) {
-        const uint64_t ad = smem_desc(sbase + b * kStage, 128, KC / 8 * 128);
-        const uint64_t bd = smem_desc(sbase + b * kStage + kA, 128, KC / 8 * 128);
+        const uint64_t ad = smem_desc(sbase + b * g.stage, 128, KC / 8 * 128);
+        const uint64_t bd = smem_desc(sbase + b * g.stage + kA, 128, KC / 8 * 128);
 #pragma unroll
         for (int q = 0; q < KC / 16; q++)
           mma_bf16(tmem, desc_add(ad, q * 256), desc_add(bd, q * 256), idesc, (it > 0 || q > 0) ? 1 : 0);
@@ -504,7 +507,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_bf16(Args g) {
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 0) tmem_dealloc(tmem, 256);
+  if (warp == 0) tmem_dealloc(tmem, g.tcols);
 }
 }  // namespace bf
 
@@ -521,9 +524,17 @@ void gemm_bf16(cudaStream_t st, int *err, int batch, int M, int N, int K, const 
     sAm = am, sAk = ak, sBk = bk, sBn = bn;
   }
   const int nt = std::min(256, (N + 15) / 16 * 16);
-  bf::Args g{A, B, C, M, N, K, ksplit, mode, nt, sAm, sAk, sBk, sBn, sCm, sCn, bA, bB, bC, alpha, err};
+  int tcols = 32;
+  while (tcols < nt) tcols *= 2;
+  const int stage = bf::kA + nt * bf::KC * 2;
+  const int kper = ((K + ksplit - 1) / ksplit + bf::KC - 1) / bf::KC * bf::KC;
+  // at most 512 / tcols CTAs may share an SM's 512 TMEM columns: ask for enough shared memory that no
+  // more fit (228 KB per SM, 1 KB of it reserved per CTA), so no CTA waits inside tcgen05.alloc
+  const int ctas = 512 / tcols;
+  const int smem = std::max((kper > bf::KC ? 2 : 1) * stage + 64, 233472 / (ctas + 1) - 1024 + 16);
+  bf::Args g{A, B, C, M, N, K, ksplit, mode, nt, stage, tcols, sAm, sAk, sBk, sBn, sCm, sCn, bA, bB, bC, alpha, err};
   count_launch();
-  bf::k_gemm_bf16<<<dim3((N + nt - 1) / nt, (M + 127) / 128, batch * ksplit), bf::kThreads, bf::kSmem, st>>>(g);
+  bf::k_gemm_bf16<<<dim3((N + nt - 1) / nt, (M + 127) / 128, batch * ksplit), bf::kThreads, smem, st>>>(g);
 }
 
 // The model's GEMMs: BF16 tcgen05 (the default) or FP32 k_gemm.

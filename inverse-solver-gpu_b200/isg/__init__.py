@@ -151,10 +151,21 @@ def _ptr(t) -> int | None:
 
 
 def _stream(stream) -> int | None:
-    """The caller's stream, defaulting to torch's current stream (0 is CUDA's legacy default)."""
+    """The caller's stream, defaulting to torch's current stream (0 is CUDA's legacy default).
+
+    A torch stream other than the current one first waits for the work queued
+    on the current stream, where torch made the call's input tensors (an
+    indexing kernel, or a copy from pageable host memory whose DMA may still
+    be in flight when `.to()` returns): the library's kernels then never read
+    an input before it is written."""
     if stream is None:
         import torch
         return torch.cuda.current_stream().cuda_stream or None
+    if hasattr(stream, "wait_stream") and hasattr(stream, "device"):
+        import torch
+        cur = torch.cuda.current_stream(stream.device)
+        if cur.cuda_stream != stream.cuda_stream:
+            stream.wait_stream(cur)
     return stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
 
 
