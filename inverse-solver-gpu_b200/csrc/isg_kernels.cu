@@ -113,7 +113,11 @@ struct M2lArgs {
 constexpr int kM2lAhead = 3;                 // steps of window rows in flight ahead of the computing step
 constexpr int kM2lRing = 6 + 2 * kM2lAhead;  // row slots per thread
 constexpr int kM2lThreads = 128;
-constexpr size_t kM2lSmem = (size_t)kM2lRing * 6 * kM2lThreads * sizeof(float2);  // 72 KB
+// window columns per ring row for NC sibling-group columns per thread (6 or 8)
+__host__ __device__ constexpr int m2l_cols(int nc) { return 4 + 2 * nc; }
+__host__ __device__ constexpr size_t m2l_smem(int nc) {  // 72 KB (NC = 1), 96 KB (NC = 2)
+  return (size_t)kM2lRing * m2l_cols(nc) * kM2lThreads * sizeof(float2);
+}
 
 __device__ __forceinline__ void cp_async8z(void *smem, const void *gmem, bool valid) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -123,15 +127,21 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-template <bool ACC>
-__global__ void __launch_bounds__(kM2lThreads, 3) k_m2l(M2lArgs A) {
-  extern __shared__ __align__(16) float2 m2l_ring[];  // [kM2lRing][6][kM2lThreads]
+// NC sibling-group columns per thread: groups 2 bp .. 2 bp + NC - 1 of the
+// thread's column pair bp read window columns 2 b0 - 2 .. 2 b0 + 2 NC + 1
+// (b0 = NC bp), so with NC = 2 one 6 x 8 window feeds 8 outputs (216 complex
+// FMAs) where two NC = 1 threads read 6 x 6 windows each: a third fewer ring
+// loads and cp.async issues per FMA, at 8 instead of 12 warps per SM.
+template <bool ACC, int NC>
+__global__ void __launch_bounds__(kM2lThreads, NC == 1 ? 3 : 2) k_m2l(M2lArgs A) {
+  constexpr int NW = m2l_cols(NC);
+  extern __shared__ __align__(16) float2 m2l_ring[];  // [kM2lRing][NW][kM2lThreads]
   const int rhs = blockIdx.z;
   if (A.active && !A.active[rhs]) return;
-  const int half = A.n >> 1, ns = A.ns;
+  const int half = A.n >> 1, ns = A.ns, ncp = half / NC;
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
-  if (f >= half * ns) return;  // no block barrier below
-  const int b = f / ns, k = f - b * ns;
+  if (f >= ncp * ns) return;  // no block barrier below
+  const int bp = f / ns, k = f - bp * ns, b0 = NC * bp;
   const int a0 = blockIdx.y * A.ty, a1 = min(a0 + A.ty, half);
   float2 tw[7][7];
 #pragma unroll
@@ -143,12 +153,12 @@ __global__ void __launch_bounds__(kM2lThreads, 3) k_m2l(M2lArgs A) {
   const float2 *m = A.mul + (size_t)rhs * A.mp + A.off + k;
   float2 *out = A.loc + (size_t)rhs * A.mp + A.off + k;
   const size_t row_stride = (size_t)A.n * ns;
-  // the six window columns 2b-2 .. 2b+3: element offsets within a row, and which are inside the grid
-  int coff[6];
+  // the window columns 2 b0 - 2 .. 2 b0 + NW - 3: element offsets within a row, and which are inside the grid
+  int coff[NW];
   unsigned cin = 0;
 #pragma unroll
-  for (int j = 0; j < 6; j++) {
-    const int col = 2 * b - 2 + j;
+  for (int j = 0; j < NW; j++) {
+    const int col = 2 * b0 - 2 + j;
     const bool ok = col >= 0 && col < A.n;
     coff[j] = ok ? col * ns : 0;
     cin |= ok ? 1u << j : 0u;
@@ -157,10 +167,10 @@ __global__ void __launch_bounds__(kM2lThreads, 3) k_m2l(M2lArgs A) {
   const int r0 = 2 * a0 - 2;  // window row of slot 0
   auto issue_row = [&](int r) {
     const bool rok = r >= 0 && r < A.n;  // the same for the whole block
-    float2 *dst = ring + (size_t)((r - r0) % kM2lRing) * 6 * kM2lThreads;
+    float2 *dst = ring + (size_t)((r - r0) % kM2lRing) * NW * kM2lThreads;
     const float2 *src = m + (rok ? (size_t)r * row_stride : 0);
 #pragma unroll
-    for (int j = 0; j < 6; j++) cp_async8z(dst + j * kM2lThreads, src + coff[j], rok && ((cin >> j) & 1));
+    for (int j = 0; j < NW; j++) cp_async8z(dst + j * kM2lThreads, src + coff[j], rok && ((cin >> j) & 1));
   };
   // groups: the first step's six rows, then two rows per step
   for (int i = 0; i < 6; i++) issue_row(r0 + i);
@@ -173,14 +183,16 @@ __global__ void __launch_bounds__(kM2lThreads, 3) k_m2l(M2lArgs A) {
     }
     cp_async_commit();
   }
-  float2 ob[2][2];
-  auto old = [&](int a, float2(&dst)[2][2]) {
+  float2 ob[NC][2][2];
+  auto old = [&](int a, float2(&dst)[NC][2][2]) {
 #pragma unroll
-    for (int oy = 0; oy < 2; oy++)
+    for (int gx = 0; gx < NC; gx++)
 #pragma unroll
-      for (int ox = 0; ox < 2; ox++)
-        dst[oy][ox] =
-            ACC ? out[(size_t)(2 * a + oy) * row_stride + (size_t)(2 * b + ox) * ns] : make_float2(0.f, 0.f);
+      for (int oy = 0; oy < 2; oy++)
+#pragma unroll
+        for (int ox = 0; ox < 2; ox++)
+          dst[gx][oy][ox] = ACC ? out[(size_t)(2 * a + oy) * row_stride + (size_t)(2 * (b0 + gx) + ox) * ns]
+                                : make_float2(0.f, 0.f);
   };
   old(a0, ob);
   float mx = 0.f;
@@ -191,33 +203,43 @@ __global__ void __launch_bounds__(kM2lThreads, 3) k_m2l(M2lArgs A) {
       issue_row(2 * (a + kM2lAhead) + 3);
     }
     cp_async_commit();
-    float2 acc[2][2] = {{ob[0][0], ob[0][1]}, {ob[1][0], ob[1][1]}};
+    float2 acc[NC][2][2];
+#pragma unroll
+    for (int gx = 0; gx < NC; gx++)
+#pragma unroll
+      for (int oy = 0; oy < 2; oy++)
+#pragma unroll
+        for (int ox = 0; ox < 2; ox++) acc[gx][oy][ox] = ob[gx][oy][ox];
     if (a + 1 < a1) old(a + 1, ob);  // the next step's old locals, in flight during this one
     cp_async_wait_group<kM2lAhead>();  // this step's rows have landed
 #pragma unroll
     for (int i = 0; i < 6; i++) {
-      const float2 *src = ring + (size_t)((2 * a - 2 + i - r0) % kM2lRing) * 6 * kM2lThreads;
-      float2 w[6];
+      const float2 *src = ring + (size_t)((2 * a - 2 + i - r0) % kM2lRing) * NW * kM2lThreads;
+      float2 w[NW];
 #pragma unroll
-      for (int j = 0; j < 6; j++) w[j] = src[j * kM2lThreads];
+      for (int j = 0; j < NW; j++) w[j] = src[j * kM2lThreads];
 #pragma unroll
-      for (int j = 0; j < 6; j++)
+      for (int gx = 0; gx < NC; gx++)
 #pragma unroll
-        for (int oy = 0; oy < 2; oy++)
+        for (int jj = 0; jj < 6; jj++)
 #pragma unroll
-          for (int ox = 0; ox < 2; ox++) {
-            const int dy = i - 2 - oy, dx = j - 2 - ox;  // source minus target
-            if (dy >= -1 && dy <= 1 && dx >= -1 && dx <= 1) continue;
-            cfma(acc[oy][ox], tw[dy + 3][dx + 3], w[j]);
-          }
+          for (int oy = 0; oy < 2; oy++)
+#pragma unroll
+            for (int ox = 0; ox < 2; ox++) {
+              const int dy = i - 2 - oy, dx = jj - 2 - ox;  // source minus target
+              if (dy >= -1 && dy <= 1 && dx >= -1 && dx <= 1) continue;
+              cfma(acc[gx][oy][ox], tw[dy + 3][dx + 3], w[2 * gx + jj]);
+            }
     }
 #pragma unroll
-    for (int oy = 0; oy < 2; oy++)
+    for (int gx = 0; gx < NC; gx++)
 #pragma unroll
-      for (int ox = 0; ox < 2; ox++) {
-        out[(size_t)(2 * a + oy) * row_stride + (size_t)(2 * b + ox) * ns] = acc[oy][ox];
-        mx = fmaxf(mx, fmaxf(fabsf(acc[oy][ox].x), fabsf(acc[oy][ox].y)));
-      }
+      for (int oy = 0; oy < 2; oy++)
+#pragma unroll
+        for (int ox = 0; ox < 2; ox++) {
+          out[(size_t)(2 * a + oy) * row_stride + (size_t)(2 * (b0 + gx) + ox) * ns] = acc[gx][oy][ox];
+          mx = fmaxf(mx, fmaxf(fabsf(acc[gx][oy][ox].x), fabsf(acc[gx][oy][ox].y)));
+        }
   }
   cp_async_wait_group<0>();
   if (A.locmax) {  // the level's maximum, for the power-of-two scale of the tensor-core L2L below it
@@ -661,7 +683,8 @@ void launch_m2l(const DevPlan &P, int lvl, const float2 *mul, float2 *loc, int n
   A.zeros = P.zeros;
   A.locmax = locmax;
   A.lvl = lvl;
-  const int half = c.n / 2, bx = (half * c.ns + 127) / 128;
+  // two sibling-group columns per thread where the level has at least four
+  const int half = c.n / 2, nc = half >= 4 ? 2 : 1, bx = (half / nc * c.ns + 127) / 128;
   // eight groups per thread when the grid stays large, fewer for small batches
   int ty = std::min(8, half);
   while (ty > 1 && (size_t)bx * ((half + ty - 1) / ty) * nrhs < 4 * 148) ty /= 2;
@@ -669,10 +692,17 @@ void launch_m2l(const DevPlan &P, int lvl, const float2 *mul, float2 *loc, int n
   A.ty = ty;
   count_launch();
   const dim3 grid(bx, (half + ty - 1) / ty, nrhs);
-  if (accumulate)
-    k_m2l<true><<<grid, kM2lThreads, kM2lSmem, st>>>(A);
-  else
-    k_m2l<false><<<grid, kM2lThreads, kM2lSmem, st>>>(A);
+  if (nc == 2) {
+    if (accumulate)
+      k_m2l<true, 2><<<grid, kM2lThreads, m2l_smem(2), st>>>(A);
+    else
+      k_m2l<false, 2><<<grid, kM2lThreads, m2l_smem(2), st>>>(A);
+  } else {
+    if (accumulate)
+      k_m2l<true, 1><<<grid, kM2lThreads, m2l_smem(1), st>>>(A);
+    else
+      k_m2l<false, 1><<<grid, kM2lThreads, m2l_smem(1), st>>>(A);
+  }
 }
 
 void launch_l2l(const DevPlan &P, int lvl, float2 *loc, int nrhs, const int *active, cudaStream_t st) {
@@ -739,8 +769,10 @@ cudaError_t kernels_setup() {
   if (e == cudaSuccess) e = allow_max_smem(k_m2m_tile, optin);
   if (e == cudaSuccess) e = allow_max_smem(k_l2l_tile, optin);
   if (e == cudaSuccess) e = allow_max_smem(k_near, optin);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_m2l<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kM2lSmem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_m2l<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kM2lSmem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_m2l<true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m2l_smem(1));
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_m2l<false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m2l_smem(1));
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_m2l<true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m2l_smem(2));
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_m2l<false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m2l_smem(2));
   return e;
 }
 
