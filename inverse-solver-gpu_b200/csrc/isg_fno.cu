@@ -418,12 +418,20 @@ __device__ __forceinline__ uint32_t pack(float a, float b) {
 __device__ __forceinline__ void stage(char *dst, const float *X, long long sr, long long sk, int r0, int nrows,
                                       int rvalid, int k0, int kend) {
   const bool kcontig = sk == 1;
+  // 16-byte loads where a row's K run is contiguous and 16-byte aligned (kb is a multiple of 8)
+  const bool vec = kcontig && (sr & 3) == 0 && (reinterpret_cast<uintptr_t>(X) & 15) == 0;
   for (int e = threadIdx.x; e < nrows * (KC / 8); e += kThreads) {
     const int row = kcontig ? e / (KC / 8) : e % nrows, kc = kcontig ? e % (KC / 8) : e / nrows;
     const int r = r0 + row, kb = k0 + kc * 8;
     float v[8];
+    if (vec && r < rvalid && kb + 8 <= kend) {
+      const float4 a = *(const float4 *)(X + (long long)r * sr + kb), b = *(const float4 *)(X + (long long)r * sr + kb + 4);
+      v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w, v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
+    } else {
 #pragma unroll
-    for (int q = 0; q < 8; q++) v[q] = (r < rvalid && kb + q < kend) ? X[(long long)r * sr + (long long)(kb + q) * sk] : 0.f;
+      for (int q = 0; q < 8; q++)
+        v[q] = (r < rvalid && kb + q < kend) ? X[(long long)r * sr + (long long)(kb + q) * sk] : 0.f;
+    }
     *(uint4 *)(dst + core_off(row, kc * 8)) = make_uint4(pack(v[0], v[1]), pack(v[2], v[3]), pack(v[4], v[5]),
                                                          pack(v[6], v[7]));
   }
@@ -489,10 +497,31 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_bf16(Args g) {
   // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31, column groups of 16 alternating between w < 4 and w >= 4
   const int qd = warp & 3, half = warp >> 2, row = m0 + 32 * qd + lane;
   const int nvalid = min(g.nt, g.N - n0);
+  // Row-major C (consecutive columns contiguous): each warp turns its 32 x 16 block around in shared
+  // memory (the stage buffers, free once the MMAs are done) so that 16 lanes write one row's 64 bytes.
+  const bool rowmajor = g.sCn == 1 && g.mode != 2;
+  float *tile = reinterpret_cast<float *>(sm) + warp * (32 * 17);
   for (int c0 = 16 * half; c0 < g.nt; c0 += 32) {
     __syncwarp();
     float d[16];
     tmem_ld16(tmem + ((uint32_t)(32 * qd) << 16) + (uint32_t)c0, d);
+    if (rowmajor) {
+#pragma unroll
+      for (int q = 0; q < 16; q++) tile[lane * 17 + q] = d[q];
+      __syncwarp();
+      const int cq = lane & 15;
+      if (ok && c0 + cq < nvalid) {
+#pragma unroll 4
+        for (int rr = lane >> 4; rr < 32; rr += 2) {
+          const int r = m0 + 32 * qd + rr;
+          if (r >= g.M) break;
+          float *c = C + (long long)r * g.sCm + (n0 + c0 + cq);
+          const float v = g.alpha * tile[rr * 17 + cq];
+          *c = g.mode == 1 ? *c + v : v;
+        }
+      }
+      continue;
+    }
     if (!ok || row >= g.M) continue;
 #pragma unroll
     for (int q = 0; q < 16; q++) {
