@@ -63,7 +63,7 @@ def shard(ntx: int, rank: int, world: int) -> range:
 def _sum(t: torch.Tensor, group) -> torch.Tensor:
     if group is not None:
         import torch.distributed as dist
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
     return t
 
 

@@ -115,3 +115,38 @@ def test_dbim_checkpoint_files_follow_the_reference(tmp_path):
     assert lines.shape == (4, 5)
     want = np.array([[h["misfit"], h["object_error"], h["reg_cost"], h["grad_norm"], h["object_norm"]] for h in hist])
     assert np.allclose(lines, want, rtol=1e-5)
+
+
+def test_sharded_driver_through_a_one_rank_nccl_group():
+    """The sharded loop with its exchanges (the gradient, step-length and
+    misfit sums of mom.cpp:271, 313-314, 362) as NCCL all-reduces of device
+    tensors in a one-rank group on this GPU: the same inversion as the loop
+    without a group, bit for bit (a one-rank sum is the identity)."""
+    import datetime
+    import os
+    import socket
+    import torch
+    import torch.distributed as dist
+    from isg import dbim_dist
+    d = dict(np.load(GOLDEN))
+    ntx = int(d["ntx"])
+    s = isg.Solver(int(d["level"]), numrx=int(d["numrx"]), max_rhs=ntx)
+    chi_tree = torch.from_numpy(s.raster_to_tree(d["phantom"].astype(np.float64) * 0.1 + 0j)).cuda()
+    tol = float(d["tol"])
+    inc_t = torch.from_numpy(s.plane_waves(ntx).astype(np.complex64)).cuda()
+    mes = s.measure(inc_t, chi_tree, order=isg.ORDER_TREE, tol=tol, engine=isg.ENGINE_TENSOR)
+    ops = dbim_dist.GpuOps(s, engine=isg.ENGINE_TENSOR, tol=tol)
+    chi0, hist0 = dbim_dist.dbim(ops, inc_t, mes, float(s.opts.k0), iterations=2)
+    os.environ["NCCL_NVLS_ENABLE"] = "0"
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", 0))
+    try:
+        chi1, hist1 = dbim_dist.dbim(ops, inc_t, mes, float(s.opts.k0), iterations=2, group=dist.group.WORLD)
+        torch.cuda.synchronize()
+    finally:
+        dist.destroy_process_group()
+    assert torch.equal(chi1, chi0)
+    assert [h["misfit"] for h in hist1] == [h["misfit"] for h in hist0]
