@@ -804,7 +804,7 @@ def main():
     out = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        # BASELINE.md publishes no number; the metric's own baseline is the plain single-RHS FP32 solver.
+        # No number is published for this metric; its own baseline is the plain single-RHS FP32 solver.
         "vs_baseline": value / (world * plain["value"]),
         "vs_baseline_basis": "value / (n_gpus x plain single-RHS complex-FP32 SIMT solver on the same workload)",
         "dtype": "c64 (FP64 dots)", "data": "synthetic",

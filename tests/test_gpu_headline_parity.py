@@ -12,8 +12,8 @@ compared with the reference's compiled CPU solver (bicgs.cpp:88-179 over the
 FP64 MLFMA of solve.cpp:25-248, oracle/_ref) on the same inputs:
 
   * converged to 1e-10, i.e. the FP64 solution of the same system.  Bar:
-    relative L2 error <= 1e-4 per field (north-star bound for fields at
-    BiCGSTAB tolerance 1e-5);
+    relative L2 error <= 1e-4 per field (the accuracy asked of fields
+    solved at BiCGSTAB tolerance 1e-5);
   * run to the same tolerance 1e-5 (an FP64 run of the same solver), whose
     own distance to the 1e-10 field is printed beside ours: stopping at
     residual 1e-5 alone leaves about 6e-5 at this size.
