@@ -149,6 +149,29 @@ isg_status isg_matvec(isg_ctx *ctx, const void *x, const void *g, int64_t g_stri
 isg_status isg_bicgs(isg_ctx *ctx, void *x, const void *g, int64_t g_stride, const void *b, int nrhs, int hermitian,
                      int order, const isg_solve_opts *opts, isg_solve_info *info, isg_stream stream);
 
+/* One member of a group solve: a context and its own batch, with the meaning
+ * of the isg_bicgs arguments of the same names. */
+typedef struct isg_group_member {
+  isg_ctx *ctx;
+  void *x;
+  const void *g;
+  int64_t g_stride;
+  const void *b;
+  int nrhs;
+  isg_solve_info *info; /* nrhs records, or NULL */
+} isg_group_member;
+/* isg_bicgs for several independent problems at once, e.g. grids of different
+ * sizes (one context each): members are distinct contexts on one device and
+ * share hermitian, order and opts.  Every block of check_every iterations of
+ * all members is one CUDA graph whose branches are the members' iteration
+ * blocks (captured on the first poll, on streams other than the legacy
+ * default stream), launched once per host poll; one poll reads every
+ * member's active count.  Returns ISG_OK when every RHS of every member
+ * reached tol, else the worst per-RHS status.  No counterpart in the
+ * reference, which solves one problem at a time (mom.cpp:250-350). */
+isg_status isg_bicgs_group(int nmembers, const isg_group_member *members, int hermitian, int order,
+                           const isg_solve_opts *opts, isg_stream stream);
+
 /* ---- receivers ---- */
 /* rx[numrx] = far-field pattern of x (aggregate, matvec_gpu.cu:266-368;
  * solve.cpp:249-355), all levels on the device. */

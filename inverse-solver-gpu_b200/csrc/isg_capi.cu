@@ -544,6 +544,71 @@ isg_status isg_bicgs(isg_ctx *c, void *x, const void *g, int64_t g_stride, const
   return rs;
 }
 
+isg_status isg_bicgs_group(int n, const isg_group_member *m, int hermitian, int order, const isg_solve_opts *opts,
+                           isg_stream stream) {
+  if (n < 1 || !m) return ISG_BAD_ARG;
+  isg_ctx *c0 = m[0].ctx;
+  if (!c0) return ISG_BAD_ARG;
+  isg_solve_opts o;
+  isg_default_solve_opts(&o);
+  if (opts) o = *opts;
+  if (!(o.tol > 0) || o.maxit < 0 || o.guess < 0 || o.guess > ISG_GUESS_LEARNED) {
+    c0->err = "bad solve options";
+    return ISG_BAD_ARG;
+  }
+  for (int i = 0; i < n; i++) {
+    isg_ctx *c = m[i].ctx;
+    isg_status e = c ? need_gpu(c) : ISG_BAD_ARG;
+    if (e != ISG_OK) return e;
+    if (!m[i].x || !m[i].b || bad_order(order) || (e = check_batch(c, m[i].nrhs)) != ISG_OK) return ISG_BAD_ARG;
+    for (int j = 0; j < i; j++)
+      if (m[j].ctx == c || m[j].ctx->opts.device != c->opts.device) {
+        c0->err = "isg_bicgs_group: members need distinct contexts on one device";
+        return ISG_BAD_ARG;
+      }
+    if (o.guess == ISG_GUESS_LEARNED && !hermitian &&
+        (!c->fno || (m[i].g_stride != 0 && m[i].g_stride != c->P.U))) {
+      c->err = "ISG_GUESS_LEARNED needs a warm-start network (isg_fno_create) and g_stride 0 or numunk";
+      return ISG_UNSUPPORTED;
+    }
+  }
+  cudaStream_t st = pick(c0, stream);
+  isg_solve_opts om = o;
+  if (om.guess == ISG_GUESS_LEARNED) om.guess = hermitian ? ISG_GUESS_ZERO : ISG_GUESS_CALLER;
+  std::vector<isg_ctx *> cs(n);
+  std::vector<float2 *> xs(n);
+  std::vector<const float2 *> gs(n), bs(n);
+  std::vector<int64_t> gss(n);
+  std::vector<int> Rs(n);
+  std::vector<isg_solve_info *> infos(n);
+  for (int i = 0; i < n; i++) {
+    isg_ctx *c = m[i].ctx;
+    isg_status e;
+    if (o.guess == ISG_GUESS_LEARNED && !hermitian &&
+        (e = fno_apply(c, (const float2 *)m[i].g, m[i].g_stride, (const float2 *)m[i].b, (float2 *)m[i].x, m[i].nrhs,
+                       order, st)) != ISG_OK)
+      return e;
+    if ((e = contrast(c, m[i].g, m[i].g_stride, m[i].nrhs, order, st, &gs[i])) != ISG_OK) return e;
+    gss[i] = (m[i].g_stride && order != ISG_ORDER_BLOCKED) ? c->P.U : m[i].g_stride;
+    bs[i] = to_blocked(c, m[i].b, c->wy, m[i].nrhs, order, st);
+    xs[i] = (float2 *)m[i].x;
+    if (order != ISG_ORDER_BLOCKED) {
+      xs[i] = c->wx;
+      if (om.guess == ISG_GUESS_CALLER)
+        launch_permute(perm_for(c, order), (const float2 *)m[i].x, xs[i], c->P.U, m[i].nrhs, true, st);
+    }
+    cs[i] = c;
+    Rs[i] = m[i].nrhs;
+    infos[i] = m[i].info;
+  }
+  isg_status rs = run_bicgs_group(n, cs.data(), xs.data(), gs.data(), gss.data(), bs.data(), Rs.data(), hermitian, &om,
+                                  infos.data(), st);
+  if (rs == ISG_CUDA_ERROR || rs == ISG_BAD_ARG || rs == ISG_UNSUPPORTED) return rs;
+  for (int i = 0; i < n; i++) from_blocked(cs[i], xs[i], m[i].x, m[i].nrhs, order, st);
+  isg_status e = cuda_check(c0, cudaStreamSynchronize(st), "bicgs group");
+  return e != ISG_OK ? e : rs;
+}
+
 isg_status isg_aggregate(isg_ctx *c, const void *x, void *rx, int nrhs, int order, isg_stream stream) {
   isg_status e = need_gpu(c);
   if (e != ISG_OK) return e;

@@ -84,6 +84,9 @@ isg_status run_matvec(isg_ctx *c, const float2 *x, const float2 *g, int64_t gs, 
                       const float2 *gx = nullptr);
 isg_status run_bicgs(isg_ctx *c, float2 *x, const float2 *g, int64_t gs, const float2 *b, int nrhs, int hermitian,
                      const isg_solve_opts *o, isg_solve_info *info, cudaStream_t st);
+isg_status run_bicgs_group(int n, isg_ctx *const *cs, float2 *const *xs, const float2 *const *gs, const int64_t *gss,
+                           const float2 *const *bs, const int *Rs, int hermitian, const isg_solve_opts *o,
+                           isg_solve_info *const *infos, cudaStream_t st);
 isg_status cuda_check(isg_ctx *c, cudaError_t e, const char *what);
 // Receiver projection and back-projection on blocked vectors (isg_capi.cu).
 isg_status run_aggregate(isg_ctx *c, const float2 *xb, float2 *rx, int nrhs, cudaStream_t st);

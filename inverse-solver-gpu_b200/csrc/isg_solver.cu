@@ -396,72 +396,137 @@ isg_status run_matvec(isg_ctx *c, const float2 *x, const float2 *g, int64_t gs, 
   return cuda_check(c, cudaGetLastError(), "matvec launch");
 }
 
-isg_status run_bicgs(isg_ctx *c, float2 *x, const float2 *g, int64_t gs, const float2 *b, int R, int hermitian,
-                     const isg_solve_opts *o, isg_solve_info *info, cudaStream_t st) {
-  const int U = c->P.U;
-  const int kind = hermitian ? OP_ADJ : OP_FWD;
-  const int nbv = c->vec_blocks;
-  const double tol = o->tol;
-  const int engine = o->engine;
-  const int nbn = (engine == ISG_ENGINE_TENSOR && tc_available(c)) ? tc_near_blocks(c) : near_blocks_per_rhs(c->P);
-  const int zero_guess = (o->guess == ISG_GUESS_ZERO);
-  isg_status e;
-  dim3 vgrid(nbv, R);
+namespace {
 
-  if (!zero_guess) {
-    e = run_matvec(c, x, g, gs, c->vt, R, kind, engine, RED_NONE, nullptr, nullptr, st);
-    if (e != ISG_OK) return e;
+// One context's batch in a BiCGSTAB solve (bicgs_gpu.cu:116-224,
+// bicgs.cpp:88-179): set-up, the block of `check` iterations, the
+// true-residual check and the results.  isg_bicgs drives one run;
+// isg_bicgs_group drives several contexts' runs together.
+struct BicgsRun {
+  isg_ctx *c;
+  float2 *x;
+  const float2 *g, *b;
+  int64_t gs;
+  int R, kind, engine, nbv, nbn, check, zero_guess;
+  const isg_solve_opts *o;
+  float2 *gx;  // forward solves on the tensor engine: the updates also write g p and g s
+
+  BicgsRun(isg_ctx *c_, float2 *x_, const float2 *g_, int64_t gs_, const float2 *b_, int R_, int hermitian,
+           const isg_solve_opts *o_)
+      : c(c_), x(x_), g(g_), b(b_), gs(gs_), R(R_), o(o_) {
+    kind = hermitian ? OP_ADJ : OP_FWD;
+    engine = o->engine;
+    nbv = c->vec_blocks;
+    nbn = (engine == ISG_ENGINE_TENSOR && tc_available(c)) ? tc_near_blocks(c) : near_blocks_per_rhs(c->P);
+    check = std::max(1, o->check_every);
+    zero_guess = o->guess == ISG_GUESS_ZERO;
+    gx = (kind == OP_FWD && engine == ISG_ENGINE_TENSOR && tc_available(c)) ? c->vgx : nullptr;
   }
-  count_launch();
-  k_init<<<vgrid, 256, 0, st>>>(b, c->vt, x, c->vr, c->vrt, U, zero_guess, c->part);
-  cudaMemsetAsync(c->count, 0, sizeof(int), st);
-  count_launch();
-  k_fin_init<<<R, 256, 0, st>>>(c->state, c->active, c->count, c->part, nbv, zero_guess, tol);
-  if ((e = cuda_check(c, cudaGetLastError(), "bicgs init")) != ISG_OK) return e;
+  dim3 vgrid() const { return dim3(nbv, R); }
+  long host_cap() const { return (long)(o->maxit + 2) * (o->max_restarts + 1) + 8; }
 
-  const int check = std::max(1, o->check_every);
-  const long host_cap = (long)(o->maxit + 2) * (o->max_restarts + 1) + 8;
-  long host_iters = 0;
+  isg_status init(cudaStream_t st) {
+    if (!zero_guess) {
+      isg_status e = run_matvec(c, x, g, gs, c->vt, R, kind, engine, RED_NONE, nullptr, nullptr, st);
+      if (e != ISG_OK) return e;
+    }
+    count_launch();
+    k_init<<<vgrid(), 256, 0, st>>>(b, c->vt, x, c->vr, c->vrt, c->P.U, zero_guess, c->part);
+    cudaMemsetAsync(c->count, 0, sizeof(int), st);
+    count_launch();
+    k_fin_init<<<R, 256, 0, st>>>(c->state, c->active, c->count, c->part, nbv, zero_guess, o->tol);
+    return cuda_check(c, cudaGetLastError(), "bicgs init");
+  }
   // `check` iterations of every active RHS (bicgs.cpp:120-177); inactive ones return at once
-  // forward solves on the tensor engine: the updates also write g p and g s,
-  // which the leaf kernels then read instead of forming them
-  float2 *gx = (kind == OP_FWD && engine == ISG_ENGINE_TENSOR && tc_available(c)) ? c->vgx : nullptr;
-  auto block = [&]() -> isg_status {
+  isg_status block(cudaStream_t st) {
+    const int U = c->P.U;
     for (int k = 0; k < check; k++) {
       count_launch();
-      k_update_p<<<vgrid, 256, 0, st>>>(c->state, c->active, c->vr, c->vp, c->vv, U, g, gs, gx);
+      k_update_p<<<vgrid(), 256, 0, st>>>(c->state, c->active, c->vr, c->vp, c->vv, U, g, gs, gx);
       isg_status be = run_matvec(c, c->vp, g, gs, c->vv, R, kind, engine, RED_DOT, c->vrt, c->active, st, gx);
       if (be != ISG_OK) return be;
       count_launch();
       k_fin_alpha<<<R, 256, 0, st>>>(c->state, c->active, c->part, nbn);
       count_launch();
-      k_update_s<<<vgrid, 256, 0, st>>>(c->state, c->active, c->vr, c->vv, c->vs, U, g, gs, gx);
+      k_update_s<<<vgrid(), 256, 0, st>>>(c->state, c->active, c->vr, c->vv, c->vs, U, g, gs, gx);
       be = run_matvec(c, c->vs, g, gs, c->vt, R, kind, engine, RED_TS, nullptr, c->active, st, gx);
       if (be != ISG_OK) return be;
       count_launch();
       k_fin_omega<<<R, 256, 0, st>>>(c->state, c->active, c->part, nbn);
       count_launch();
-      k_update_xr<<<vgrid, 256, 0, st>>>(c->state, c->active, x, c->vr, c->vrt, c->vp, c->vs, c->vt, U, c->part);
+      k_update_xr<<<vgrid(), 256, 0, st>>>(c->state, c->active, x, c->vr, c->vrt, c->vp, c->vs, c->vt, U, c->part);
       cudaMemsetAsync(c->count, 0, sizeof(int), st);
       count_launch();
-      k_fin_iter<<<R, 256, 0, st>>>(c->state, c->active, c->count, c->part, nbv, tol, o->maxit);
+      k_fin_iter<<<R, 256, 0, st>>>(c->state, c->active, c->count, c->part, nbv, o->tol, o->maxit);
     }
     return cuda_check(c, cudaGetLastError(), "bicgs iteration");
-  };
+  }
+  void read_count(cudaStream_t st) {
+    cudaMemcpyAsync(c->h_count, c->count, sizeof(int), cudaMemcpyDeviceToHost, st);
+  }
+  // True residual b - A x of every RHS; restarts any that stopped early (k_fin_true).
+  isg_status true_residual(cudaStream_t st) {
+    isg_status e = run_matvec(c, x, g, gs, c->vt, R, kind, engine, RED_NONE, nullptr, nullptr, st);
+    if (e != ISG_OK) return e;
+    count_launch();
+    k_true_res<<<vgrid(), 256, 0, st>>>(b, c->vt, c->vr, c->vrt, c->P.U, c->part);
+    cudaMemsetAsync(c->count, 0, sizeof(int), st);
+    count_launch();
+    k_fin_true<<<R, 256, 0, st>>>(c->state, c->active, c->count, c->part, nbv, o->tol, o->max_restarts, o->maxit);
+    read_count(st);
+    return ISG_OK;
+  }
+  isg_status results(isg_solve_info *info, cudaStream_t st) {
+    std::vector<RhsState> hs(R);
+    cudaMemcpyAsync(hs.data(), c->state, R * sizeof(RhsState), cudaMemcpyDeviceToHost, st);
+    isg_status e = cuda_check(c, cudaStreamSynchronize(st), "bicgs results");
+    if (e != ISG_OK) return e;
+    if (engine == ISG_ENGINE_TENSOR && tc_error(c)) {
+      c->err = "a tensor-core kernel hit its wait limit";
+      return ISG_TIMEOUT;
+    }
+    isg_status worst = ISG_OK;
+    for (int r = 0; r < R; r++) {
+      if (info) {
+        info[r].iterations = hs[r].iter;
+        info[r].matvecs = hs[r].matvecs;
+        info[r].status = hs[r].status;
+        info[r].restarts = hs[r].restarts;
+        info[r].residual = hs[r].err;
+        info[r].true_residual = hs[r].tres;
+      }
+      if (hs[r].status != ISG_OK && (worst == ISG_OK || hs[r].status > worst)) worst = (isg_status)hs[r].status;
+    }
+    return worst;
+  }
+};
+
+bool capturable(const isg_solve_opts *o, cudaStream_t st) {
+  return o->graph && st != nullptr && st != cudaStreamLegacy && st != cudaStreamPerThread;
+}
+
+}  // namespace
+
+isg_status run_bicgs(isg_ctx *c, float2 *x, const float2 *g, int64_t gs, const float2 *b, int R, int hermitian,
+                     const isg_solve_opts *o, isg_solve_info *info, cudaStream_t st) {
+  BicgsRun run(c, x, g, gs, b, R, hermitian, o);
+  isg_status e = run.init(st);
+  if (e != ISG_OK) return e;
+  const long host_cap = run.host_cap();
+  long host_iters = 0;
   // The block's launches depend only on the pointers and sizes below, so it is
   // captured once and replayed (not on the legacy default stream, which cannot
-  // be captured).
+  // be captured); the executable graph is cached in the context.
   isg_ctx::GraphKey key;
   key.x = x;
   key.g = g;
   key.gs = gs;
   key.R = R;
-  key.kind = kind;
-  key.engine = engine;
-  key.check = check;
+  key.kind = run.kind;
+  key.engine = run.engine;
+  key.check = run.check;
   key.maxit = o->maxit;
-  key.tol = tol;
-  const bool want_graph = o->graph && st != nullptr && st != cudaStreamLegacy && st != cudaStreamPerThread;
+  key.tol = o->tol;
   auto replay = [&]() -> isg_status {
     if (!(c->graph_exec && c->graph_key == key)) {
       if (c->graph_exec) cudaGraphExecDestroy((cudaGraphExec_t)c->graph_exec);
@@ -470,7 +535,7 @@ isg_status run_bicgs(isg_ctx *c, float2 *x, const float2 *g, int64_t gs, const f
       isg_status ce = cuda_check(c, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "graph capture");
       if (ce != ISG_OK) return ce;
       capture_launches(&captured);
-      isg_status be = block();
+      isg_status be = run.block(st);
       capture_launches(nullptr);
       cudaGraph_t gr = nullptr;
       ce = cuda_check(c, cudaStreamEndCapture(st, &gr), "graph capture end");
@@ -489,46 +554,120 @@ isg_status run_bicgs(isg_ctx *c, float2 *x, const float2 *g, int64_t gs, const f
     count_launch((int)c->graph_launches);
     return cuda_check(c, cudaGraphLaunch((cudaGraphExec_t)c->graph_exec, st), "graph launch");
   };
+  const bool want_graph = capturable(o, st);
   for (;;) {
-    cudaMemcpyAsync(c->h_count, c->count, sizeof(int), cudaMemcpyDeviceToHost, st);
+    run.read_count(st);
     if ((e = cuda_check(c, cudaStreamSynchronize(st), "bicgs poll")) != ISG_OK) return e;
     if (*c->h_count > 0 && host_iters < host_cap) {
-      if ((e = want_graph ? replay() : block()) != ISG_OK) return e;
-      host_iters += check;
+      if ((e = want_graph ? replay() : run.block(st)) != ISG_OK) return e;
+      host_iters += run.check;
       continue;
     }
     if (!o->true_residual) break;
-    // True residual of every RHS; restarts any that stopped early.
-    e = run_matvec(c, x, g, gs, c->vt, R, kind, engine, RED_NONE, nullptr, nullptr, st);
-    if (e != ISG_OK) return e;
-    count_launch();
-    k_true_res<<<vgrid, 256, 0, st>>>(b, c->vt, c->vr, c->vrt, U, c->part);
-    cudaMemsetAsync(c->count, 0, sizeof(int), st);
-    count_launch();
-    k_fin_true<<<R, 256, 0, st>>>(c->state, c->active, c->count, c->part, nbv, tol, o->max_restarts, o->maxit);
-    cudaMemcpyAsync(c->h_count, c->count, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if ((e = run.true_residual(st)) != ISG_OK) return e;
     if ((e = cuda_check(c, cudaStreamSynchronize(st), "bicgs true residual")) != ISG_OK) return e;
     if (*c->h_count == 0 || host_iters >= host_cap) break;
   }
+  return run.results(info, st);
+}
 
-  std::vector<RhsState> hs(R);
-  cudaMemcpyAsync(hs.data(), c->state, R * sizeof(RhsState), cudaMemcpyDeviceToHost, st);
-  if ((e = cuda_check(c, cudaStreamSynchronize(st), "bicgs results")) != ISG_OK) return e;
-  if (engine == ISG_ENGINE_TENSOR && tc_error(c)) {
-    c->err = "a tensor-core kernel hit its wait limit";
-    return ISG_TIMEOUT;
-  }
-  isg_status worst = ISG_OK;
-  for (int r = 0; r < R; r++) {
-    if (info) {
-      info[r].iterations = hs[r].iter;
-      info[r].matvecs = hs[r].matvecs;
-      info[r].status = hs[r].status;
-      info[r].restarts = hs[r].restarts;
-      info[r].residual = hs[r].err;
-      info[r].true_residual = hs[r].tres;
+// Several contexts' batches solved together (same device, same options).  One
+// host poll reads every member's active count; each block of `check`
+// iterations of all members is one CUDA graph whose branches are the members'
+// iteration blocks on forked streams (joined back on st), captured once per
+// call and launched once per poll.  The true-residual checks run member after
+// member on st.  Results go to each member's info; returns the worst status.
+isg_status run_bicgs_group(int n, isg_ctx *const *cs, float2 *const *xs, const float2 *const *gs_, const int64_t *gss,
+                           const float2 *const *bs, const int *Rs, int hermitian, const isg_solve_opts *o,
+                           isg_solve_info *const *infos, cudaStream_t st) {
+  std::vector<BicgsRun> runs;
+  runs.reserve(n);
+  for (int i = 0; i < n; i++) runs.emplace_back(cs[i], xs[i], gs_[i], gss[i], bs[i], Rs[i], hermitian, o);
+  isg_ctx *c0 = cs[0];
+  isg_status e = ISG_OK;
+  for (auto &r : runs)
+    if ((e = r.init(st)) != ISG_OK) return e;
+  long host_cap = 0;
+  for (auto &r : runs) host_cap = std::max(host_cap, r.host_cap());
+  long host_iters = 0;
+  std::vector<cudaStream_t> side(n, nullptr);
+  std::vector<cudaEvent_t> join(n, nullptr);
+  cudaEvent_t fork = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int64_t captured = 0;
+  auto cleanup = [&]() {
+    if (exec) cudaGraphExecDestroy(exec);
+    for (int i = 0; i < n; i++) {
+      if (join[i]) cudaEventDestroy(join[i]);
+      if (side[i]) cudaStreamDestroy(side[i]);
     }
-    if (hs[r].status != ISG_OK && (worst == ISG_OK || hs[r].status > worst)) worst = (isg_status)hs[r].status;
+    if (fork) cudaEventDestroy(fork);
+  };
+  const bool want_graph = capturable(o, st);
+  auto step = [&]() -> isg_status {
+    if (!want_graph) {
+      for (auto &r : runs)
+        if ((e = r.block(st)) != ISG_OK) return e;
+      return ISG_OK;
+    }
+    if (!exec) {
+      isg_status ce = cuda_check(c0, cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), "group event");
+      for (int i = 0; i < n && ce == ISG_OK; i++) {
+        ce = cuda_check(c0, cudaStreamCreateWithFlags(&side[i], cudaStreamNonBlocking), "group stream");
+        if (ce == ISG_OK) ce = cuda_check(c0, cudaEventCreateWithFlags(&join[i], cudaEventDisableTiming), "group event");
+      }
+      if (ce != ISG_OK) return ce;
+      if ((ce = cuda_check(c0, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "group capture")) != ISG_OK)
+        return ce;
+      capture_launches(&captured);
+      isg_status be = cuda_check(c0, cudaEventRecord(fork, st), "group fork");
+      for (int i = 0; i < n && be == ISG_OK; i++) {
+        be = cuda_check(c0, cudaStreamWaitEvent(side[i], fork, 0), "group fork");
+        if (be == ISG_OK) be = runs[i].block(side[i]);
+        if (be == ISG_OK) be = cuda_check(c0, cudaEventRecord(join[i], side[i]), "group join");
+        if (be == ISG_OK) be = cuda_check(c0, cudaStreamWaitEvent(st, join[i], 0), "group join");
+      }
+      capture_launches(nullptr);
+      cudaGraph_t gr = nullptr;
+      ce = cuda_check(c0, cudaStreamEndCapture(st, &gr), "group capture end");
+      if (be != ISG_OK || ce != ISG_OK) {
+        if (gr) cudaGraphDestroy(gr);
+        return be != ISG_OK ? be : ce;
+      }
+      ce = cuda_check(c0, cudaGraphInstantiate(&exec, gr, 0), "group instantiate");
+      cudaGraphDestroy(gr);
+      if (ce != ISG_OK) return ce;
+    }
+    count_launch((int)captured);
+    return cuda_check(c0, cudaGraphLaunch(exec, st), "group graph launch");
+  };
+  auto active = [&]() {
+    long t = 0;
+    for (auto &r : runs) t += *r.c->h_count;
+    return t;
+  };
+  for (;;) {
+    for (auto &r : runs) r.read_count(st);
+    if ((e = cuda_check(c0, cudaStreamSynchronize(st), "group poll")) != ISG_OK) break;
+    if (active() > 0 && host_iters < host_cap) {
+      if ((e = step()) != ISG_OK) break;
+      host_iters += runs[0].check;
+      continue;
+    }
+    if (!o->true_residual) break;
+    for (auto &r : runs)
+      if ((e = r.true_residual(st)) != ISG_OK) break;
+    if (e != ISG_OK) break;
+    if ((e = cuda_check(c0, cudaStreamSynchronize(st), "group true residual")) != ISG_OK) break;
+    if (active() == 0 || host_iters >= host_cap) break;
+  }
+  cleanup();
+  if (e != ISG_OK) return e;
+  isg_status worst = ISG_OK;
+  for (int i = 0; i < n; i++) {
+    const isg_status ri = runs[i].results(infos ? infos[i] : nullptr, st);
+    if (ri == ISG_CUDA_ERROR || ri == ISG_TIMEOUT) return ri;
+    if (ri != ISG_OK && (worst == ISG_OK || ri > worst)) worst = ri;
   }
   return worst;
 }

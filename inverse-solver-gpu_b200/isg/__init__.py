@@ -54,6 +54,11 @@ class SolveInfo(ctypes.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class GroupMember(ctypes.Structure):
+    _fields_ = [("ctx", ctypes.c_void_p), ("x", ctypes.c_void_p), ("g", ctypes.c_void_p), ("g_stride", ctypes.c_int64),
+                ("b", ctypes.c_void_p), ("nrhs", ctypes.c_int), ("info", ctypes.POINTER(SolveInfo))]
+
+
 class DbimOpts(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int), ("regular", ctypes.c_double), ("start_from_chi", ctypes.c_int),
                 ("solve", SolveOpts), ("warm_start", ctypes.c_int), ("checkpoint", ctypes.c_char_p)]
@@ -101,6 +106,7 @@ SIGNATURES = {
     "isg_mlfma": (_I, [_P, _P, _P, _I, _I, _I, _I, _P]),
     "isg_matvec": (_I, [_P, _P, _P, _L, _P, _I, _I, _I, _I, _P]),
     "isg_bicgs": (_I, [_P, _P, _P, _L, _P, _I, _I, _I, ctypes.POINTER(SolveOpts), ctypes.POINTER(SolveInfo), _P]),
+    "isg_bicgs_group": (_I, [_I, ctypes.POINTER(GroupMember), _I, _I, ctypes.POINTER(SolveOpts), _P]),
     "isg_aggregate": (_I, [_P, _P, _P, _I, _I, _P]),
     "isg_aggregateh": (_I, [_P, _P, _P, _I, _I, _P]),
     "isg_aggregate_noalloc": (_I, [_P, _P, _P, _I, _I, _P]),
@@ -167,6 +173,27 @@ def _stream(stream) -> int | None:
         if cur.cuda_stream != stream.cuda_stream:
             stream.wait_stream(cur)
     return stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+
+
+def bicgs_group(members, hermitian: bool = False, order: int = ORDER_TREE, opts: SolveOpts | None = None,
+                stream=None, check: bool = False, **kw) -> list[list[dict]]:
+    """isg_bicgs_group: BiCGSTAB for several independent problems at once.
+    members: (solver, x, g, b) per problem, distinct Solvers (contexts) on one
+    device, tensors as for Solver.bicgs.  Returns per member its per-RHS info."""
+    o = opts if opts is not None else default_solve_opts(**kw)
+    arr = (GroupMember * len(members))()
+    infos = []
+    for i, (s, x, g, b) in enumerate(members):
+        n = s._nrhs(b)
+        inf = (SolveInfo * n)()
+        infos.append(inf)
+        arr[i].ctx, arr[i].x, arr[i].g, arr[i].b, arr[i].nrhs = s._h, _ptr(x), _ptr(g), _ptr(b), n
+        arr[i].g_stride = 0 if g.dim() == 1 else s.numunk
+        arr[i].info = ctypes.cast(inf, ctypes.POINTER(SolveInfo))
+    st = lib().isg_bicgs_group(len(members), arr, int(hermitian), order, ctypes.byref(o), _stream(stream))
+    if st in (4, 5, 7, 8) or (check and st != 0):
+        members[0][0]._check(st, "bicgs_group")
+    return [[i.as_dict() for i in inf] for inf in infos]
 
 
 def kernel_launches() -> int:

@@ -2,18 +2,16 @@
 
 Problems that share a grid size become one multi-RHS block: every transmitter
 of every such problem is one right-hand side, with its own contrast (g_stride =
-numunk) and its own convergence mask inside isg_bicgs, in chunks of at most
-`max_rhs`.  The size groups run at the same time, each driven by its own host
-thread on its own CUDA stream (isg_bicgs releases the interpreter while it
-polls convergence).  The reference solves one problem at a time (mom.cpp:250-350);
-this is the library's batching of its solve path, with the same per-RHS
-results.
+numunk) and its own convergence mask, in chunks of at most `max_rhs`.  The
+size groups are solved together by isg_bicgs_group, one chunk of every group
+per call: each block of iterations of all of them is one CUDA-graph launch
+(one branch per grid size) and one host poll.  The reference solves one
+problem at a time (mom.cpp:250-350); this is the library's batching of its
+solve path, with the same per-RHS results.
 """
 from __future__ import annotations
 
-import threading
-
-from . import ENGINE_TENSOR, ORDER_TREE, Solver, default_solve_opts
+from . import ENGINE_TENSOR, ORDER_TREE, Solver, bicgs_group, default_solve_opts
 
 
 def level_of(numunk: int, box: int = 8) -> int:
@@ -55,41 +53,34 @@ class MultiSolver:
         for p, (g, b) in enumerate(problems):
             groups.setdefault(level_of(g.shape[-1]), []).append(p)
         out: list = [None] * len(problems)
-        errors: list = []
         for lvl in groups:
-            self.solver(lvl)  # built here, not in the worker threads
-        torch.cuda.synchronize(self.device)  # the inputs are complete before other streams read them
-
-        def run(level: int, idx: list[int]):
-            try:
-                s = self.solver(level)
-                stream = torch.cuda.Stream(device=self.device)
-                opts = default_solve_opts(tol=tol, maxit=maxit, engine=self.engine, check_every=check_every)
-                # (problem, transmitter) pairs of the group, in order
-                pairs = [(p, t) for p in idx for t in range(problems[p][1].shape[0])]
-                infos = {p: [None] * problems[p][1].shape[0] for p in idx}
-                with torch.cuda.stream(stream):
-                    xs = {p: torch.zeros_like(problems[p][1]) for p in idx}
-                    for c0 in range(0, len(pairs), self.max_rhs):
-                        chunk = pairs[c0:c0 + self.max_rhs]
-                        G = torch.stack([problems[p][0] for p, _ in chunk])
-                        B = torch.stack([problems[p][1][t] for p, t in chunk])
-                        X = torch.zeros_like(B)
-                        inf = s.bicgs(X, G, B, order=order, opts=opts, stream=stream)
-                        for j, (p, t) in enumerate(chunk):
-                            xs[p][t].copy_(X[j])
-                            infos[p][t] = inf[j]
-                stream.synchronize()
-                for p in idx:
-                    out[p] = (xs[p], infos[p])
-            except Exception as e:  # reported on the calling thread
-                errors.append(e)
-
-        threads = [threading.Thread(target=run, args=(lvl, idx)) for lvl, idx in sorted(groups.items())]
-        for th in threads:
-            th.start()
-        for th in threads:
-            th.join()
-        if errors:
-            raise errors[0]
+            self.solver(lvl)
+        opts = default_solve_opts(tol=tol, maxit=maxit, engine=self.engine, check_every=check_every)
+        # (problem, transmitter) pairs of each group, in order, cut into chunks of max_rhs
+        chunks = {lvl: [] for lvl in groups}
+        for lvl, idx in groups.items():
+            pairs = [(p, t) for p in idx for t in range(problems[p][1].shape[0])]
+            chunks[lvl] = [pairs[c:c + self.max_rhs] for c in range(0, len(pairs), self.max_rhs)]
+        xs = {p: torch.zeros_like(problems[p][1]) for p in range(len(problems))}
+        infos = {p: [None] * problems[p][1].shape[0] for p in range(len(problems))}
+        stream = torch.cuda.Stream(device=self.device)
+        with torch.cuda.stream(stream):
+            for r in range(max(len(c) for c in chunks.values())):
+                members, picks = [], []
+                for lvl in sorted(chunks):
+                    if r >= len(chunks[lvl]):
+                        continue
+                    chunk = chunks[lvl][r]
+                    G = torch.stack([problems[p][0] for p, _ in chunk])
+                    B = torch.stack([problems[p][1][t] for p, t in chunk])
+                    members.append((self.solver(lvl), torch.zeros_like(B), G, B))
+                    picks.append(chunk)
+                res = bicgs_group(members, order=order, opts=opts, stream=stream)
+                for (_, X, _, _), chunk, inf in zip(members, picks, res):
+                    for j, (p, t) in enumerate(chunk):
+                        xs[p][t].copy_(X[j])
+                        infos[p][t] = inf[j]
+        stream.synchronize()
+        for p in range(len(problems)):
+            out[p] = (xs[p], infos[p])
         return out
