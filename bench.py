@@ -382,8 +382,9 @@ def run_config3(isg, torch, dev, seed: int = 3000) -> dict:
     """64 independent forward problems, grid sides drawn from {128, 256, 512,
     1024}, 16-128 plane-wave transmitters each, random ellipses eps_r in
     [1.1, 1.8], solved together by isg.multi.MultiSolver (one multi-RHS block
-    per grid size, per-RHS contrasts and masks, the size groups on concurrent
-    streams) to true residual 1e-5."""
+    per grid size, per-RHS contrasts and masks, the sizes' iteration blocks as
+    branches of one CUDA graph per poll, isg_bicgs_group) to true residual
+    1e-5."""
     from isg.multi import MultiSolver, level_of
     rng = np.random.default_rng(seed)
     ms = MultiSolver(max_rhs=256, device=dev.index or 0, engine=isg.ENGINE_TENSOR)
