@@ -842,7 +842,7 @@ def main():
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
-    if rank == 0 and not args.no_cpu:
+    if rank == 0 and world == 1 and not args.no_cpu:  # the CPU baseline and the FP64 check: one GPU only
         from _oracle import Reference
         if Reference.available():
             ref = Reference(LEVEL, 2 * math.pi, 32)
