@@ -86,6 +86,16 @@ __device__ __forceinline__ void ring_load8(const BandArgs &A, const RingRef &r, 
   } else {
     j0 = (kw0 + kk0) % A.ns_in;  // the window may be longer than the ring; weights past it are zero
   }
+  if (r.p && !(j0 & 1) && j0 + 8 <= A.ns_in) {  // eight samples inside the ring, 16-byte aligned
+    const float4 *q4 = (const float4 *)(r.p + j0);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const float4 t = q4[k];
+      v[2 * k] = make_float2(t.x, t.y);
+      v[2 * k + 1] = make_float2(t.z, t.w);
+    }
+    return;
+  }
 #pragma unroll
   for (int k = 0; k < 8; k++) {
     int j = j0 + k;
