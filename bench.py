@@ -185,9 +185,10 @@ def cpu_reference_sample(ref, g, b, budget_s: float, max_solves: int):
                       f"{threads} OpenMP threads, {t_total:.1f} s"}, x0
 
 
-def field_parity(ref, g, b_tx, x_ours, x_fp64_same_tol, tx: int) -> dict:
+def field_parity(ref, g, b_tx, x_ours, x_fp64_same_tol, tx: int):
     """Relative L2 error of our field against the reference's FP64 solver
-    converged to 1e-10 (and of the reference's own 1e-5 run against it)."""
+    converged to 1e-10 (and of the reference's own 1e-5 run against it);
+    returns the record and that FP64 field."""
     from _oracle import rel
     t0 = time.perf_counter()
     x10, it10 = ref.bicgs(g, b_tx, False, 1e-10, 2000)
@@ -197,7 +198,7 @@ def field_parity(ref, g, b_tx, x_ours, x_fp64_same_tol, tx: int) -> dict:
     if x_fp64_same_tol is not None:
         out["fp64_at_tol_field_err_vs_fp64"] = rel(x_fp64_same_tol, x10)
         out["field_err_vs_fp64_at_tol"] = rel(x_ours, x_fp64_same_tol)
-    return out
+    return out, x10
 
 
 def max_over_ranks(v: float, dist, device) -> float:
@@ -208,6 +209,54 @@ def max_over_ranks(v: float, dist, device) -> float:
     t = torch.tensor([v], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def run_reference_gpu(args):
+    """--impl reference-gpu (a helper process of the one-GPU run): forward
+    solves of the workload through the reference's own GPU path (FP64,
+    oracle/_ref/libisgref_gpu.so), timed by the host clock around each
+    synchronous call; Tx 0's field goes to --ref-gpu-out."""
+    from _oracle import ReferenceGpu
+    ref = ReferenceGpu(LEVEL, 2 * math.pi, 32)
+    txs = list(range(args.warmup + args.steps))
+    g, b = reference_inputs(ref, 0, txs)
+    times, its = [], []
+    for k, tx in enumerate(txs):
+        t0 = time.perf_counter()
+        x, it = ref.bicgs(g, b[tx], False, TOL, 300)
+        dt = time.perf_counter() - t0
+        if tx == 0 and args.ref_gpu_out:
+            np.save(args.ref_gpu_out, x)
+        if k >= args.warmup:
+            times.append(dt)
+            its.append(it)
+    print(json.dumps({"value": len(times) / sum(times), "unit": "solves/s", "solves": len(times),
+                      "mean_iterations": float(np.mean(its)), "seconds_per_solve": sum(times) / len(times)}))
+
+
+def reference_gpu_sample(x10) -> dict:
+    """The reference's own GPU path on this GPU, in a child process (its error
+    handler exits on a CUDA error); x10: the FP64 solution of Tx 0 for the
+    error of the reference's field."""
+    from _oracle import ReferenceGpu, rel
+    if not ReferenceGpu.available():
+        return {"unavailable": "oracle/_ref/libisgref_gpu.so was not built"}
+    with tempfile.TemporaryDirectory() as d:
+        out = os.path.join(d, "x0.npy")
+        try:
+            r = subprocess.run([sys.executable, os.path.abspath(__file__), "--impl", "reference-gpu", "--steps", "2",
+                                "--warmup", "1", "--ref-gpu-out", out], capture_output=True, text=True, timeout=900)
+        except subprocess.TimeoutExpired:
+            return {"unavailable": "the reference's GPU path did not finish 3 solves in 900 s"}
+        lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+        if r.returncode != 0 or not lines:
+            return {"unavailable": f"the reference's GPU path exited with {r.returncode}: {r.stderr[-300:]}"}
+        res = json.loads(lines[-1])
+        res["kind"] = ("the reference's own GPU path (gpu.cu, kernels.cu, matvec_gpu.cu, bicgs_gpu.cu; FP64, "
+                       "one transmitter per solve), compiled for sm_100a")
+        if x10 is not None and os.path.exists(out):
+            res["tx0_field_err_vs_fp64"] = rel(np.load(out), x10)
+        return res
 
 
 def run_reference_arm(args, rank: int, world: int):
@@ -640,7 +689,8 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-gpu"])
+    ap.add_argument("--ref-gpu-out", default="", help=argparse.SUPPRESS)
     ap.add_argument("--engine", default="auto", choices=["auto", "simt", "tensor"])
     ap.add_argument("--plain-sample", type=int, default=4, help="single-RHS solves timed for the plain solvers")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
@@ -660,6 +710,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
+        return
+    if args.impl == "reference-gpu":
+        run_reference_gpu(args)
         return
 
     import torch
@@ -847,7 +900,10 @@ def main():
         if Reference.available():
             ref = Reference(LEVEL, 2 * math.pi, 32)
             out["cpu_baseline"], x5 = cpu_reference_sample(ref, g_np, b_np, args.cpu_budget, 8)
-            out["parity"] = field_parity(ref, g_np, b_np[0], x_tx0, x5, 0)
+            out["parity"], x10 = field_parity(ref, g_np, b_np[0], x_tx0, x5, 0)
+            out["reference_gpu"] = reference_gpu_sample(x10)
+            if "value" in out["reference_gpu"]:
+                out["reference_gpu"]["e2e_vs_reference_gpu"] = out["e2e"]["value"] / out["reference_gpu"]["value"]
     if dist:
         dist.barrier()
         dist.destroy_process_group()

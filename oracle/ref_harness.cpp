@@ -1,6 +1,8 @@
 // Harness around the reference's own CPU path (setup_mlfma.cpp, integrate.cpp,
 // solve.cpp, bicgs.cpp, compiled unmodified from the reference tree by
-// oracle/Makefile).  TEST INFRASTRUCTURE ONLY: it is the checker used to pin
+// oracle/Makefile); compiled with REF_GPU, around the reference's GPU path
+// instead (gpu.cu, kernels.cu, matvec_gpu.cu, bicgs_gpu.cu: the same entry
+// points, FP64 on the GPU).  TEST INFRASTRUCTURE ONLY: it is the checker used to pin
 // the restated oracle (isg_oracle.c) and to produce the golden fixtures, and
 // the CPU baseline arm of bench.py.  Nothing in the product links it.
 //
@@ -37,6 +39,9 @@ int matvecin = 0, matvecout = 0;
 // ---- reference routines (vars.h:14-38, bicgs.cpp) ----
 void setup_mlfma();
 void setup_bicgs();
+#ifdef REF_GPU
+void setup_gpu();  // gpu.cu:69, between the two as in mom.cpp:184-190
+#endif
 void mlfma(complex<double> *, complex<double> *);
 void mlfmah(complex<double> *, complex<double> *);
 void aggregate(complex<double> *, complex<double> *);
@@ -107,6 +112,9 @@ int ref_setup(int lvl, double wavenumber, int nrx) {
   if (chdir(dir) != 0) return -4;
   capture_stdout([] {
     setup_mlfma();
+#ifdef REF_GPU
+    setup_gpu();
+#endif
     setup_bicgs();
   });
   if (chdir(cwd) != 0) return -5;

@@ -17,6 +17,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_DIR = os.path.join(ROOT, "oracle")
 ORACLE_LIB = os.path.join(ORACLE_DIR, "liboracle.so")
 REF_LIB = os.path.join(ORACLE_DIR, "_ref", "libisgref.so")
+REF_GPU_LIB = os.path.join(ORACLE_DIR, "_ref", "libisgref_gpu.so")
 
 _P, _I, _D = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
 
@@ -181,15 +182,16 @@ class Reference:
     """The reference's own CPU path (one global instance per process)."""
 
     _lib = None
+    _path = REF_LIB
 
     @classmethod
     def available(cls) -> bool:
-        return os.path.exists(REF_LIB)
+        return os.path.exists(cls._path)
 
     @classmethod
     def lib(cls):
         if cls._lib is None:
-            L = ctypes.CDLL(REF_LIB)
+            L = ctypes.CDLL(cls._path)
             L.ref_setup.argtypes = [_I, _D, _I]
             L.ref_table.restype = _P
             L.ref_table.argtypes = [ctypes.c_char_p, _I]
@@ -249,6 +251,16 @@ class Reference:
         out = np.zeros(2)
         self.L.ref_integrate(t.real, t.imag, b.real, b.imag, _arr(out))
         return complex(out[0], out[1])
+
+
+class ReferenceGpu(Reference):
+    """The reference's own GPU path (gpu.cu, kernels.cu, matvec_gpu.cu,
+    bicgs_gpu.cu: FP64 on the GPU, the product its Makefile links) behind the
+    same harness and entry points.  Load it in a process of its own: its error
+    handler exits the process on any CUDA error (kernels.h gpuAssert)."""
+
+    _lib = None
+    _path = REF_GPU_LIB
 
 
 def rel(a, b) -> float:
