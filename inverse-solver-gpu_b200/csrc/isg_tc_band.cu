@@ -42,7 +42,7 @@ constexpr int kParents = 32;
 constexpr int kKC = 64;           // K chunk
 constexpr int kAHalf = 128 * kKC * 2;    // 16 KB: one FP16 split of an A chunk
 constexpr int kBHalf = kCols * kKC * 2;  // 32 KB
-constexpr int kSmem = 2 * kAHalf + 2 * kBHalf + 256;  // + barriers, TMEM slot, scratch, per-parent maxima
+constexpr int kSmem = 2 * kAHalf + 2 * kBHalf + 256 + 4 * kParents;  // + barriers, TMEM slot, scratch, per-parent maxima and flags
 constexpr int kErrBand = 121;
 
 struct BandArgs {
@@ -120,6 +120,11 @@ __global__ void __launch_bounds__(256, 2) k_tc_band(BandArgs A) {
   float *fscr = (float *)(abar + 3);  // [8]
   unsigned *pmax = (unsigned *)(abar + 16);  // [kParents] output maxima (FP32 bits)
   if (threadIdx.x < kParents) pmax[threadIdx.x] = 0u;
+  int *pvalid = (int *)(pmax + kParents);  // [kParents] the parent exists and its RHS is active
+  if (threadIdx.x < kParents) {
+    const int gp = blockIdx.x * kParents + threadIdx.x;
+    pvalid[threadIdx.x] = gp < A.ncols && !(A.active && !A.active[gp / A.nparents]);
+  }
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int mt = blockIdx.y, m0 = mt * 128;
   const int kw0 = A.kw0[mt], nch = A.nchunk[mt];
@@ -205,6 +210,9 @@ __global__ void __launch_bounds__(256, 2) k_tc_band(BandArgs A) {
   const int qd = warp & 3, h = warp >> 2;
   const int km = m0 + 32 * qd + lane;
   const bool row_ok = ok && km < A.ns_out;
+  float2 sh[4];  // the row's four child shift phases, the same for every parent
+#pragma unroll
+  for (int q = 0; q < 4; q++) sh[q] = row_ok ? __ldg(&A.shift[q * A.ns_out + km]) : make_float2(0.f, 0.f);
   for (int pp = 0; pp < 8; pp++) {
     float d[16];
     tmem_ld16(tmem + ((uint32_t)(32 * qd) << 16) + 128 * h + 16 * pp, d);
@@ -212,17 +220,15 @@ __global__ void __launch_bounds__(256, 2) k_tc_band(BandArgs A) {
     for (int u = 0; u < 2; u++) {
       // the parent is the same for every lane of the warp
       const int pl = 16 * h + 2 * pp + u, gp = blockIdx.x * kParents + pl;
-      if (gp >= A.ncols) continue;
+      if (!pvalid[pl]) continue;
       const int rhs = gp / A.nparents, P = gp % A.nparents;
-      if (A.active && !A.active[rhs]) continue;
       unsigned mbits = 0u;
       if (row_ok) {
         float2 *base = A.dst + (size_t)rhs * A.mp;
         const float *dv = d + 8 * u;
         float2 acc = make_float2(0.f, 0.f);
 #pragma unroll
-        for (int q = 0; q < 4; q++)
-          cfma(acc, __ldg(&A.shift[q * A.ns_out + km]), make_float2(dv[2 * q] * inv, dv[2 * q + 1] * inv));
+        for (int q = 0; q < 4; q++) cfma(acc, sh[q], make_float2(dv[2 * q] * inv, dv[2 * q + 1] * inv));
         base[(size_t)P * A.ns_out + km] = acc;
         mbits = __float_as_uint(fmaxf(fabsf(acc.x), fabsf(acc.y)));
       }
