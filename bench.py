@@ -217,9 +217,16 @@ def run_reference_gpu(args):
     oracle/_ref/libisgref_gpu.so), timed by the host clock around each
     synchronous call; Tx 0's field goes to --ref-gpu-out."""
     from _oracle import ReferenceGpu
-    ref = ReferenceGpu(LEVEL, 2 * math.pi, 32)
-    txs = list(range(args.warmup + args.steps))
-    g, b = reference_inputs(ref, 0, txs)
+    if args.ref_gpu_in:  # another workload's inputs: level, numrx, g and b in tree order
+        d = np.load(args.ref_gpu_in)
+        ref = ReferenceGpu(int(d["level"]), 2 * math.pi, int(d["numrx"]))
+        g = d["g"]
+        b = dict(enumerate(d["b"]))
+        txs = [k % len(b) for k in range(args.warmup + args.steps)]
+    else:
+        ref = ReferenceGpu(LEVEL, 2 * math.pi, 32)
+        txs = list(range(args.warmup + args.steps))
+        g, b = reference_inputs(ref, 0, txs)
     times, its = [], []
     for k, tx in enumerate(txs):
         t0 = time.perf_counter()
@@ -234,20 +241,25 @@ def run_reference_gpu(args):
                       "mean_iterations": float(np.mean(its)), "seconds_per_solve": sum(times) / len(times)}))
 
 
-def reference_gpu_sample(x10) -> dict:
+def reference_gpu_sample(x10, inputs: dict | None = None, steps: int = 2, warmup: int = 1) -> dict:
     """The reference's own GPU path on this GPU, in a child process (its error
     handler exits on a CUDA error); x10: the FP64 solution of Tx 0 for the
-    error of the reference's field."""
+    error of the reference's field.  inputs: another workload's level, numrx,
+    g and b (tree order) instead of the headline workload's."""
     from _oracle import ReferenceGpu, rel
     if not ReferenceGpu.available():
         return {"unavailable": "oracle/_ref/libisgref_gpu.so was not built"}
     with tempfile.TemporaryDirectory() as d:
         out = os.path.join(d, "x0.npy")
+        cmd = [sys.executable, os.path.abspath(__file__), "--impl", "reference-gpu", "--steps", str(steps),
+               "--warmup", str(warmup), "--ref-gpu-out", out]
+        if inputs is not None:
+            np.savez(os.path.join(d, "in.npz"), **inputs)
+            cmd += ["--ref-gpu-in", os.path.join(d, "in.npz")]
         try:
-            r = subprocess.run([sys.executable, os.path.abspath(__file__), "--impl", "reference-gpu", "--steps", "2",
-                                "--warmup", "1", "--ref-gpu-out", out], capture_output=True, text=True, timeout=900)
+            r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
         except subprocess.TimeoutExpired:
-            return {"unavailable": "the reference's GPU path did not finish 3 solves in 900 s"}
+            return {"unavailable": f"the reference's GPU path did not finish {steps + warmup} solves in 900 s"}
         lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
         if r.returncode != 0 or not lines:
             return {"unavailable": f"the reference's GPU path exited with {r.returncode}: {r.stderr[-300:]}"}
@@ -416,7 +428,8 @@ def run_config1(isg, torch, dev, reps: int = 5) -> dict:
     t_cpu = time.perf_counter() - t0
     out["cpu_baseline"] = {"value": ntx / t_cpu, "unit": "solves/s", "cores": threads, "kind": "reference",
                            "sample": f"all {ntx} forward solves, FP64, {threads} OpenMP threads, {t_cpu:.2f} s"}
-    errs = [rel(X[j], ref.bicgs(g64, b64[j], False, 1e-10, 2000)[0]) for j in range(ntx)]
+    x10s = [ref.bicgs(g64, b64[j], False, 1e-10, 2000)[0] for j in range(ntx)]
+    errs = [rel(X[j], x10s[j]) for j in range(ntx)]
     dits = [infos[j]["iterations"] - ref_its[j] for j in range(ntx)]
     out["parity"] = {"max_field_err_vs_fp64": max(errs), "mean_field_err_vs_fp64": float(np.mean(errs)),
                      "bar": 1e-4, "iterations_minus_reference": sorted(set(dits)),
@@ -424,6 +437,10 @@ def run_config1(isg, torch, dev, reps: int = 5) -> dict:
                      "receivers": f"{nrx} near-field samples per Tx computed (isg_receive)",
                      "rx_norm": float(np.linalg.norm(rx))}
     out["speedup_gpu_vs_cpu"] = out["gpu"]["value"] / out["cpu_baseline"]["value"]
+    out["reference_gpu"] = reference_gpu_sample(x10s[0], {"level": level, "numrx": nrx, "g": g64, "b": b64},
+                                                steps=ntx, warmup=2)
+    if "value" in out["reference_gpu"]:
+        out["speedup_gpu_vs_reference_gpu"] = out["gpu"]["value"] / out["reference_gpu"]["value"]
     return out
 
 
@@ -691,6 +708,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-gpu"])
     ap.add_argument("--ref-gpu-out", default="", help=argparse.SUPPRESS)
+    ap.add_argument("--ref-gpu-in", default="", help=argparse.SUPPRESS)
     ap.add_argument("--engine", default="auto", choices=["auto", "simt", "tensor"])
     ap.add_argument("--plain-sample", type=int, default=4, help="single-RHS solves timed for the plain solvers")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
