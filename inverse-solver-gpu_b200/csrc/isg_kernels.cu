@@ -297,12 +297,23 @@ __device__ __forceinline__ const float2 *ring_ptr(const TileArgs &A, const float
   return base + (size_t)rhs * A.mp + off + cl * ns;
 }
 
+// Whether some column c0 .. c0 + cols - 1 of a tiled block exists and belongs
+// to an active RHS; the same answer in every thread of the block (block size
+// >= cols).  A block without one returns before it loads anything: in the last
+// iterations of a batch most RHS have converged, and their columns would
+// otherwise still be staged and multiplied as zeros.
+__device__ __forceinline__ bool any_active_column(const TileArgs &A, int c0) {
+  const int gc = c0 + (int)threadIdx.x;
+  return __syncthreads_or(threadIdx.x < (unsigned)A.cols && gc < A.ncols && !inactive(A.active, gc / A.nparent));
+}
+
 // L2L into the children of each column's parent: z = parent local, four
 // shifted copies shl[q][j] z[j], anterpolated by the tile's band weights and
 // written over the children's locals.
 __global__ void __launch_bounds__(128) k_l2l_tile(TileArgs A) {
   extern __shared__ float2 sm[];
   const int cols = A.cols, TO = A.tb.out, tile = blockIdx.y, c0 = blockIdx.x * cols;
+  if (!any_active_column(A, c0)) return;
   const int a0 = A.tb.a0[tile], wl = A.tb.wl[tile], ld = cols + 1;
   const TileSmem L(A.tb.wmax, ld, TO, cols, 4 * cols, (size_t)4 * TO * ld, true);
   const float2 **sp = (const float2 **)(sm + L.src);
@@ -386,6 +397,7 @@ __global__ void __launch_bounds__(128) k_l2l_tile(TileArgs A) {
 __global__ void __launch_bounds__(128) k_m2m_tile(TileArgs A) {
   extern __shared__ float2 sm[];
   const int cols = A.cols, TO = A.tb.out, tile = blockIdx.y, c0 = blockIdx.x * cols;
+  if (!any_active_column(A, c0)) return;
   const int a0 = A.tb.a0[tile], wl = A.tb.wl[tile], ld = 4 * cols + 1;
   const TileSmem L(A.tb.wmax, ld, TO, 4 * cols, cols, (size_t)TO * (cols + 1));
   const float2 **sp = (const float2 **)(sm + L.src);

@@ -125,6 +125,9 @@ __global__ void __launch_bounds__(256, 2) k_tc_band(BandArgs A) {
     const int gp = blockIdx.x * kParents + threadIdx.x;
     pvalid[threadIdx.x] = gp < A.ncols && !(A.active && !A.active[gp / A.nparents]);
   }
+  // no parent of this CTA exists with an active RHS (converged RHS at the end
+  // of a batch): nothing to load, multiply or write
+  if (!__syncthreads_or(threadIdx.x < kParents && pvalid[threadIdx.x])) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int mt = blockIdx.y, m0 = mt * 128;
   const int kw0 = A.kw0[mt], nch = A.nchunk[mt];
