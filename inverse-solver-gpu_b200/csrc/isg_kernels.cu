@@ -132,6 +132,10 @@ __device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.w
 // (b0 = NC bp), so with NC = 2 one 6 x 8 window feeds 8 outputs (216 complex
 // FMAs) where two NC = 1 threads read 6 x 6 windows each: a third fewer ring
 // loads and cp.async issues per FMA, at 8 instead of 12 warps per SM.
+// Each complex multiply-add is two packed FP32 pair FMAs (fma.rn.f32x2) on
+// two accumulators per output, one for the window value's real part and one
+// for its imaginary part, combined once per step: half the FMA instructions
+// of the scalar form, with the weights kept as their natural (re, im) pairs.
 template <bool ACC, int NC>
 __global__ void __launch_bounds__(kM2lThreads, NC == 1 ? 3 : 2) k_m2l(M2lArgs A) {
   constexpr int NW = m2l_cols(NC);
@@ -143,13 +147,14 @@ __global__ void __launch_bounds__(kM2lThreads, NC == 1 ? 3 : 2) k_m2l(M2lArgs A)
   if (f >= ncp * ns) return;  // no block barrier below
   const int bp = f / ns, k = f - bp * ns, b0 = NC * bp;
   const int a0 = blockIdx.y * A.ty, a1 = min(a0 + A.ty, half);
-  float2 tw[7][7];
+  f32x2 tw[7][7];  // (re, im) of each translation weight as one packed pair
 #pragma unroll
   for (int dy = 0; dy < 7; dy++)
 #pragma unroll
     for (int dx = 0; dx < 7; dx++)
-      tw[dy][dx] = (dy >= 2 && dy <= 4 && dx >= 2 && dx <= 4) ? make_float2(0.f, 0.f)
-                                                              : __ldg(&A.T[(dy * 7 + dx) * ns + k]);
+      tw[dy][dx] = (dy >= 2 && dy <= 4 && dx >= 2 && dx <= 4)
+                       ? 0ull
+                       : __ldg((const unsigned long long *)&A.T[(dy * 7 + dx) * ns + k]);
   const float2 *m = A.mul + (size_t)rhs * A.mp + A.off + k;
   float2 *out = A.loc + (size_t)rhs * A.mp + A.off + k;
   const size_t row_stride = (size_t)A.n * ns;
@@ -203,33 +208,42 @@ __global__ void __launch_bounds__(kM2lThreads, NC == 1 ? 3 : 2) k_m2l(M2lArgs A)
       issue_row(2 * (a + kM2lAhead) + 3);
     }
     cp_async_commit();
-    float2 acc[NC][2][2];
+    // complex products on packed pairs: ax += (w.x, w.x) * (t.x, t.y) and
+    // ay += (w.y, w.y) * (t.x, t.y), so that t w = (ax.x - ay.y, ax.y + ay.x)
+    f32x2 ax[NC][2][2], ay[NC][2][2];
 #pragma unroll
     for (int gx = 0; gx < NC; gx++)
 #pragma unroll
       for (int oy = 0; oy < 2; oy++)
 #pragma unroll
-        for (int ox = 0; ox < 2; ox++) acc[gx][oy][ox] = ob[gx][oy][ox];
+        for (int ox = 0; ox < 2; ox++) {
+          ax[gx][oy][ox] = pk2(ob[gx][oy][ox].x, ob[gx][oy][ox].y);
+          ay[gx][oy][ox] = 0ull;
+        }
     if (a + 1 < a1) old(a + 1, ob);  // the next step's old locals, in flight during this one
     cp_async_wait_group<kM2lAhead>();  // this step's rows have landed
 #pragma unroll
     for (int i = 0; i < 6; i++) {
       const float2 *src = ring + (size_t)((2 * a - 2 + i - r0) % kM2lRing) * NW * kM2lThreads;
-      float2 w[NW];
 #pragma unroll
-      for (int j = 0; j < NW; j++) w[j] = src[j * kM2lThreads];
+      for (int j = 0; j < NW; j++) {
+        const float2 w = src[j * kM2lThreads];
+        const f32x2 wx = pk2(w.x, w.x), wy = pk2(w.y, w.y);
 #pragma unroll
-      for (int gx = 0; gx < NC; gx++)
-#pragma unroll
-        for (int jj = 0; jj < 6; jj++)
+        for (int gx = 0; gx < NC; gx++) {
+          const int jj = j - 2 * gx;
+          if (jj < 0 || jj >= 6) continue;
 #pragma unroll
           for (int oy = 0; oy < 2; oy++)
 #pragma unroll
             for (int ox = 0; ox < 2; ox++) {
               const int dy = i - 2 - oy, dx = jj - 2 - ox;  // source minus target
               if (dy >= -1 && dy <= 1 && dx >= -1 && dx <= 1) continue;
-              cfma(acc[gx][oy][ox], tw[dy + 3][dx + 3], w[2 * gx + jj]);
+              ax[gx][oy][ox] = fma2(wx, tw[dy + 3][dx + 3], ax[gx][oy][ox]);
+              ay[gx][oy][ox] = fma2(wy, tw[dy + 3][dx + 3], ay[gx][oy][ox]);
             }
+        }
+      }
     }
 #pragma unroll
     for (int gx = 0; gx < NC; gx++)
@@ -237,8 +251,10 @@ __global__ void __launch_bounds__(kM2lThreads, NC == 1 ? 3 : 2) k_m2l(M2lArgs A)
       for (int oy = 0; oy < 2; oy++)
 #pragma unroll
         for (int ox = 0; ox < 2; ox++) {
-          out[(size_t)(2 * a + oy) * row_stride + (size_t)(2 * (b0 + gx) + ox) * ns] = acc[gx][oy][ox];
-          mx = fmaxf(mx, fmaxf(fabsf(acc[gx][oy][ox].x), fabsf(acc[gx][oy][ox].y)));
+          const float2 px = upk2(ax[gx][oy][ox]), py = upk2(ay[gx][oy][ox]);
+          const float2 r = make_float2(px.x - py.y, px.y + py.x);
+          out[(size_t)(2 * a + oy) * row_stride + (size_t)(2 * (b0 + gx) + ox) * ns] = r;
+          mx = fmaxf(mx, fmaxf(fabsf(r.x), fabsf(r.y)));
         }
   }
   cp_async_wait_group<0>();
