@@ -7,8 +7,10 @@
 // restricted to the circular window of input samples its rows touch (a few
 // dozen more than 128 x the rate ratio), precomputed on the host as FP16 hi/lo
 // K-chunks of 64 in the core-matrix layout and brought in by bulk copies.  The
-// CTA's 256 MMA columns are 32 parents x 4 children x (re, im) of one level of
-// one or more RHS; ring values are split into FP16 hi/lo after a power-of-two
+// CTA's 128 MMA columns are 16 parents x 4 children x (re, im) of one level of
+// one or more RHS (64 KB of shared memory and 128 TMEM columns, so three CTAs
+// share an SM: each CTA's load, MMA and epilogue phases run one after another,
+// and the SM overlaps them across CTAs); ring values are split into FP16 hi/lo after a power-of-two
 // scale per CTA (3 products, FP32 accumulation in TMEM).  The child shift
 // phases are folded into the epilogue (sum over the four children), exactly as
 // in the reference.
@@ -37,11 +39,11 @@ namespace {
 
 using namespace tc;
 
-constexpr int kCols = 256;        // MMA N: 32 parents x 4 children x (re, im)
-constexpr int kParents = 32;
+constexpr int kCols = 128;        // MMA N: 16 parents x 4 children x (re, im)
+constexpr int kParents = 16;
 constexpr int kKC = 64;           // K chunk
 constexpr int kAHalf = 128 * kKC * 2;    // 16 KB: one FP16 split of an A chunk
-constexpr int kBHalf = kCols * kKC * 2;  // 32 KB
+constexpr int kBHalf = kCols * kKC * 2;  // 16 KB
 constexpr int kSmem = 2 * kAHalf + 2 * kBHalf + 256 + 4 * kParents;  // + barriers, TMEM slot, scratch, per-parent maxima and flags
 constexpr int kErrBand = 121;
 
@@ -111,7 +113,7 @@ __device__ __forceinline__ void ring_load8(const BandArgs &A, const RingRef &r, 
   }
 }
 
-__global__ void __launch_bounds__(256, 2) k_tc_band(BandArgs A) {
+__global__ void __launch_bounds__(256, 3) k_tc_band(BandArgs A) {
   extern __shared__ __align__(1024) char sm[];
   char *ahi = sm, *bhi = sm + 2 * kAHalf, *blo = bhi + kBHalf;
   uint64_t *abar = (uint64_t *)(blo + kBHalf);
@@ -147,7 +149,7 @@ __global__ void __launch_bounds__(256, 2) k_tc_band(BandArgs A) {
     mbar_init(mbar, 1);
     fence_mbar_init();
   }
-  if (warp == 0) tmem_alloc(tslot, 256);
+  if (warp == 0) tmem_alloc(tslot, kCols);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -166,7 +168,7 @@ __global__ void __launch_bounds__(256, 2) k_tc_band(BandArgs A) {
     }
     // B chunk: ring r gives rows 2r (re) and 2r + 1 (im); item = (ring, 8-sample group)
 #pragma unroll 2
-    for (int it = threadIdx.x; it < 128 * (kKC / 8); it += blockDim.x) {
+    for (int it = threadIdx.x; it < 4 * kParents * (kKC / 8); it += blockDim.x) {
       const int r = it >> 3, g8 = it & 7;
       __align__(16) __half hr[8], lr[8], hi8[8], li8[8];
       float2 v[8];
@@ -216,13 +218,13 @@ __global__ void __launch_bounds__(256, 2) k_tc_band(BandArgs A) {
   float2 sh[4];  // the row's four child shift phases, the same for every parent
 #pragma unroll
   for (int q = 0; q < 4; q++) sh[q] = row_ok ? __ldg(&A.shift[q * A.ns_out + km]) : make_float2(0.f, 0.f);
-  for (int pp = 0; pp < 8; pp++) {
+  for (int pp = 0; pp < kCols / 32; pp++) {
     float d[16];
-    tmem_ld16(tmem + ((uint32_t)(32 * qd) << 16) + 128 * h + 16 * pp, d);
+    tmem_ld16(tmem + ((uint32_t)(32 * qd) << 16) + (kCols / 2) * h + 16 * pp, d);
 #pragma unroll
     for (int u = 0; u < 2; u++) {
       // the parent is the same for every lane of the warp
-      const int pl = 16 * h + 2 * pp + u, gp = blockIdx.x * kParents + pl;
+      const int pl = (kParents / 2) * h + 2 * pp + u, gp = blockIdx.x * kParents + pl;
       if (!pvalid[pl]) continue;
       const int rhs = gp / A.nparents, P = gp % A.nparents;
       unsigned mbits = 0u;
@@ -247,7 +249,7 @@ __global__ void __launch_bounds__(256, 2) k_tc_band(BandArgs A) {
     if (gp < A.ncols && pmax[threadIdx.x])
       atomicMax(&A.levmax[(gp / A.nparents) * kMaxLevels + A.lvl_out], pmax[threadIdx.x]);
   }
-  if (warp == 0) tmem_dealloc(tmem, 256);
+  if (warp == 0) tmem_dealloc(tmem, kCols);
 }
 
 // ---- L2L ----
