@@ -94,7 +94,8 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // 8-byte cp.async copies kM2lAhead steps ahead of the step being computed,
 // one commit group per step.  Each thread waits only for its own copies
 // (cp.async.wait_group), so there is no block barrier, and the loads in
-// flight hold no registers (155 registers, three blocks and 12 warps per SM).
+// flight hold no registers (one column per thread: 157 registers, three blocks
+// and 12 warps per SM; two columns: 204 registers, two blocks).
 // Rows outside the grid are the same for the whole block and copy as zeros; a
 // column outside the grid copies zeros by a zero source size.  Consecutive
 // threads take consecutive samples, so every load and store is coalesced.
@@ -110,12 +111,12 @@ struct M2lArgs {
   int lvl;
 };
 
-constexpr int kM2lAhead = 3;                 // steps of window rows in flight ahead of the computing step
+constexpr int kM2lAhead = 2;                 // steps of window rows in flight ahead of the computing step
 constexpr int kM2lRing = 6 + 2 * kM2lAhead;  // row slots per thread
 constexpr int kM2lThreads = 128;
 // window columns per ring row for NC sibling-group columns per thread (6 or 8)
 __host__ __device__ constexpr int m2l_cols(int nc) { return 4 + 2 * nc; }
-__host__ __device__ constexpr size_t m2l_smem(int nc) {  // 72 KB (NC = 1), 96 KB (NC = 2)
+__host__ __device__ constexpr size_t m2l_smem(int nc) {  // 60 KB (NC = 1), 80 KB (NC = 2)
   return (size_t)kM2lRing * m2l_cols(nc) * kM2lThreads * sizeof(float2);
 }
 
