@@ -64,6 +64,33 @@ def test_batched_masks_uneven_difficulty():
         assert rel(Xh[j], xt) < 1e-4
 
 
+@pytest.mark.parametrize("engine", [isg.ENGINE_SIMT, isg.ENGINE_TENSOR])
+def test_converged_columns_are_skipped_without_changing_the_others(engine):
+    """512 x 512 pixels (MLFMA levels 2 .. 6, so the banded tensor-core M2M and
+    the tiled L2L run at the coarse levels).  Two RHS solved in a batch of
+    four whose other two are zero (inactive from the start, so every tree
+    block holding only their columns returns at once, and mixed blocks skip
+    them) give the same fields, iteration counts and residuals bit for bit as
+    the two solved on their own."""
+    import torch
+    s = isg.Solver(7, numrx=16, max_rhs=4)
+    chi = s.raster_to_tree(s.phantom(seed=77, count=4, axis=(1.0, 3.0), eps=(1.1, 1.6)))
+    g = torch.from_numpy(((2 * np.pi) ** 2 * chi).astype(np.complex64)).cuda()
+    b2 = torch.from_numpy(s.plane_waves(16, first=3, count=2).astype(np.complex64)).cuda()
+    b4 = torch.zeros((4, s.numunk), dtype=torch.complex64, device="cuda")
+    b4[0], b4[2] = b2[0], b2[1]
+    opts = isg.default_solve_opts(tol=1e-5, maxit=400, engine=engine, check_every=2)
+    x2, x4 = torch.zeros_like(b2), torch.zeros_like(b4)
+    inf2 = s.bicgs(x2, g, b2, opts=opts)
+    inf4 = s.bicgs(x4, g, b4, opts=opts)
+    torch.cuda.synchronize()
+    assert [i["iterations"] for i in inf4] == [inf2[0]["iterations"], 0, inf2[1]["iterations"], 0]
+    assert all(i["status"] == 0 for i in inf4) and all(0 <= i["true_residual"] <= 1e-5 for i in inf2)
+    assert [inf4[0]["true_residual"], inf4[2]["true_residual"]] == [i["true_residual"] for i in inf2]
+    assert torch.equal(x4[0], x2[0]) and torch.equal(x4[2], x2[1])
+    assert not x4[1].abs().max().item() and not x4[3].abs().max().item()
+
+
 def test_caller_guess_and_iteration_cap():
     s = isg.Solver(4, max_rhs=2)
     o = Oracle(4)
