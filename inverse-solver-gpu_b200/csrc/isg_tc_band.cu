@@ -10,8 +10,9 @@
 // CTA's 128 MMA columns are 16 parents x 4 children x (re, im) of one level of
 // one or more RHS (64 KB of shared memory and 128 TMEM columns, so three CTAs
 // share an SM: each CTA's load, MMA and epilogue phases run one after another,
-// and the SM overlaps them across CTAs); ring values are split into FP16 hi/lo after a power-of-two
-// scale per CTA (3 products, FP32 accumulation in TMEM).  The child shift
+// and the SM overlaps them across CTAs); ring values are split into FP16
+// hi/lo after a power-of-two scale per CTA (3 products, FP32 accumulation in
+// TMEM).  The child shift
 // phases are folded into the epilogue (sum over the four children), exactly as
 // in the reference.
 //
